@@ -1,0 +1,197 @@
+/*
+ * svdimager_b200 — B200-native snapshot imager (drop-in for the imaging path of the
+ * Transient-Oriented Imager, egbdfX/SVDimager).
+ *
+ * C ABI: plain pointers and sizes, status codes, no exceptions across the boundary.
+ * Reference files cited by path relative to the reference project root:
+ *   SVDIntegratedImager.cu (main path), archive/FIPkernels.cu and archive/pipe_interface.cpp
+ *   (archive path).
+ *
+ * Thread safety: every function may be called from any host thread. An engine handle is owned by
+ * one caller at a time (calls on one handle serialise on an internal mutex). The process-wide
+ * default engine used by FIpipe / svdi_fipipe is guarded the same way.
+ */
+#ifndef SVDIMAGER_B200_H
+#define SVDIMAGER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------------ */
+#define SVDI_OK 0
+#define SVDI_ERR_INVALID_ARGUMENT 1   /* null pointer, zero size, non-positive cell size, ... */
+#define SVDI_ERR_EMPTY_INPUT 2        /* zero samples (SVDIntegratedImager.cu:640-642)          */
+#define SVDI_ERR_CUDA 3               /* a CUDA runtime call failed                             */
+#define SVDI_ERR_CUFFT 4              /* a cuFFT call failed                                    */
+#define SVDI_ERR_OUT_OF_MEMORY 5      /* admission refused / device allocation failed          */
+#define SVDI_ERR_UNSUPPORTED 6        /* option outside the implemented range                  */
+#define SVDI_ERR_INTERNAL 7
+
+/* Message of the last failing call on this host thread ("" when none). */
+const char* svdi_last_error(void);
+
+/* ---- archive entry point ----------------------------------------------------------------- */
+/*
+ * Replaces int FIpipe(float* Visreal, float* Visimag, float* Bin, float* Vin, float* dirty_image,
+ *                     size_t num_baselines, size_t image_size, float cell_size)
+ * declared at archive/pipe_interface.cpp:8 and defined at archive/FIPkernels.cu:679.
+ * All pointers are HOST pointers owned by the caller. Visreal/Visimag: [num_baselines] collapsed
+ * visibilities; Bin: [num_baselines][3] rotated baselines in wavelengths (row-major); Vin: 3x3
+ * row-major basis; dirty_image: [image_size][image_size] output. num_baselines counts samples
+ * (rows x channels). Semantics of the archive path: one w-slab, the smallest Chebyshev order in
+ * 1..32 whose sampled Jacobi-Anger error is <= 1e-2 (archive/FIPkernels.cu:287-366), the
+ * trigonometric SIN reprojection (archive/FIPkernels.cu:577-677). Returns SVDI_OK (0) or an error
+ * status (the reference always returns 0 and reports nothing).
+ * The library also exports the C++-linkage symbol `int FIpipe(float*, float*, float*, float*,
+ * float*, size_t, size_t, float)` so that archive/pipe_interface.cpp links against it unchanged.
+ */
+int svdi_fipipe(const float* Visreal, const float* Visimag, const float* Bin, const float* Vin,
+                float* dirty_image, size_t num_baselines, size_t image_size, float cell_size);
+
+/* ---- main-path mirror ---------------------------------------------------------------------- */
+/* Field for field HostMeasurementSetData (SVDIntegratedImager.cu:39-54). Samples are flattened
+ * channel-major: idx = row + chan * num_rows (SVDIntegratedImager.cu:90-92). Host pointers. */
+typedef struct svdi_host_ms {
+    size_t num_rows;
+    size_t num_channels;
+    size_t num_samples;            /* must equal num_rows * num_channels */
+    const float* uvw;              /* [num_rows][3] metres */
+    const float* frequencies_hz;   /* [num_channels] */
+    const float* vis0_real;        /* [num_samples] polarisation 0 */
+    const float* vis0_imag;
+    const float* vis3_real;        /* [num_samples] polarisation 3 */
+    const float* vis3_imag;
+    const uint8_t* flag0;          /* [num_samples] 1 = flagged */
+    const uint8_t* flag3;
+    const float* weight0;          /* [num_samples] WEIGHT_SPECTRUM */
+    const float* weight3;
+    float array_center_x;          /* ARRAY_CENTER.x of the OBSERVATION table (0 = unknown) */
+} svdi_host_ms;
+
+/* Mirror of DevicePreprocessBuffers (SVDIntegratedImager.cu:63-69) with the FP64 extensions the
+ * B200 path keeps: rotated baselines are separable, r[row + chan*R] = s[chan] * q[row]. */
+typedef struct svdi_device_buffers {
+    float* d_bin;                  /* [num_samples][3] float rotated baselines (only if requested) */
+    float* d_vin;                  /* [9] float basis, row-major                               */
+    float* d_vis_real;             /* [num_samples] collapsed visibilities                     */
+    float* d_vis_imag;
+    size_t num_samples;
+    /* extensions */
+    size_t num_rows;
+    size_t num_channels;
+    double* d_vin64;               /* [9] FP64 basis                                            */
+    double* d_q;                   /* [num_rows][3] FP64 Vin . uvw_row (metres)                 */
+    double* d_s;                   /* [num_channels] FP64 f / c                                 */
+    double* d_stats;               /* device scalars: r3 min/max etc. (internal layout)         */
+    void* internal;
+} svdi_device_buffers;
+
+/* Replaces preprocess_measurement_set_gpu (SVDIntegratedImager.cu:635-853): uploads the host data
+ * and computes the FP64 SVD rotation and the flag/weight collapse on the device. want_bin != 0
+ * also materialises the float d_bin array of the reference layout. */
+int svdi_preprocess_measurement_set(const svdi_host_ms* host, svdi_device_buffers* dev, int want_bin);
+
+/* Replaces FIpipeDevice (SVDIntegratedImager.cu:1498-1761): images preprocessed device buffers into
+ * the HOST array dirty_image [image_size][image_size]. Slab + bucket-K semantics
+ * (SVDIntegratedImager.cu:926-991, 1577-1603), simplified SIN reprojection
+ * (SVDIntegratedImager.cu:1325-1379). */
+int svdi_fipipe_device(const svdi_device_buffers* dev, float* dirty_image, size_t image_size,
+                       float cell_size);
+
+/* Replaces free_device_preprocess_buffers (SVDIntegratedImager.cu:855-865). */
+void svdi_free_device_buffers(svdi_device_buffers* dev);
+
+/* ---- engine (device-resident, reusable) -------------------------------------------------- */
+/* New export: the reference allocates, plans and frees on every call (SVDIntegratedImager.cu:1630-
+ * 1676); an engine keeps grids, cuFFT plans, bins and staging buffers resident between calls. */
+typedef struct svdi_engine svdi_engine;
+
+#define SVDI_KRULE_BUCKET 0      /* K in {8,16,24,32}, sampled error <= 1e-2 (main path)        */
+#define SVDI_KRULE_MIN 1         /* smallest K in 1..32, sampled error <= 1e-2 (archive path)   */
+#define SVDI_KRULE_TARGET 2      /* smallest K whose truncation error <= target_error           */
+#define SVDI_KRULE_FIXED 3       /* K = fixed_k                                                 */
+
+#define SVDI_EDGE_CLIP 0         /* reference rule: truncate footprints at the grid edge        */
+#define SVDI_EDGE_STRICT 1       /* drop samples whose footprint leaves the grid                */
+
+#define SVDI_COORD_FP64 0        /* grid coordinates in FP64                                    */
+#define SVDI_COORD_REF32 1       /* the reference's FP32 rounding of Bin * (cell * G)          */
+
+#define SVDI_REPROJ_SII 0        /* simplified SIN deprojection (SVDIntegratedImager.cu)        */
+#define SVDI_REPROJ_FIPK 1       /* trigonometric SIN deprojection (archive/FIPkernels.cu)      */
+
+#define SVDI_GRIDDER_FP32 0      /* tile-local FP32 gridder (CUDA cores, shared memory)         */
+#define SVDI_GRIDDER_TC 1        /* split-precision tcgen05 tensor-core gridder                */
+
+typedef struct svdi_options {
+    int device;                  /* CUDA device ordinal                                        */
+    int k_rule;                  /* SVDI_KRULE_*                                               */
+    int fixed_k;                 /* for SVDI_KRULE_FIXED                                       */
+    double target_error;         /* for SVDI_KRULE_TARGET                                      */
+    double target_alpha;         /* slab alpha target; <= 0: SVD_CHEB_TARGET_ALPHA env or 10   */
+    int edge_mode;               /* SVDI_EDGE_*                                                */
+    int coord_mode;              /* SVDI_COORD_*                                               */
+    int reprojection;            /* SVDI_REPROJ_*                                              */
+    int support;                 /* ES support W (8 in the reference)                          */
+    double beta;                 /* ES beta (15.3704324328 in the reference)                   */
+    double sigma;                /* oversampling, G = ceil(sigma N) (1.5 in the reference)     */
+    int tile;                    /* gridder tile size (32 or 64); 0 = automatic                 */
+    int gridder;                 /* SVDI_GRIDDER_*                                             */
+    size_t max_batch_slabs;      /* 0 = SVDIMAGER_MAX_BATCH_SLABS env or the HBM budget        */
+} svdi_options;
+
+/* Defaults of the reference main path (bucket K, clip, FP64 coordinates, SIN-simplified). */
+void svdi_default_options(svdi_options* opt);
+
+int svdi_engine_create(const svdi_options* opt, svdi_engine** out);
+void svdi_engine_destroy(svdi_engine* e);
+
+/* Full main path from HOST snapshot data to a HOST image (uploads, preprocesses, images). */
+int svdi_engine_image_host(svdi_engine* e, const svdi_host_ms* host, size_t image_size,
+                           float cell_size, float* dirty_image);
+
+/* Device-resident snapshot: the same fields as svdi_host_ms but DEVICE pointers (no upload). */
+int svdi_engine_image_device(svdi_engine* e, const svdi_host_ms* dev_ms, size_t image_size,
+                             float cell_size, float* d_dirty_image, void* cuda_stream);
+
+/* Archive path on an engine: host pointers, same contract as svdi_fipipe. */
+int svdi_engine_fipipe_host(svdi_engine* e, const float* Visreal, const float* Visimag,
+                            const float* Bin, const float* Vin, float* dirty_image,
+                            size_t num_baselines, size_t image_size, float cell_size);
+
+/* Statistics of the last imaging call on an engine. */
+typedef struct svdi_stats {
+    size_t num_samples;          /* N_s (the image normalisation)                              */
+    size_t num_gridded;          /* samples with at least one footprint cell on the grid       */
+    size_t grid_size;            /* G                                                          */
+    int num_slabs;               /* w-slabs                                                    */
+    int num_terms;               /* Chebyshev terms K                                          */
+    int num_planes;              /* num_slabs * K moment planes                                */
+    double r3_min, r3_max;       /* range of the third rotated coordinate (wavelengths)        */
+    double max_abs_t3;           /* max |t3| over valid pixels                                 */
+    size_t valid_pixels;
+    double alpha_max;            /* 2 pi max|t3| (r3 range / 2)                                */
+    double slab_alpha_max;
+    double vin[9];               /* FP64 basis used                                            */
+    float ms_total;              /* device time of the call (CUDA events)                      */
+    float ms_preprocess, ms_bin, ms_grid, ms_fft, ms_image;
+} svdi_stats;
+
+int svdi_engine_last_stats(const svdi_engine* e, svdi_stats* out);
+
+/* Number of kernel launches this library has issued in the calling process. */
+uint64_t svdi_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+
+/* C++ linkage, the exact declaration of archive/pipe_interface.cpp:8. */
+int FIpipe(float* Visreal, float* Visimag, float* Bin, float* Vin, float* dirty_image,
+           size_t num_baselines, size_t image_size, float cell_size);
+#endif
+
+#endif /* SVDIMAGER_B200_H */
