@@ -142,6 +142,10 @@ typedef struct svdi_options {
     int tile;                    /* gridder tile size (32 or 64); 0 = automatic                 */
     int gridder;                 /* SVDI_GRIDDER_*                                             */
     size_t max_batch_slabs;      /* 0 = SVDIMAGER_MAX_BATCH_SLABS env or the HBM budget        */
+    int keep_grid;               /* != 0: keep a copy of the first slab batch's grid before the
+                                    FFT for svdi_engine_copy_buffer (testing aid)              */
+    int presplat;                /* != 0: output the rotated-frame image R(x, y) before the
+                                    reprojection (NaN where the pixel is invalid)              */
 } svdi_options;
 
 /* Defaults of the reference main path (bucket K, clip, FP64 coordinates, SIN-simplified). */
@@ -177,11 +181,28 @@ typedef struct svdi_stats {
     double alpha_max;            /* 2 pi max|t3| (r3 range / 2)                                */
     double slab_alpha_max;
     double vin[9];               /* FP64 basis used                                            */
+    int tile;                    /* gridder tile side T                                        */
+    int num_keys;                /* tile keys: num_slabs * ceil(G/T)^2                         */
+    double slab_r3_min, slab_width, slab_half;  /* slab geometry used by the gridder           */
     float ms_total;              /* device time of the call (CUDA events)                      */
     float ms_preprocess, ms_bin, ms_grid, ms_fft, ms_image;
 } svdi_stats;
 
 int svdi_engine_last_stats(const svdi_engine* e, svdi_stats* out);
+
+/* Intermediate buffers of the last call, for inspection and tests (device-to-host copy). */
+#define SVDI_BUF_VIS_REAL 0      /* float [N_s] collapsed visibilities                         */
+#define SVDI_BUF_VIS_IMAG 1
+#define SVDI_BUF_Q 2             /* double [rows][3] Vin . uvw_row                             */
+#define SVDI_BUF_S 3             /* double [channels] f / c                                    */
+#define SVDI_BUF_VIN 4           /* double [9]                                                 */
+#define SVDI_BUF_OFFSETS 5       /* uint32 [n_keys + 1] record offsets per tile key            */
+#define SVDI_BUF_RECORDS 6       /* 16-byte records {int xq, int yq, float vre, float vim}     */
+#define SVDI_BUF_RECORDS_S 7     /* float Chebyshev argument per record (K > 1)                */
+#define SVDI_BUF_GRID 8          /* complex64 [planes][G][G] grid before the FFT (keep_grid)   */
+#define SVDI_BUF_MOMENTS 9       /* complex64 [planes][G][G] after the FFT (last slab batch)   */
+int svdi_engine_buffer_size(const svdi_engine* e, int which, size_t* bytes);
+int svdi_engine_copy_buffer(svdi_engine* e, int which, void* host_dst, size_t bytes);
 
 /* Number of kernel launches this library has issued in the calling process. */
 uint64_t svdi_kernel_launch_count(void);

@@ -209,21 +209,26 @@ void orc_es_correction(long half_n, long G, int W, double beta, double* phi) {
 }
 
 /* ------------------------------------------------------------------------------------------ */
-/* Footprint of one sample along one axis: cells [ceil(p - W/2), floor(p + W/2)] clipped to   */
-/* the grid [-G/2, (G-1)/2] (SII:1261-1267, FIPK:404-410). edge_mode 1 ("strict") drops the   */
-/* sample instead when its full footprint does not fit.                                        */
-/* Returns 0 when the sample is dropped.                                                       */
+/* Footprint of one sample along one axis. The grid position is quantised to 2^-24 cells,     */
+/* Q = floor(p 2^24), pq = Q 2^-24 (the binning contract of the B200 path); the footprint is    */
+/* [ceil(pq - W/2), floor(pq + W/2)] (SII:1261-1267, FIPK:404-410) clipped to the grid          */
+/* [-G/2, (G-1)/2]. edge_mode 1 ("strict") drops the sample instead when its footprint leaves  */
+/* the grid. Returns 0 when the sample is dropped; *pq receives the quantised position.       */
 /* ------------------------------------------------------------------------------------------ */
-static int orc_footprint(double p, int W, long G, int edge_mode, long* lo, long* hi) {
+static int orc_footprint(double p, int W, long G, int edge_mode, long* lo, long* hi, double* pq) {
     const long gmin = -(G / 2), gmax = (G - 1) / 2;
-    const double half = 0.5 * (double)W;
-    long a = (long)ceil(p - half), b = (long)floor(p + half);
+    if (!(fabs(p) < 1e15)) return 0;
+    const long long Q = (long long)floor(p * 16777216.0);
+    const long long cell = Q >> 24, frac = Q & 0xFFFFFFLL;
+    const long hw = W / 2;
+    long a = (long)(frac ? cell - (hw - 1) : cell - hw), b = (long)(cell + hw);
     if (edge_mode == 1 && (a < gmin || b > gmax)) return 0;
     if (a < gmin) a = gmin;
     if (b > gmax) b = gmax;
     if (a > b) return 0;
     *lo = a;
     *hi = b;
+    *pq = (double)Q / 16777216.0;
     return 1;
 }
 
@@ -250,27 +255,36 @@ static void orc_slab(double r3, int nslab, double r3_min, double slab_width, dou
 
 /* ------------------------------------------------------------------------------------------ */
 /* Tile binning keys. For every sample: the grid position p = r * scale (FP64, scale =        */
-/* cell_size * G), its clipped footprint origin (lo1, lo2), and the key                         */
+/* cell_size * G, or the reference's FP32 rounding), its clipped footprint origin (lo1, lo2),  */
+/* and the key                                                                                  */
 /*   key = (slab * ntile + (lo1 + G/2) / T) * ntile + (lo2 + G/2) / T,  ntile = ceil(G / T)   */
-/* or -1 when the sample touches no cell. This is the binning contract of the B200 path        */
-/* (bit-exact); the reference grids unsorted (SII:1218-1293).                                  */
+/* or -1 when the sample touches no cell. xq/yq (optional) receive the record coordinates of   */
+/* the B200 path: Q - (tile origin) * 2^24 with Q = floor(p 2^24). This is the binning         */
+/* contract of the B200 path (bit-exact); the reference grids unsorted (SII:1218-1293).         */
 /* ------------------------------------------------------------------------------------------ */
 void orc_tile_keys(long n, const double* r, double scale, int coord_mode, long G, int W, int T,
                    int edge_mode, int nslab, double r3_min, double slab_width, double inv_half,
-                   int64_t* keys) {
+                   int64_t* keys, int32_t* xq, int32_t* yq, float* sarg) {
     const long ntile = (G + T - 1) / T;
+    const long gmin = -(G / 2);
     for (long k = 0; k < n; ++k) {
         const double p1 = orc_pos(r[k * 3 + 0], scale, coord_mode);
         const double p2 = orc_pos(r[k * 3 + 1], scale, coord_mode);
         long a1, b1, a2, b2;
-        if (!orc_footprint(p1, W, G, edge_mode, &a1, &b1) || !orc_footprint(p2, W, G, edge_mode, &a2, &b2)) {
+        double q1, q2;
+        if (!orc_footprint(p1, W, G, edge_mode, &a1, &b1, &q1) ||
+            !orc_footprint(p2, W, G, edge_mode, &a2, &b2, &q2)) {
             keys[k] = -1;
             continue;
         }
         int slab;
         double s;
         orc_slab(r[k * 3 + 2], nslab, r3_min, slab_width, inv_half, &slab, &s);
-        keys[k] = ((int64_t)slab * ntile + (a1 + G / 2) / T) * ntile + (a2 + G / 2) / T;
+        const long t1 = (a1 - gmin) / T, t2 = (a2 - gmin) / T;
+        keys[k] = ((int64_t)slab * ntile + t1) * ntile + t2;
+        if (xq) xq[k] = (int32_t)((long long)floor(p1 * 16777216.0) - (gmin + t1 * T) * 16777216LL);
+        if (yq) yq[k] = (int32_t)((long long)floor(p2 * 16777216.0) - (gmin + t2 * T) * 16777216LL);
+        if (sarg) sarg[k] = (float)s;
     }
 }
 
@@ -301,7 +315,9 @@ void orc_grid(long n, const double* r, const float* vr, const float* vi, double 
             const double p1 = orc_pos(r[k * 3 + 0], scale, coord_mode);
             const double p2 = orc_pos(r[k * 3 + 1], scale, coord_mode);
             long a1, b1, a2, b2;
-            if (!orc_footprint(p1, W, G, edge_mode, &a1, &b1) || !orc_footprint(p2, W, G, edge_mode, &a2, &b2))
+            double q1, q2;
+            if (!orc_footprint(p1, W, G, edge_mode, &a1, &b1, &q1) ||
+                !orc_footprint(p2, W, G, edge_mode, &a2, &b2, &q2))
                 continue;
             if (b1 < row_lo || a1 > row_hi) continue;
             int slab;
@@ -310,8 +326,8 @@ void orc_grid(long n, const double* r, const float* vr, const float* vi, double 
             cheb[0] = 1.0;
             if (K > 1) cheb[1] = s;
             for (int t = 2; t < K; ++t) cheb[t] = 2.0 * s * cheb[t - 1] - cheb[t - 2];
-            for (long g = a1; g <= b1; ++g) w1[g - a1] = orc_es(beta, ((double)g - p1) * half_w_inv);
-            for (long g = a2; g <= b2; ++g) w2[g - a2] = orc_es(beta, ((double)g - p2) * half_w_inv);
+            for (long g = a1; g <= b1; ++g) w1[g - a1] = orc_es(beta, ((double)g - q1) * half_w_inv);
+            for (long g = a2; g <= b2; ++g) w2[g - a2] = orc_es(beta, ((double)g - q2) * half_w_inv);
             const double vre = (double)vr[k] * inv_det, vim = (double)vi[k] * inv_det;
             for (long g1 = a1; g1 <= b1; ++g1) {
                 if (g1 < row_lo || g1 > row_hi) continue;

@@ -1,0 +1,259 @@
+// Tile binning of visibility samples: a counting sort of samples by (w-slab, grid tile).
+//
+// The reference grids every sample straight into global memory with float atomics
+// (SVDIntegratedImager.cu:1218-1293, 64 * K * 2 atomics per sample). Here samples are first
+// binned by the tile that holds the origin of their ES footprint, so that each tile is gridded in
+// shared memory by one CTA. The binning contract is bit-exact and shared with the CPU oracle:
+//
+//   p      = r * (cell_size * G)                FP64 (or the reference's FP32 rounding)
+//   Q      = floor(p * 2^24)                    position quantised to 2^-24 cells
+//   cell   = Q >> 24, frac = Q & (2^24 - 1)
+//   lo     = frac ? cell - (W/2 - 1) : cell - W/2   (= ceil(p - W/2)),  hi = cell + W/2
+//   clip   lo, hi to [-G/2, (G-1)/2] (SVDIntegratedImager.cu:1261-1267); drop if lo > hi
+//          (strict mode: drop if the footprint leaves the grid)
+//   tile   = (lo + G/2) / T  per axis;  slab = clamp(floor((r3 - r3_min) / width), 0, nslab-1)
+//   key    = (slab * ntile + tile1) * ntile + tile2
+#include "svdi_internal.cuh"
+
+namespace svdi {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kPerThread = 8;                       // samples per thread per scatter chunk
+constexpr int kChunk = kThreads * kPerThread;       // samples per scatter block
+constexpr int kSmemKeyLimit = 24576;                // keys aggregated in shared memory
+
+struct KeyRec {
+    int key;     // -1: dropped
+    int xq, yq;
+    float s;
+};
+
+__device__ inline bool quantise_axis(double p, const GridGeom& g, int& tile, int& qrel) {
+    if (!(fabs(p) < 1e15)) return false;
+    const long long Q = (long long)floor(p * 16777216.0);
+    const long long cell = Q >> 24;
+    const long long frac = Q & 0xFFFFFFLL;
+    const long long hw = g.W / 2;
+    long long lo = frac ? cell - (hw - 1) : cell - hw;
+    long long hi = cell + hw;
+    if (g.edge_mode == SVDI_EDGE_STRICT) {
+        if (lo < g.gmin || hi > g.gmax) return false;
+    } else {
+        if (lo < g.gmin) lo = g.gmin;
+        if (hi > g.gmax) hi = g.gmax;
+        if (lo > hi) return false;
+    }
+    tile = (int)((lo - g.gmin) / g.T);
+    const long long origin = g.gmin + (long long)tile * g.T;
+    qrel = (int)(Q - origin * 16777216LL);
+    return true;
+}
+
+__device__ inline double grid_pos(double r, const GridGeom& g) {
+    if (g.coord_mode == SVDI_COORD_REF32) return (double)__fmul_rn((float)r, g.scale32);
+    return __dmul_rn(r, g.scale);
+}
+
+__device__ inline void sample_coords(const SampleSource& src, long long idx, double& r1, double& r2,
+                                     double& r3) {
+    if (src.bin) {
+        r1 = (double)src.bin[idx * 3 + 0];
+        r2 = (double)src.bin[idx * 3 + 1];
+        r3 = (double)src.bin[idx * 3 + 2];
+    } else {
+        const long long row = idx % src.R, c = idx / src.R;
+        const double sc = src.s[c];
+        r1 = __dmul_rn(sc, src.q[row * 3 + 0]);
+        r2 = __dmul_rn(sc, src.q[row * 3 + 1]);
+        r3 = __dmul_rn(sc, src.q[row * 3 + 2]);
+    }
+}
+
+__device__ inline KeyRec sample_key(const SampleSource& src, long long idx, const GridGeom& g,
+                                    const SlabParams& sp) {
+    KeyRec k;
+    k.key = -1;
+    double r1, r2, r3;
+    sample_coords(src, idx, r1, r2, r3);
+    int t1, t2;
+    if (!quantise_axis(grid_pos(r1, g), g, t1, k.xq) || !quantise_axis(grid_pos(r2, g), g, t2, k.yq))
+        return k;
+    int j = 0;
+    double sv = 0.0;
+    if (sp.nslab > 1 || sp.K > 1) {
+        double jf = floor(__ddiv_rn(__dsub_rn(r3, sp.r3_min), sp.slab_width));
+        if (!(jf >= 0.0)) jf = 0.0;  // also NaN
+        if (jf > (double)(sp.nslab - 1)) jf = (double)(sp.nslab - 1);
+        j = (int)jf;
+        const double centre = __dadd_rn(sp.r3_min, __dmul_rn((double)j + 0.5, sp.slab_width));
+        sv = __dmul_rn(__dsub_rn(r3, centre), sp.inv_half);
+        sv = fmin(1.0, fmax(-1.0, sv));
+    }
+    k.s = (float)sv;
+    k.key = (j * g.ntile + t1) * g.ntile + t2;
+    return k;
+}
+
+// Per-block shared-memory histogram (warp-aggregated), flushed once per block.
+__global__ void __launch_bounds__(kThreads) k_histogram(SampleSource src, GridGeom g, SlabParams sp,
+                                                       unsigned int* __restrict__ counts, int n_keys,
+                                                       unsigned long long* __restrict__ dropped) {
+    extern __shared__ unsigned int sh[];
+    const bool use_smem = n_keys <= kSmemKeyLimit;
+    if (use_smem) {
+        for (int k = threadIdx.x; k < n_keys; k += kThreads) sh[k] = 0;
+        __syncthreads();
+    }
+    unsigned int ndrop = 0;
+    const int lane = threadIdx.x & 31;
+    const long long n = src.n;
+    const long long stride = (long long)gridDim.x * kThreads;
+    const long long n_round = ((n + stride - 1) / stride) * stride;
+    for (long long idx = blockIdx.x * (long long)kThreads + threadIdx.x; idx < n_round; idx += stride) {
+        int key = -2;
+        if (idx < n) {
+            key = sample_key(src, idx, g, sp).key;
+            if (key < 0) ++ndrop;
+        }
+        const unsigned int peers = __match_any_sync(0xffffffffu, key);
+        const int leader = __ffs(peers) - 1;
+        if (key >= 0 && lane == leader) {
+            const unsigned int c = __popc(peers);
+            if (use_smem) atomicAdd(&sh[key], c);
+            else atomicAdd(&counts[key], c);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) ndrop += __shfl_xor_sync(0xffffffffu, ndrop, o);
+    if (lane == 0 && ndrop) atomicAdd(dropped, (unsigned long long)ndrop);
+    if (use_smem) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < n_keys; k += kThreads)
+            if (sh[k]) atomicAdd(&counts[k], sh[k]);
+    }
+}
+
+// Exclusive scan of the key counts (one block): offsets[0..n_keys], cursor = offsets.
+__global__ void __launch_bounds__(1024) k_scan(const unsigned int* __restrict__ counts, int n_keys,
+                                              unsigned int* __restrict__ offsets,
+                                              unsigned int* __restrict__ cursor) {
+    __shared__ unsigned int part[1024];
+    const int t = threadIdx.x;
+    const int per = (n_keys + 1023) / 1024;
+    const int b = t * per, e = min(n_keys, b + per);
+    unsigned int s = 0;
+    for (int k = b; k < e; ++k) s += counts[k];
+    part[t] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        unsigned int v = (t >= off) ? part[t - off] : 0u;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    unsigned int run = part[t] - s;
+    for (int k = b; k < e; ++k) {
+        offsets[k] = run;
+        cursor[k] = run;
+        run += counts[k];
+    }
+    if (t == 1023) offsets[n_keys] = part[1023];
+}
+
+// Scatter: block-aggregated reservation of output ranges per key, then 16-byte record writes.
+__global__ void __launch_bounds__(kThreads) k_scatter(SampleSource src, GridGeom g, SlabParams sp,
+                                                     unsigned int* __restrict__ cursor, int n_keys,
+                                                     SampleRec* __restrict__ rec, float* __restrict__ rec_s) {
+    extern __shared__ unsigned int sh[];  // [n_keys] counts, then [n_keys] bases
+    unsigned int* cnt = sh;
+    unsigned int* base = sh + n_keys;
+    const bool use_smem = n_keys <= kSmemKeyLimit / 2;
+    const int lane = threadIdx.x & 31;
+    const long long n = src.n;
+    for (long long c0 = (long long)blockIdx.x * kChunk; c0 < n; c0 += (long long)gridDim.x * kChunk) {
+        KeyRec kr[kPerThread];
+        unsigned int rank[kPerThread];
+        if (use_smem) {
+            for (int k = threadIdx.x; k < n_keys; k += kThreads) cnt[k] = 0;
+            __syncthreads();
+        }
+#pragma unroll
+        for (int i = 0; i < kPerThread; ++i) {
+            const long long idx = c0 + i * kThreads + threadIdx.x;
+            kr[i].key = -2;
+            if (idx < n) kr[i] = sample_key(src, idx, g, sp);
+            const int key = kr[i].key;
+            const unsigned int peers = __match_any_sync(0xffffffffu, key);
+            const int leader = __ffs(peers) - 1;
+            const unsigned int before = __popc(peers & ((1u << lane) - 1u));
+            unsigned int b0 = 0;
+            if (key >= 0 && lane == leader)
+                b0 = use_smem ? atomicAdd(&cnt[key], __popc(peers)) : atomicAdd(&cursor[key], __popc(peers));
+            b0 = __shfl_sync(0xffffffffu, b0, leader);
+            rank[i] = b0 + before;
+        }
+        if (use_smem) {
+            __syncthreads();
+            for (int k = threadIdx.x; k < n_keys; k += kThreads) {
+                const unsigned int c = cnt[k];
+                base[k] = c ? atomicAdd(&cursor[k], c) : 0u;
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int i = 0; i < kPerThread; ++i) {
+            const long long idx = c0 + i * kThreads + threadIdx.x;
+            const int key = kr[i].key;
+            if (key < 0) continue;
+            const unsigned int pos = use_smem ? base[key] + rank[i] : rank[i];
+            SampleRec r;
+            r.xq = kr[i].xq;
+            r.yq = kr[i].yq;
+            r.vre = __fmul_rn(src.vr[idx], src.inv_det);
+            r.vim = __fmul_rn(src.vi[idx], src.inv_det);
+            rec[pos] = r;
+            if (rec_s) rec_s[pos] = kr[i].s;
+        }
+        if (use_smem) __syncthreads();
+    }
+}
+
+}  // namespace
+
+int launch_histogram(const SampleSource& src, const GridGeom& g, const SlabParams& sp,
+                     unsigned int* d_counts, int n_keys, unsigned long long* d_dropped,
+                     cudaStream_t st) {
+    const size_t smem = n_keys <= kSmemKeyLimit ? (size_t)n_keys * 4 : 0;
+    if (smem > 48 * 1024)
+        SVDI_CUDA(cudaFuncSetAttribute(k_histogram, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    long long blocks = (src.n + kThreads - 1) / kThreads;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks < 1) blocks = 1;
+    k_histogram<<<(int)blocks, kThreads, smem, st>>>(src, g, sp, d_counts, n_keys, d_dropped);
+    SVDI_LAUNCHED();
+    return SVDI_OK;
+}
+
+int launch_scan(const unsigned int* d_counts, int n_keys, unsigned int* d_offsets,
+                unsigned int* d_cursor, cudaStream_t st) {
+    k_scan<<<1, 1024, 0, st>>>(d_counts, n_keys, d_offsets, d_cursor);
+    SVDI_LAUNCHED();
+    return SVDI_OK;
+}
+
+int launch_scatter(const SampleSource& src, const GridGeom& g, const SlabParams& sp,
+                   unsigned int* d_cursor, int n_keys, SampleRec* d_rec, float* d_rec_s,
+                   cudaStream_t st) {
+    const size_t smem = n_keys <= kSmemKeyLimit / 2 ? (size_t)n_keys * 8 : 0;
+    if (smem > 48 * 1024)
+        SVDI_CUDA(cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    long long blocks = (src.n + kChunk - 1) / kChunk;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (blocks < 1) blocks = 1;
+    k_scatter<<<(int)blocks, kThreads, smem, st>>>(src, g, sp, d_cursor, n_keys, d_rec, d_rec_s);
+    SVDI_LAUNCHED();
+    return SVDI_OK;
+}
+
+}  // namespace svdi

@@ -1,0 +1,1001 @@
+// Imaging engine and the C ABI.
+//
+// Orchestration replaces FIpipeDevice (SVDIntegratedImager.cu:1498-1761) and FIpipe
+// (archive/FIPkernels.cu:679-911). Differences by design:
+//   - device buffers, cuFFT plans, grid-correction tables and ES polynomials are kept resident in
+//     an engine and grown on demand (the reference allocates, plans and frees on every call);
+//   - the Chebyshev/slab statistics need one small device-to-host read per snapshot (the
+//     reference needs two, plus a serial single-thread reduction kernel);
+//   - samples are binned by tile before gridding (binning.cu, gridder.cu).
+#include "svdi_internal.cuh"
+#include "math.cuh"
+
+#include <cufft.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+namespace svdi {
+
+static thread_local std::string g_last_error;
+static std::atomic<uint64_t> g_launches{0};
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+void note_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
+
+namespace {
+
+constexpr double kRefBeta = 15.3704324328;   // SVDIntegratedImager.cu:1235
+constexpr int kRefSupport = 8;               // SVDIntegratedImager.cu:1234
+constexpr int kChebMaxMoments = 32;          // SVDIntegratedImager.cu:35
+constexpr double kChebTargetError = 1.0e-2;  // SVDIntegratedImager.cu:36
+constexpr double kChebTargetAlpha = 10.0;    // SVDIntegratedImager.cu:37
+constexpr int kPartialCap = 4096;
+
+#define SVDI_CUFFT(call)                                                                  \
+    do {                                                                                  \
+        cufftResult r__ = (call);                                                         \
+        if (r__ != CUFFT_SUCCESS) {                                                       \
+            ::svdi::set_error(std::string("cuFFT error ") + std::to_string((int)r__) +    \
+                              " at " + __FILE__ + ":" + std::to_string(__LINE__));        \
+            return SVDI_ERR_CUFFT;                                                        \
+        }                                                                                 \
+    } while (0)
+
+// Grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    int ensure(size_t bytes) {
+        if (bytes <= cap) return SVDI_OK;
+        if (p) {
+            cudaFree(p);
+            p = nullptr;
+            cap = 0;
+        }
+        const size_t want = std::max<size_t>(bytes, 256);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            set_error(std::string("device allocation of ") + std::to_string(want) + " bytes failed: " +
+                      cudaGetErrorString(e));
+            return SVDI_ERR_OUT_OF_MEMORY;
+        }
+        cap = want;
+        return SVDI_OK;
+    }
+    template <typename T>
+    T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+long long next_nice_even(long long n) {
+    for (long long m = std::max<long long>(2, n + (n & 1));; m += 2) {
+        long long r = m;
+        for (long long f : {2, 3, 5, 7})
+            while (r % f == 0) r /= f;
+        if (r == 1) return m;
+    }
+}
+
+}  // namespace
+
+}  // namespace svdi
+
+struct svdi_engine {
+    svdi_options opt;
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    bool own_stream = true;
+    std::mutex mu;
+    // staging for host inputs
+    svdi::DevBuf in_uvw, in_freq, in_v0r, in_v0i, in_v3r, in_v3i, in_f0, in_f3, in_w0, in_w3;
+    svdi::DevBuf in_bin, in_vin;
+    // intermediates
+    svdi::DevBuf vr, vi, q, s, vin64, vin32, stats, partial, counts, offsets, cursor, dropped, rec,
+        rec_s, planes, corr, image, cheb_err, bin_out, grid_keep;
+    size_t sz_vr = 0, sz_q = 0, sz_s = 0, sz_off = 0, sz_rec = 0, sz_rec_s = 0, sz_grid = 0, sz_mom = 0;
+    const float* cur_vr = nullptr;
+    const float* cur_vi = nullptr;
+    const double* cur_q = nullptr;
+    const double* cur_s = nullptr;
+    double* h_stats = nullptr;  // pinned
+    std::map<std::pair<long long, int>, cufftHandle> plans;
+    std::map<std::tuple<long long, long long, int, double>, std::vector<float>> corr_cache;
+    std::tuple<long long, long long, int, double> corr_key{-1, -1, -1, 0.0};
+    std::map<std::tuple<double, int, int>, std::vector<double>> cheb_cache;
+    svdi::EsPoly poly{};
+    int poly_W = -1;
+    double poly_beta = 0.0;
+    svdi_stats last{};
+    cudaEvent_t ev[8] = {};
+
+    ~svdi_engine() {
+        if (device >= 0) cudaSetDevice(device);
+        for (auto& kv : plans) cufftDestroy(kv.second);
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        if (h_stats) cudaFreeHost(h_stats);
+        if (stream && own_stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace svdi {
+namespace {
+
+int engine_init(svdi_engine* e, const svdi_options* opt) {
+    e->opt = *opt;
+    e->device = opt->device;
+    SVDI_CUDA(cudaSetDevice(e->device));
+    SVDI_CUDA(cudaDeviceGetAttribute(&e->sm_count, cudaDevAttrMultiProcessorCount, e->device));
+    SVDI_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    SVDI_CUDA(cudaMallocHost(&e->h_stats, ST_COUNT * sizeof(double)));
+    for (auto& ev : e->ev) SVDI_CUDA(cudaEventCreate(&ev));
+    return SVDI_OK;
+}
+
+template <typename T>
+int upload(DevBuf& b, const T* host, size_t n, cudaStream_t st) {
+    SVDI_TRY(b.ensure(n * sizeof(T)));
+    if (n) SVDI_CUDA(cudaMemcpyAsync(b.p, host, n * sizeof(T), cudaMemcpyHostToDevice, st));
+    return SVDI_OK;
+}
+
+double read_target_alpha(const svdi_options& o) {
+    if (o.target_alpha > 0) return o.target_alpha;
+    if (const char* env = std::getenv("SVD_CHEB_TARGET_ALPHA")) {  // SVDIntegratedImager.cu:963-971
+        const double v = std::atof(env);
+        if (v > 0) return v;
+    }
+    return kChebTargetAlpha;
+}
+
+// Sampled Jacobi-Anger truncation errors for K = 1..32 at alpha_max (device FP64, cached).
+int cheb_errors(svdi_engine* e, double amax, int na, int ns, std::vector<double>& out) {
+    auto key = std::make_tuple(amax, na, ns);
+    auto it = e->cheb_cache.find(key);
+    if (it != e->cheb_cache.end()) {
+        out = it->second;
+        return SVDI_OK;
+    }
+    SVDI_TRY(e->cheb_err.ensure(kChebMaxMoments * sizeof(unsigned long long)));
+    SVDI_TRY(launch_cheb_errors(amax, na, ns, kChebMaxMoments, e->cheb_err.as<unsigned long long>(),
+                                e->stream));
+    unsigned long long h[kChebMaxMoments];
+    SVDI_CUDA(cudaMemcpyAsync(h, e->cheb_err.p, sizeof(h), cudaMemcpyDeviceToHost, e->stream));
+    SVDI_CUDA(cudaStreamSynchronize(e->stream));
+    out.resize(kChebMaxMoments);
+    for (int k = 0; k < kChebMaxMoments; ++k) {
+        double d;
+        memcpy(&d, &h[k], sizeof(d));
+        out[k] = d;
+    }
+    if (e->cheb_cache.size() > 4096) e->cheb_cache.clear();
+    e->cheb_cache[key] = out;
+    return SVDI_OK;
+}
+
+// Upper bound of the Jacobi-Anger truncation error on |s| <= 1 when K terms are kept:
+// 2 sum_{n >= K} |J_n(a)| (|T_n| <= 1).
+double truncation_bound(double a, int K) {
+    double j[200];
+    const int nmax = std::min(199, K + 60 + (int)std::fabs(a));
+    bessel_jn(a, nmax, j);
+    double s = 0.0;
+    for (int n = K; n <= nmax; ++n) s += std::fabs(j[n]);
+    return 2.0 * s;
+}
+
+int k_for_target(double a, double target) {
+    for (int K = 1; K <= kMaxTerms; ++K)
+        if (truncation_bound(a, K) <= target) return K;
+    return -1;
+}
+
+// Slab / Chebyshev configuration from the device statistics.
+int choose_slabs(svdi_engine* e, bool archive, double r3min, double r3max, double mt3, SlabParams& sp,
+                 double& alpha_max, double& slab_alpha) {
+    const svdi_options& o = e->opt;
+    const double half_range = std::max(0.5 * (r3max - r3min), 1.0e-6);
+    alpha_max = 2.0 * kPi * mt3 * half_range;
+    if (archive) {  // archive/FIPkernels.cu:327-366: one slab centred on the range
+        const double centre = 0.5 * (r3max + r3min);
+        sp.nslab = 1;
+        sp.r3_min = centre - half_range;
+        sp.slab_width = 2.0 * half_range;
+        sp.slab_half = half_range;
+        sp.inv_half = 1.0 / half_range;
+        slab_alpha = alpha_max;
+    } else {  // SVDIntegratedImager.cu:973-991
+        const double r3_range = std::max(r3max - r3min, 2.0e-6);
+        int nslab;
+        if (o.k_rule == SVDI_KRULE_TARGET && o.target_alpha <= 0) {
+            // minimise the number of moment planes nslab * K(alpha_slab) at the error target
+            int best_n = 1, best_p = 1 << 30;
+            for (int n = 1; n <= 64; ++n) {
+                const double h = std::max(0.5 * r3_range / n, 1.0e-6);
+                const int K = k_for_target(2.0 * kPi * mt3 * h, o.target_error);
+                if (K < 0) continue;
+                if (n * K < best_p) {
+                    best_p = n * K;
+                    best_n = n;
+                }
+                if (K == 1) break;
+            }
+            nslab = best_n;
+        } else {
+            nslab = (int)std::ceil(std::max(alpha_max, 0.0) / read_target_alpha(o));
+            if (nslab < 1) nslab = 1;
+        }
+        sp.nslab = nslab;
+        sp.r3_min = r3min;
+        sp.slab_width = r3_range / nslab;
+        sp.slab_half = std::max(0.5 * sp.slab_width, 1.0e-6);
+        sp.inv_half = 1.0 / sp.slab_half;
+        slab_alpha = 2.0 * kPi * mt3 * sp.slab_half;
+    }
+    int K = kChebMaxMoments;
+    std::vector<double> err;
+    switch (o.k_rule) {
+        case SVDI_KRULE_BUCKET: {  // SVDIntegratedImager.cu:1577-1603
+            SVDI_TRY(cheb_errors(e, slab_alpha, 257, 1024, err));
+            for (int kb : {8, 16, 24, 32})
+                if (err[kb - 1] <= kChebTargetError) {
+                    K = kb;
+                    break;
+                }
+            break;
+        }
+        case SVDI_KRULE_MIN: {  // archive/FIPkernels.cu:287-366
+            SVDI_TRY(cheb_errors(e, slab_alpha, 513, 2048, err));
+            for (int k = 1; k <= kChebMaxMoments; ++k)
+                if (err[k - 1] <= kChebTargetError) {
+                    K = k;
+                    break;
+                }
+            break;
+        }
+        case SVDI_KRULE_TARGET: {
+            const int k = k_for_target(slab_alpha, o.target_error);
+            if (k < 0) {
+                set_error("no Chebyshev order <= 64 reaches the error target; increase the slab count");
+                return SVDI_ERR_UNSUPPORTED;
+            }
+            K = k;
+            break;
+        }
+        case SVDI_KRULE_FIXED:
+            K = o.fixed_k;
+            break;
+        default:
+            set_error("unknown k_rule");
+            return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    if (K < 1 || K > kMaxTerms) {
+        set_error("Chebyshev order out of range");
+        return SVDI_ERR_UNSUPPORTED;
+    }
+    sp.K = K;
+    return SVDI_OK;
+}
+
+int get_plan(svdi_engine* e, long long G, int batch, cufftHandle& plan) {
+    auto key = std::make_pair(G, batch);
+    auto it = e->plans.find(key);
+    if (it != e->plans.end()) {
+        plan = it->second;
+        return SVDI_OK;
+    }
+    int dims[2] = {(int)G, (int)G};
+    SVDI_CUFFT(cufftPlanMany(&plan, 2, dims, nullptr, 1, (int)(G * G), nullptr, 1, (int)(G * G), CUFFT_C2C,
+                             batch));
+    SVDI_CUFFT(cufftSetStream(plan, e->stream));
+    e->plans[key] = plan;
+    return SVDI_OK;
+}
+
+// 1 / Phi(i), i = 0..N/2: inverse of the ES kernel's Fourier transform at image offset i, computed
+// in FP64 by composite Gauss-Legendre quadrature (the reference tabulates the same integral with a
+// 28-point rule in FP32, SVDIntegratedImager.cu:867-882, 1204-1216).
+int ensure_corr(svdi_engine* e, long long N, long long G, int W, double beta) {
+    auto key = std::make_tuple(N, G, W, beta);
+    if (e->corr_key == key) return SVDI_OK;
+    auto it = e->corr_cache.find(key);
+    if (it == e->corr_cache.end()) {
+        static const double x16[8] = {0.0950125098376374, 0.2816035507792589, 0.4580167776572274,
+                                      0.6178762444026438, 0.7554044083550030, 0.8656312023878318,
+                                      0.9445750230732326, 0.9894009349916499};
+        static const double w16[8] = {0.1894506104550685, 0.1826034150449236, 0.1691565193950025,
+                                      0.1495959888165767, 0.1246289712555339, 0.0951585116824928,
+                                      0.0622535239386479, 0.0271524594117541};
+        auto psi = [&](double x) {
+            if (std::fabs(x) > 1.0) return 0.0;
+            return std::exp(-beta * x * x / (1.0 + std::sqrt((1.0 - x) * (1.0 + x))));
+        };
+        std::vector<float> c(N / 2 + 1);
+        const int panels = 64;
+        for (long long i = 0; i <= N / 2; ++i) {
+            const double f = kPi * (double)W * ((double)i / (double)G);
+            double acc = 0.0;
+            for (int p = 0; p < panels; ++p) {
+                const double a = (double)p / panels, b = (double)(p + 1) / panels;
+                const double mid = 0.5 * (a + b), hw = 0.5 * (b - a);
+                for (int j = 0; j < 8; ++j) {
+                    const double t1 = mid - hw * x16[j], t2 = mid + hw * x16[j];
+                    acc += w16[j] * hw * (psi(t1) * std::cos(f * t1) + psi(t2) * std::cos(f * t2));
+                }
+            }
+            c[i] = (float)(1.0 / ((double)W * acc));
+        }
+        if (e->corr_cache.size() > 64) e->corr_cache.clear();
+        it = e->corr_cache.emplace(key, std::move(c)).first;
+    }
+    SVDI_TRY(e->corr.ensure(it->second.size() * sizeof(float)));
+    SVDI_CUDA(cudaMemcpyAsync(e->corr.p, it->second.data(), it->second.size() * sizeof(float),
+                              cudaMemcpyHostToDevice, e->stream));
+    e->corr_key = key;
+    return SVDI_OK;
+}
+
+long long grid_size(long long N, double sigma) {
+    if (sigma == 1.5) return (3 * N + 1) / 2;  // ceil(1.5 N), SVDIntegratedImager.cu:1510
+    return next_nice_even((long long)std::ceil(sigma * (double)N - 1e-9));
+}
+
+size_t batch_slabs_for(svdi_engine* e, int nslab, int K, long long G) {
+    // SVDIntegratedImager.cu:1470-1496 (env SVDIMAGER_MAX_BATCH_SLABS or 25 % of free HBM)
+    if (e->opt.max_batch_slabs > 0) return std::min<size_t>(nslab, e->opt.max_batch_slabs);
+    if (const char* env = std::getenv("SVDIMAGER_MAX_BATCH_SLABS")) {
+        const long long v = std::atoll(env);
+        if (v > 0) return std::min<size_t>(nslab, (size_t)v);
+    }
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    const size_t per_slab = (size_t)K * (size_t)G * (size_t)G * sizeof(float2);
+    const size_t budget = (free_b + e->planes.cap) / 4;
+    return std::min<size_t>(nslab, std::max<size_t>(1, budget / per_slab));
+}
+
+// Imaging core: given vin64 and sample source on the device, produce the image in d_out.
+int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, float cell_f,
+               float* d_out) {
+    cudaStream_t st = e->stream;
+    const svdi_options& o = e->opt;
+    const double cell = (double)cell_f;
+    const long long n = src.n;
+    // statistics: max |t3|, then one small read
+    SVDI_TRY(launch_t3_stats(e->vin64.as<double>(), N, cell, e->partial.as<double>(), kPartialCap,
+                             e->stats.as<double>(), st));
+    SVDI_CUDA(cudaMemcpyAsync(e->h_stats, e->stats.p, ST_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st));
+    SVDI_CUDA(cudaMemcpyAsync(e->last.vin, e->vin64.p, 9 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    SVDI_CUDA(cudaStreamSynchronize(st));
+    const double r3min = e->h_stats[ST_R3_MIN], r3max = e->h_stats[ST_R3_MAX];
+    const double mt3 = e->h_stats[ST_MAX_T3];
+    const double* V = e->last.vin;
+    const double det = std::fabs(V[0] * V[4] - V[1] * V[3]);
+    if (!(det > 0.0) || !std::isfinite(det)) {
+        set_error("degenerate basis: |V00 V11 - V01 V10| is zero");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    src.inv_det = (float)(1.0 / det);
+
+    SlabParams sp{};
+    double alpha_max = 0, slab_alpha = 0;
+    SVDI_TRY(choose_slabs(e, archive, r3min, r3max, mt3, sp, alpha_max, slab_alpha));
+
+    GridGeom g{};
+    g.G = grid_size(N, o.sigma);
+    g.gmin = -(g.G / 2);
+    g.gmax = (g.G - 1) / 2;
+    g.W = o.support;
+    g.T = o.tile ? o.tile : (sp.K == 1 ? 64 : 32);
+    g.ntile = (int)((g.G + g.T - 1) / g.T);
+    g.edge_mode = o.edge_mode;
+    g.coord_mode = o.coord_mode;
+    g.scale = cell * (double)g.G;
+    g.scale32 = cell_f * (float)g.G;
+    const long long n_keys_ll = (long long)sp.nslab * g.ntile * g.ntile;
+    if (n_keys_ll > (1LL << 26)) {
+        set_error("too many tile keys");
+        return SVDI_ERR_UNSUPPORTED;
+    }
+    const int n_keys = (int)n_keys_ll;
+
+    if (e->poly_W != g.W || e->poly_beta != o.beta) {
+        build_es_poly(g.W, o.beta, &e->poly);
+        e->poly_W = g.W;
+        e->poly_beta = o.beta;
+    }
+
+    // binning
+    SVDI_CUDA(cudaEventRecord(e->ev[1], st));
+    SVDI_TRY(e->counts.ensure((size_t)n_keys * 4));
+    SVDI_TRY(e->offsets.ensure((size_t)(n_keys + 1) * 4));
+    SVDI_TRY(e->cursor.ensure((size_t)n_keys * 4));
+    SVDI_TRY(e->dropped.ensure(8));
+    SVDI_TRY(e->rec.ensure((size_t)std::max<long long>(n, 1) * sizeof(SampleRec)));
+    const bool need_s = sp.K > 1;
+    if (need_s) SVDI_TRY(e->rec_s.ensure((size_t)std::max<long long>(n, 1) * sizeof(float)));
+    SVDI_CUDA(cudaMemsetAsync(e->counts.p, 0, (size_t)n_keys * 4, st));
+    SVDI_CUDA(cudaMemsetAsync(e->dropped.p, 0, 8, st));
+    SVDI_TRY(launch_histogram(src, g, sp, e->counts.as<unsigned int>(), n_keys,
+                              e->dropped.as<unsigned long long>(), st));
+    SVDI_TRY(launch_scan(e->counts.as<unsigned int>(), n_keys, e->offsets.as<unsigned int>(),
+                         e->cursor.as<unsigned int>(), st));
+    SVDI_TRY(launch_scatter(src, g, sp, e->cursor.as<unsigned int>(), n_keys, e->rec.as<SampleRec>(),
+                            need_s ? e->rec_s.as<float>() : nullptr, st));
+    SVDI_CUDA(cudaEventRecord(e->ev[2], st));
+
+    // slab batches: grid -> FFT -> recombine
+    const size_t bslabs = batch_slabs_for(e, sp.nslab, sp.K, g.G);
+    const int planes_per_batch = (int)bslabs * sp.K;
+    const size_t plane_bytes = (size_t)g.G * g.G * sizeof(float2);
+    SVDI_TRY(e->planes.ensure(plane_bytes * planes_per_batch));
+    cufftHandle plan;
+    SVDI_TRY(get_plan(e, g.G, planes_per_batch, plan));
+    SVDI_TRY(ensure_corr(e, N, g.G, g.W, o.beta));
+    SVDI_CUDA(cudaMemsetAsync(d_out, 0, (size_t)N * N * sizeof(float), st));
+    float ms_grid = 0, ms_fft = 0, ms_img = 0;
+    for (int s0 = 0; s0 < sp.nslab; s0 += (int)bslabs) {
+        const int s1 = std::min(sp.nslab, s0 + (int)bslabs);
+        SlabParams bp = sp;
+        SVDI_CUDA(cudaEventRecord(e->ev[3], st));
+        SVDI_CUDA(cudaMemsetAsync(e->planes.p, 0, plane_bytes * planes_per_batch, st));
+        const int tiles2 = g.ntile * g.ntile;
+        SVDI_TRY(launch_grid_fp32(e->rec.as<SampleRec>(), need_s ? e->rec_s.as<float>() : nullptr,
+                                  e->offsets.as<unsigned int>(), n_keys, s0 * tiles2, s1 * tiles2, s0, g, sp,
+                                  e->poly, e->planes.as<float2>(), e->sm_count, st));
+        if (o.keep_grid && s0 == 0) {
+            SVDI_TRY(e->grid_keep.ensure(plane_bytes * planes_per_batch));
+            SVDI_CUDA(cudaMemcpyAsync(e->grid_keep.p, e->planes.p, plane_bytes * planes_per_batch,
+                                      cudaMemcpyDeviceToDevice, st));
+            e->sz_grid = plane_bytes * (size_t)(std::min(sp.nslab, (int)bslabs) * sp.K);
+        }
+        SVDI_CUDA(cudaEventRecord(e->ev[4], st));
+        SVDI_CUFFT(cufftExecC2C(plan, e->planes.as<cufftComplex>(), e->planes.as<cufftComplex>(), CUFFT_INVERSE));
+        SVDI_CUDA(cudaEventRecord(e->ev[5], st));
+        // recombine the slabs of this batch (moment plane index relative to the batch)
+        bp.nslab = s1 - s0;
+        bp.r3_min = sp.r3_min + (double)s0 * sp.slab_width;
+        SVDI_TRY(launch_recombine(e->planes.as<float2>(), g, N, cell, e->vin64.as<double>(), bp,
+                                  e->corr.as<float>(), 1.0 / (double)n, o.reprojection, o.presplat, d_out,
+                                  st));
+        SVDI_CUDA(cudaEventRecord(e->ev[6], st));
+        SVDI_CUDA(cudaEventSynchronize(e->ev[6]));
+        float a = 0, b = 0, c = 0;
+        cudaEventElapsedTime(&a, e->ev[3], e->ev[4]);
+        cudaEventElapsedTime(&b, e->ev[4], e->ev[5]);
+        cudaEventElapsedTime(&c, e->ev[5], e->ev[6]);
+        ms_grid += a;
+        ms_fft += b;
+        ms_img += c;
+    }
+    unsigned long long ndrop = 0;
+    SVDI_CUDA(cudaMemcpyAsync(&ndrop, e->dropped.p, 8, cudaMemcpyDeviceToHost, st));
+    SVDI_CUDA(cudaStreamSynchronize(st));
+
+    e->sz_off = (size_t)(n_keys + 1) * 4;
+    e->sz_rec = (size_t)(n - (long long)ndrop) * sizeof(SampleRec);
+    e->sz_rec_s = need_s ? (size_t)(n - (long long)ndrop) * 4 : 0;
+    e->sz_mom = plane_bytes * (size_t)planes_per_batch;
+    e->cur_vr = src.vr;
+    e->cur_vi = src.vi;
+    e->sz_vr = (size_t)n * 4;
+    e->cur_q = src.q;
+    e->cur_s = src.s;
+    svdi_stats& L = e->last;
+    L.tile = g.T;
+    L.num_keys = n_keys;
+    L.slab_r3_min = sp.r3_min;
+    L.slab_width = sp.slab_width;
+    L.slab_half = sp.slab_half;
+    L.num_samples = (size_t)n;
+    L.num_gridded = (size_t)(n - (long long)ndrop);
+    L.grid_size = (size_t)g.G;
+    L.num_slabs = sp.nslab;
+    L.num_terms = sp.K;
+    L.num_planes = sp.nslab * sp.K;
+    L.r3_min = r3min;
+    L.r3_max = r3max;
+    L.max_abs_t3 = mt3;
+    L.valid_pixels = (size_t)e->h_stats[ST_VALID_PIX];
+    L.alpha_max = alpha_max;
+    L.slab_alpha_max = slab_alpha;
+    float mb = 0;
+    cudaEventElapsedTime(&mb, e->ev[1], e->ev[2]);
+    L.ms_bin = mb;
+    L.ms_grid = ms_grid;
+    L.ms_fft = ms_fft;
+    L.ms_image = ms_img;
+    return SVDI_OK;
+}
+
+int check_ms(const svdi_host_ms* h) {
+    if (!h) {
+        set_error("null measurement-set descriptor");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    if (h->num_samples == 0 || h->num_rows == 0 || h->num_channels == 0) {
+        set_error("Measurement set is empty");  // SVDIntegratedImager.cu:640-642
+        return SVDI_ERR_EMPTY_INPUT;
+    }
+    if (h->num_samples != h->num_rows * h->num_channels) {
+        set_error("num_samples must equal num_rows * num_channels");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    if (h->num_samples >= (1ULL << 32) - 1) {
+        set_error("more than 2^32 - 2 samples per snapshot");
+        return SVDI_ERR_UNSUPPORTED;
+    }
+    if (!h->uvw || !h->frequencies_hz || !h->vis0_real || !h->vis0_imag || !h->vis3_real ||
+        !h->vis3_imag || !h->flag0 || !h->flag3 || !h->weight0 || !h->weight3) {
+        set_error("null array in measurement-set descriptor");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    return SVDI_OK;
+}
+
+int check_image_args(size_t N, float cell) {
+    if (N == 0 || N > 65536) {
+        set_error("Image_Size must be in 1..65536");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    if (!(cell > 0.0f) || !std::isfinite(cell)) {
+        set_error("Cell_Size must be greater than zero");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    return SVDI_OK;
+}
+
+int check_options(const svdi_options& o) {
+    if (o.support != 6 && o.support != 8 && o.support != 10 && o.support != 12) {
+        set_error("support must be 6, 8, 10 or 12");
+        return SVDI_ERR_UNSUPPORTED;
+    }
+    if (!(o.beta > 0) || !(o.sigma >= 1.0) || o.sigma > 4.0) {
+        set_error("beta must be > 0 and sigma in [1, 4]");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    if (o.tile != 0 && o.tile != 32 && o.tile != 64) {
+        set_error("tile must be 0, 32 or 64");
+        return SVDI_ERR_UNSUPPORTED;
+    }
+    if (o.gridder != SVDI_GRIDDER_FP32 && o.gridder != SVDI_GRIDDER_TC) {
+        set_error("unknown gridder");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    return SVDI_OK;
+}
+
+// Main path on device-resident raw snapshot arrays.
+int main_path_device(svdi_engine* e, const svdi_host_ms* d, size_t N, float cell, float* d_out) {
+    cudaStream_t st = e->stream;
+    const long long R = (long long)d->num_rows, C = (long long)d->num_channels;
+    const long long n = (long long)d->num_samples;
+    SVDI_CUDA(cudaEventRecord(e->ev[0], st));
+    SVDI_TRY(e->vr.ensure(n * 4));
+    SVDI_TRY(e->vi.ensure(n * 4));
+    SVDI_TRY(e->q.ensure(R * 24));
+    SVDI_TRY(e->s.ensure(C * 8));
+    SVDI_TRY(e->vin64.ensure(9 * 8));
+    SVDI_TRY(e->vin32.ensure(9 * 4));
+    SVDI_TRY(e->stats.ensure(ST_COUNT * 8));
+    SVDI_TRY(e->partial.ensure((size_t)kPartialCap * 9 * 8));
+    SVDI_TRY(launch_collapse(d->vis0_real, d->vis0_imag, d->vis3_real, d->vis3_imag, d->flag0, d->flag3,
+                             d->weight0, d->weight3, e->vr.as<float>(), e->vi.as<float>(), n, st));
+    SVDI_TRY(launch_preprocess(d->uvw, d->frequencies_hz, R, C, d->array_center_x, e->partial.as<double>(),
+                               kPartialCap, e->vin64.as<double>(), e->vin32.as<float>(), e->q.as<double>(),
+                               e->s.as<double>(), e->stats.as<double>(), st));
+    SampleSource src{};
+    src.q = e->q.as<double>();
+    src.s = e->s.as<double>();
+    src.R = R;
+    src.vr = e->vr.as<float>();
+    src.vi = e->vi.as<float>();
+    src.n = n;
+    e->sz_q = (size_t)R * 24;
+    e->sz_s = (size_t)C * 8;
+    SVDI_TRY(image_core(e, false, src, (long long)N, cell, d_out));
+    float mp = 0, mt = 0;
+    cudaEventElapsedTime(&mp, e->ev[0], e->ev[1]);
+    SVDI_CUDA(cudaEventRecord(e->ev[7], st));
+    SVDI_CUDA(cudaEventSynchronize(e->ev[7]));
+    cudaEventElapsedTime(&mt, e->ev[0], e->ev[7]);
+    e->last.ms_preprocess = mp;
+    e->last.ms_total = mt;
+    return SVDI_OK;
+}
+
+int check_archive_args(const float* Visreal, const float* Visimag, const float* Bin, const float* Vin,
+                       const float* dirty_image, size_t n, size_t N, float cell) {
+    if (!Visreal || !Visimag || !Bin || !Vin || !dirty_image) {
+        set_error("null pointer argument");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    if (n == 0) {
+        set_error("num_baselines must be greater than zero");
+        return SVDI_ERR_EMPTY_INPUT;
+    }
+    if (n >= (1ULL << 32) - 1) {
+        set_error("more than 2^32 - 2 samples per call");
+        return SVDI_ERR_UNSUPPORTED;
+    }
+    return check_image_args(N, cell);
+}
+
+int archive_path(svdi_engine* e, const float* Visreal, const float* Visimag, const float* Bin,
+                 const float* Vin, float* dirty_image, size_t n, size_t N, float cell) {
+    SVDI_TRY(check_archive_args(Visreal, Visimag, Bin, Vin, dirty_image, n, N, cell));
+    cudaStream_t st = e->stream;
+    SVDI_CUDA(cudaSetDevice(e->device));
+    SVDI_CUDA(cudaEventRecord(e->ev[0], st));
+    SVDI_TRY(upload(e->vr, Visreal, n, st));
+    SVDI_TRY(upload(e->vi, Visimag, n, st));
+    SVDI_TRY(upload(e->in_bin, Bin, n * 3, st));
+    SVDI_TRY(upload(e->vin32, Vin, 9, st));
+    SVDI_TRY(e->vin64.ensure(9 * 8));
+    SVDI_TRY(e->stats.ensure(ST_COUNT * 8));
+    SVDI_TRY(e->partial.ensure((size_t)kPartialCap * 9 * 8));
+    SVDI_TRY(e->image.ensure(N * N * 4));
+    SVDI_TRY(launch_vin_from_float(e->vin32.as<float>(), e->vin64.as<double>(), st));
+    SVDI_TRY(launch_bin_stats(e->in_bin.as<float>(), (long long)n, e->partial.as<double>(), kPartialCap,
+                              e->stats.as<double>(), st));
+    SampleSource src{};
+    src.bin = e->in_bin.as<float>();
+    src.vr = e->vr.as<float>();
+    src.vi = e->vi.as<float>();
+    src.n = (long long)n;
+    e->sz_q = 0;
+    e->sz_s = 0;
+    SVDI_TRY(image_core(e, true, src, (long long)N, cell, e->image.as<float>()));
+    SVDI_CUDA(cudaMemcpyAsync(dirty_image, e->image.p, N * N * 4, cudaMemcpyDeviceToHost, st));
+    SVDI_CUDA(cudaEventRecord(e->ev[7], st));
+    SVDI_CUDA(cudaStreamSynchronize(st));
+    float mt = 0;
+    cudaEventElapsedTime(&mt, e->ev[0], e->ev[7]);
+    e->last.ms_total = mt;
+    return SVDI_OK;
+}
+
+svdi_options archive_defaults() {
+    svdi_options o;
+    svdi_default_options(&o);
+    o.k_rule = SVDI_KRULE_MIN;
+    o.reprojection = SVDI_REPROJ_FIPK;
+    return o;
+}
+
+std::mutex g_default_mu;
+std::map<int, std::unique_ptr<svdi_engine>> g_default_engines;
+
+int default_engine(svdi_engine** out) {
+    int dev = 0;
+    SVDI_CUDA(cudaGetDevice(&dev));
+    auto it = g_default_engines.find(dev);
+    if (it == g_default_engines.end()) {
+        std::unique_ptr<svdi_engine> e(new svdi_engine());
+        svdi_options o = archive_defaults();
+        o.device = dev;
+        SVDI_TRY(engine_init(e.get(), &o));
+        it = g_default_engines.emplace(dev, std::move(e)).first;
+    }
+    *out = it->second.get();
+    return SVDI_OK;
+}
+
+}  // namespace
+}  // namespace svdi
+
+using namespace svdi;
+
+extern "C" {
+
+const char* svdi_last_error(void) { return g_last_error.c_str(); }
+
+uint64_t svdi_kernel_launch_count(void) { return g_launches.load(); }
+
+void svdi_default_options(svdi_options* opt) {
+    if (!opt) return;
+    memset(opt, 0, sizeof(*opt));
+    opt->device = 0;
+    opt->k_rule = SVDI_KRULE_BUCKET;
+    opt->fixed_k = 1;
+    opt->target_error = 1e-6;
+    opt->target_alpha = 0.0;
+    opt->edge_mode = SVDI_EDGE_CLIP;
+    opt->coord_mode = SVDI_COORD_FP64;
+    opt->reprojection = SVDI_REPROJ_SII;
+    opt->support = kRefSupport;
+    opt->beta = kRefBeta;
+    opt->sigma = 1.5;
+    opt->tile = 0;
+    opt->gridder = SVDI_GRIDDER_FP32;
+    opt->max_batch_slabs = 0;
+}
+
+int svdi_engine_create(const svdi_options* opt, svdi_engine** out) {
+    g_last_error.clear();
+    if (!out) {
+        set_error("null output handle");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    svdi_options o;
+    if (opt) o = *opt;
+    else svdi_default_options(&o);
+    SVDI_TRY(check_options(o));
+    std::unique_ptr<svdi_engine> e(new svdi_engine());
+    SVDI_TRY(engine_init(e.get(), &o));
+    *out = e.release();
+    return SVDI_OK;
+}
+
+void svdi_engine_destroy(svdi_engine* e) { delete e; }
+
+int svdi_engine_image_host(svdi_engine* e, const svdi_host_ms* h, size_t N, float cell, float* dirty_image) {
+    g_last_error.clear();
+    if (!e || !dirty_image) {
+        set_error("null argument");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    SVDI_TRY(check_ms(h));
+    SVDI_TRY(check_image_args(N, cell));
+    std::lock_guard<std::mutex> lk(e->mu);
+    SVDI_CUDA(cudaSetDevice(e->device));
+    cudaStream_t st = e->stream;
+    const size_t n = h->num_samples, R = h->num_rows, C = h->num_channels;
+    SVDI_TRY(upload(e->in_uvw, h->uvw, R * 3, st));
+    SVDI_TRY(upload(e->in_freq, h->frequencies_hz, C, st));
+    SVDI_TRY(upload(e->in_v0r, h->vis0_real, n, st));
+    SVDI_TRY(upload(e->in_v0i, h->vis0_imag, n, st));
+    SVDI_TRY(upload(e->in_v3r, h->vis3_real, n, st));
+    SVDI_TRY(upload(e->in_v3i, h->vis3_imag, n, st));
+    SVDI_TRY(upload(e->in_f0, h->flag0, n, st));
+    SVDI_TRY(upload(e->in_f3, h->flag3, n, st));
+    SVDI_TRY(upload(e->in_w0, h->weight0, n, st));
+    SVDI_TRY(upload(e->in_w3, h->weight3, n, st));
+    svdi_host_ms d = *h;
+    d.uvw = e->in_uvw.as<float>();
+    d.frequencies_hz = e->in_freq.as<float>();
+    d.vis0_real = e->in_v0r.as<float>();
+    d.vis0_imag = e->in_v0i.as<float>();
+    d.vis3_real = e->in_v3r.as<float>();
+    d.vis3_imag = e->in_v3i.as<float>();
+    d.flag0 = e->in_f0.as<uint8_t>();
+    d.flag3 = e->in_f3.as<uint8_t>();
+    d.weight0 = e->in_w0.as<float>();
+    d.weight3 = e->in_w3.as<float>();
+    SVDI_TRY(e->image.ensure(N * N * 4));
+    SVDI_TRY(main_path_device(e, &d, N, cell, e->image.as<float>()));
+    SVDI_CUDA(cudaMemcpyAsync(dirty_image, e->image.p, N * N * 4, cudaMemcpyDeviceToHost, st));
+    SVDI_CUDA(cudaStreamSynchronize(st));
+    return SVDI_OK;
+}
+
+int svdi_engine_image_device(svdi_engine* e, const svdi_host_ms* d, size_t N, float cell, float* d_out,
+                             void* cuda_stream) {
+    g_last_error.clear();
+    if (!e || !d_out) {
+        set_error("null argument");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    SVDI_TRY(check_ms(d));
+    SVDI_TRY(check_image_args(N, cell));
+    std::lock_guard<std::mutex> lk(e->mu);
+    SVDI_CUDA(cudaSetDevice(e->device));
+    cudaStream_t user = (cudaStream_t)cuda_stream;
+    if (user) {  // order the engine stream after the caller's work
+        SVDI_CUDA(cudaEventRecord(e->ev[0], user));
+        SVDI_CUDA(cudaStreamWaitEvent(e->stream, e->ev[0], 0));
+    }
+    SVDI_TRY(main_path_device(e, d, N, cell, d_out));
+    if (user) {
+        SVDI_CUDA(cudaEventRecord(e->ev[7], e->stream));
+        SVDI_CUDA(cudaStreamWaitEvent(user, e->ev[7], 0));
+    }
+    return SVDI_OK;
+}
+
+int svdi_engine_fipipe_host(svdi_engine* e, const float* Visreal, const float* Visimag, const float* Bin,
+                            const float* Vin, float* dirty_image, size_t n, size_t N, float cell) {
+    g_last_error.clear();
+    if (!e) {
+        set_error("null engine");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    std::lock_guard<std::mutex> lk(e->mu);
+    return archive_path(e, Visreal, Visimag, Bin, Vin, dirty_image, n, N, cell);
+}
+
+int svdi_engine_last_stats(const svdi_engine* e, svdi_stats* out) {
+    if (!e || !out) {
+        set_error("null argument");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    *out = e->last;
+    return SVDI_OK;
+}
+
+static int buffer_of(const svdi_engine* e, int which, const void** p, size_t* bytes) {
+    switch (which) {
+        case SVDI_BUF_VIS_REAL: *p = e->cur_vr; *bytes = e->cur_vr ? e->sz_vr : 0; return SVDI_OK;
+        case SVDI_BUF_VIS_IMAG: *p = e->cur_vi; *bytes = e->cur_vi ? e->sz_vr : 0; return SVDI_OK;
+        case SVDI_BUF_Q: *p = e->cur_q; *bytes = e->cur_q ? e->sz_q : 0; return SVDI_OK;
+        case SVDI_BUF_S: *p = e->cur_s; *bytes = e->cur_s ? e->sz_s : 0; return SVDI_OK;
+        case SVDI_BUF_VIN: *p = e->vin64.p; *bytes = e->vin64.p ? 72 : 0; return SVDI_OK;
+        case SVDI_BUF_OFFSETS: *p = e->offsets.p; *bytes = e->sz_off; return SVDI_OK;
+        case SVDI_BUF_RECORDS: *p = e->rec.p; *bytes = e->sz_rec; return SVDI_OK;
+        case SVDI_BUF_RECORDS_S: *p = e->rec_s.p; *bytes = e->sz_rec_s; return SVDI_OK;
+        case SVDI_BUF_GRID: *p = e->grid_keep.p; *bytes = e->sz_grid; return SVDI_OK;
+        case SVDI_BUF_MOMENTS: *p = e->planes.p; *bytes = e->sz_mom; return SVDI_OK;
+        default:
+            set_error("unknown buffer id");
+            return SVDI_ERR_INVALID_ARGUMENT;
+    }
+}
+
+int svdi_engine_buffer_size(const svdi_engine* e, int which, size_t* bytes) {
+    if (!e || !bytes) {
+        set_error("null argument");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    const void* p = nullptr;
+    return buffer_of(e, which, &p, bytes);
+}
+
+int svdi_engine_copy_buffer(svdi_engine* e, int which, void* host_dst, size_t bytes) {
+    if (!e || !host_dst) {
+        set_error("null argument");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    std::lock_guard<std::mutex> lk(e->mu);
+    const void* p = nullptr;
+    size_t have = 0;
+    SVDI_TRY(buffer_of(e, which, &p, &have));
+    if (!p || bytes > have) {
+        set_error("buffer not available or request larger than the buffer");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    SVDI_CUDA(cudaSetDevice(e->device));
+    SVDI_CUDA(cudaMemcpyAsync(host_dst, p, bytes, cudaMemcpyDeviceToHost, e->stream));
+    SVDI_CUDA(cudaStreamSynchronize(e->stream));
+    return SVDI_OK;
+}
+
+int svdi_fipipe(const float* Visreal, const float* Visimag, const float* Bin, const float* Vin,
+                float* dirty_image, size_t num_baselines, size_t image_size, float cell_size) {
+    g_last_error.clear();
+    SVDI_TRY(check_archive_args(Visreal, Visimag, Bin, Vin, dirty_image, num_baselines, image_size, cell_size));
+    std::lock_guard<std::mutex> lk(g_default_mu);
+    svdi_engine* e = nullptr;
+    SVDI_TRY(default_engine(&e));
+    std::lock_guard<std::mutex> lk2(e->mu);
+    return archive_path(e, Visreal, Visimag, Bin, Vin, dirty_image, num_baselines, image_size, cell_size);
+}
+
+// ---- main-path mirror ----------------------------------------------------------------------
+struct svdi_pre_internal {
+    svdi_engine* engine;
+};
+
+int svdi_preprocess_measurement_set(const svdi_host_ms* h, svdi_device_buffers* dev, int want_bin) {
+    g_last_error.clear();
+    if (!dev) {
+        set_error("null device buffers");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    memset(dev, 0, sizeof(*dev));
+    SVDI_TRY(check_ms(h));
+    svdi_options o;
+    svdi_default_options(&o);
+    SVDI_CUDA(cudaGetDevice(&o.device));
+    svdi_engine* e = nullptr;
+    SVDI_TRY(svdi_engine_create(&o, &e));
+    std::unique_ptr<svdi_engine> guard(e);
+    cudaStream_t st = e->stream;
+    const size_t n = h->num_samples, R = h->num_rows, C = h->num_channels;
+    SVDI_TRY(upload(e->in_uvw, h->uvw, R * 3, st));
+    SVDI_TRY(upload(e->in_freq, h->frequencies_hz, C, st));
+    SVDI_TRY(upload(e->in_v0r, h->vis0_real, n, st));
+    SVDI_TRY(upload(e->in_v0i, h->vis0_imag, n, st));
+    SVDI_TRY(upload(e->in_v3r, h->vis3_real, n, st));
+    SVDI_TRY(upload(e->in_v3i, h->vis3_imag, n, st));
+    SVDI_TRY(upload(e->in_f0, h->flag0, n, st));
+    SVDI_TRY(upload(e->in_f3, h->flag3, n, st));
+    SVDI_TRY(upload(e->in_w0, h->weight0, n, st));
+    SVDI_TRY(upload(e->in_w3, h->weight3, n, st));
+    SVDI_TRY(e->vr.ensure(n * 4));
+    SVDI_TRY(e->vi.ensure(n * 4));
+    SVDI_TRY(e->q.ensure(R * 24));
+    SVDI_TRY(e->s.ensure(C * 8));
+    SVDI_TRY(e->vin64.ensure(9 * 8));
+    SVDI_TRY(e->vin32.ensure(9 * 4));
+    SVDI_TRY(e->stats.ensure(ST_COUNT * 8));
+    SVDI_TRY(e->partial.ensure((size_t)kPartialCap * 9 * 8));
+    SVDI_TRY(launch_collapse(e->in_v0r.as<float>(), e->in_v0i.as<float>(), e->in_v3r.as<float>(),
+                             e->in_v3i.as<float>(), e->in_f0.as<uint8_t>(), e->in_f3.as<uint8_t>(),
+                             e->in_w0.as<float>(), e->in_w3.as<float>(), e->vr.as<float>(), e->vi.as<float>(),
+                             (long long)n, st));
+    SVDI_TRY(launch_preprocess(e->in_uvw.as<float>(), e->in_freq.as<float>(), (long long)R, (long long)C,
+                               h->array_center_x, e->partial.as<double>(), kPartialCap, e->vin64.as<double>(),
+                               e->vin32.as<float>(), e->q.as<double>(), e->s.as<double>(), e->stats.as<double>(),
+                               st));
+    if (want_bin) {
+        SVDI_TRY(e->bin_out.ensure(n * 12));
+        SVDI_TRY(launch_expand_bin(e->q.as<double>(), e->s.as<double>(), (long long)R, (long long)C,
+                                   e->bin_out.as<float>(), st));
+    }
+    SVDI_CUDA(cudaStreamSynchronize(st));
+    // hand the buffers over to the descriptor; the engine keeps ownership of the rest
+    dev->d_vis_real = e->vr.as<float>();
+    dev->d_vis_imag = e->vi.as<float>();
+    dev->d_vin = e->vin32.as<float>();
+    dev->d_bin = want_bin ? e->bin_out.as<float>() : nullptr;
+    dev->num_samples = n;
+    dev->num_rows = R;
+    dev->num_channels = C;
+    dev->d_vin64 = e->vin64.as<double>();
+    dev->d_q = e->q.as<double>();
+    dev->d_s = e->s.as<double>();
+    dev->d_stats = e->stats.as<double>();
+    auto* in = new svdi_pre_internal{guard.release()};
+    dev->internal = in;
+    return SVDI_OK;
+}
+
+int svdi_fipipe_device(const svdi_device_buffers* dev, float* dirty_image, size_t N, float cell) {
+    g_last_error.clear();
+    if (!dev || !dev->internal || !dirty_image) {
+        set_error("device buffers not initialised by svdi_preprocess_measurement_set");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    SVDI_TRY(check_image_args(N, cell));
+    svdi_engine* e = static_cast<svdi_pre_internal*>(dev->internal)->engine;
+    std::lock_guard<std::mutex> lk(e->mu);
+    SVDI_CUDA(cudaSetDevice(e->device));
+    SVDI_TRY(e->image.ensure(N * N * 4));
+    SampleSource src{};
+    src.q = dev->d_q;
+    src.s = dev->d_s;
+    src.R = (long long)dev->num_rows;
+    src.vr = dev->d_vis_real;
+    src.vi = dev->d_vis_imag;
+    src.n = (long long)dev->num_samples;
+    SVDI_TRY(image_core(e, false, src, (long long)N, cell, e->image.as<float>()));
+    SVDI_CUDA(cudaMemcpyAsync(dirty_image, e->image.p, N * N * 4, cudaMemcpyDeviceToHost, e->stream));
+    SVDI_CUDA(cudaStreamSynchronize(e->stream));
+    return SVDI_OK;
+}
+
+void svdi_free_device_buffers(svdi_device_buffers* dev) {
+    if (!dev) return;
+    if (dev->internal) {
+        auto* in = static_cast<svdi_pre_internal*>(dev->internal);
+        delete in->engine;
+        delete in;
+    }
+    memset(dev, 0, sizeof(*dev));
+}
+
+}  // extern "C"
+
+// C++-linkage archive entry, exactly archive/pipe_interface.cpp:8.
+int FIpipe(float* Visreal, float* Visimag, float* Bin, float* Vin, float* dirty_image, size_t num_baselines,
+           size_t image_size, float cell_size) {
+    return svdi_fipipe(Visreal, Visimag, Bin, Vin, dirty_image, num_baselines, image_size, cell_size);
+}

@@ -1,0 +1,198 @@
+// Moment recombination, ES grid correction and reprojection with bilinear splat.
+//
+// One thread per rotated-frame pixel (SVDIntegratedImager.cu:1295-1463 fused_interpolation;
+// archive/FIPkernels.cu:463-677 accumulation, scaling, coordschange, p2p, finalinterp):
+//   t3 = -v33 + sgn(v33) sqrt(1 - (t1 + v13)^2 - (t2 + v23)^2)        (pixel skipped if < 0)
+//   R  = | Re sum_slab sum_n J_n(alpha) c_n i^n e^{i beta_slab} M_{slab,n}(x, y) | * (-1)^(x+y)
+//        / (Phi(|x|) Phi(|y|)) / N_s,  alpha = 2 pi t3 h, beta_slab = 2 pi t3 centre_slab
+// then a SIN deprojection of the pixel to the output grid and a bilinear splat.
+// Bessel coefficients and geometry in FP64 (the reference evaluates a FP32 power series,
+// SVDIntegratedImager.cu:901-920, whose cancellation grows with alpha).
+#include "svdi_internal.cuh"
+#include "math.cuh"
+
+namespace svdi {
+
+namespace {
+
+struct SplatTarget {
+    double LL, MM;
+    bool ok;
+};
+
+// SVDIntegratedImager.cu:1325-1379 (simplified SIN deprojection; keeps p1, p2 when h > r0)
+__device__ inline SplatTarget reproject_sii(long long idx, long long idy, long long N, double dc_rad,
+                                            const double* V) {
+    const double r0 = 180.0 / kPi;
+    const double dc = dc_rad / kPi * 180.0;
+    const double di2 = (double)N * 0.5;
+    const long long half = N / 2;
+    const double xi = V[6] / V[8], eta = V[7] / V[8];
+    const double idxf = (double)idx - di2, idyf = (double)idy - di2;
+    const double p1 = (-V[0] * idxf + V[3] * idyf) / fabs(V[8]) + di2;
+    const double p2 = (-V[1] * idxf + V[4] * idyf) / fabs(V[8]) + di2;
+    double x = -dc * (p1 - (di2 + 1.0));
+    double y = dc * (p2 - (di2 + 1.0));
+    const double h = hypot(x, y), hr0 = h / r0;
+    if (h != 0.0) {
+        x /= h;
+        y /= -h;
+    } else {
+        x = 0.0;
+        y = 1.0;
+    }
+    double oi0, oi1;
+    if (h <= r0) {
+        const double r = h;
+        const double z = (h < r0 * sqrt(0.5)) ? 1.0 - sqrt(1.0 - hr0 * hr0)
+                                              : hr0 * hr0 / (1.0 + sqrt(1.0 - hr0 * hr0));
+        const double w = xi * xi + eta * eta;
+        if (w == 0.0) {
+            x = r * x;
+            y = -r * y;
+        } else {
+            x = r * x + z * r0 * xi;
+            y = -r * y + z * r0 * eta;
+        }
+        oi0 = -x / dc + di2 + 1.0;
+        oi1 = y / dc + di2 + 1.0;
+    } else {
+        oi0 = p1;
+        oi1 = p2;
+    }
+    return {oi0 - (double)half, oi1 - (double)half, true};
+}
+
+// archive/FIPkernels.cu:552-624 (coordschange with the integer half size, then the
+// trigonometric SIN p2p of Calabretta & Greisen that drops r^2 > 1)
+__device__ inline SplatTarget reproject_fipk(long long idx, long long idy, long long N, double dc_rad,
+                                             const double* V) {
+    const long long half = N / 2;
+    const double dc = dc_rad / kPi * 180.0;
+    const double r0 = 180.0 / kPi;
+    const double xi = V[6] / V[8], eta = V[7] / V[8];
+    const double p1 = (-V[0] * (double)(idx - half) + V[3] * (double)(idy - half)) / fabs(V[8]) + (double)half;
+    const double p2 = (-V[1] * (double)(idx - half) + V[4] * (double)(idy - half)) / fabs(V[8]) + (double)half;
+    double x = -dc * (p1 - ((double)N / 2.0 + 1.0));
+    double y = dc * (p2 - ((double)N / 2.0 + 1.0));
+    const double x0 = x / r0, y0 = y / r0, r2 = x0 * x0 + y0 * y0;
+    const double phi = (r2 != 0.0) ? atan2(x0, -y0) : 0.0;
+    double theta;
+    if (r2 < 0.5) theta = acos(sqrt(r2));
+    else if (r2 <= 1.0) theta = asin(sqrt(1.0 - r2));
+    else return {0.0, 0.0, false};
+    double sx, cy;
+    sincos(phi, &sx, &cy);
+    const double t = kPi / 2.0 - fabs(theta);
+    double z, costhe;
+    if (t < 1.0e-5) {
+        z = theta > 0.0 ? t * t / 2.0 : 2.0 - t * t / 2.0;
+        costhe = t;
+    } else {
+        z = 1.0 - sin(theta);
+        costhe = cos(theta);
+    }
+    const double r = r0 * costhe;
+    const double w = xi * xi + eta * eta;
+    if (w == 0.0) {
+        x = r * sx;
+        y = -r * cy;
+    } else {
+        z *= r0;
+        x = r * sx + xi * z;
+        y = -r * cy + eta * z;
+    }
+    const double oi0 = -1.0 / dc * x + (double)N / 2.0 + 1.0;
+    const double oi1 = 1.0 / dc * y + (double)N / 2.0 + 1.0;
+    return {oi0 - (double)half, oi1 - (double)half, true};
+}
+
+template <int KMAX>
+__global__ void __launch_bounds__(256) k_recombine(const float2* __restrict__ moments, GridGeom g, long long N,
+                                                  double cell, const double* __restrict__ vin,
+                                                  SlabParams sp, const float* __restrict__ corr,
+                                                  double inv_n, int reprojection, int presplat,
+                                                  float* __restrict__ out) {
+    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long y = blockIdx.y * (long long)blockDim.y + threadIdx.y;
+    if (x >= N || y >= N) return;
+    double V[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) V[k] = vin[k];
+    const long long half = N / 2;
+    const long long xr = x - half, yr = y - half;
+    const double t1 = cell * (double)yr, t2 = cell * (double)xr;
+    const double ra = 1.0 - (t1 + V[2]) * (t1 + V[2]) - (t2 + V[5]) * (t2 + V[5]);
+    if (ra < 0.0) {
+        if (presplat) out[y * N + x] = __int_as_float(0x7fc00000);  // NaN
+        return;
+    }
+    const double t3 = -V[8] + (V[8] >= 0.0 ? 1.0 : -1.0) * sqrt(ra);
+
+    const int K = sp.K;
+    double jv[KMAX];
+    bessel_jn(2.0 * kPi * t3 * sp.slab_half, K - 1, jv);
+    const long long G = g.G, GG = G * G;
+    const long long gidx = GG / 2 + G / 2 + yr * G + xr;  // SVDIntegratedImager.cu:1397
+    double sum = 0.0;
+    for (int j = 0; j < sp.nslab; ++j) {
+        const double centre = sp.r3_min + ((double)j + 0.5) * sp.slab_width;
+        double sb, cb;
+        sincos(2.0 * kPi * t3 * centre, &sb, &cb);
+        const float2* mp = moments + (long long)j * K * GG + gidx;
+        for (int n = 0; n < K; ++n) {
+            const float2 m = mp[(long long)n * GG];
+            const double amp = (n == 0) ? jv[0] : 2.0 * jv[n];
+            double cr, ci;  // amp * i^n * e^{i beta}
+            switch (n & 3) {
+                case 0: cr = amp * cb; ci = amp * sb; break;
+                case 1: cr = -amp * sb; ci = amp * cb; break;
+                case 2: cr = -amp * cb; ci = -amp * sb; break;
+                default: cr = amp * sb; ci = -amp * cb; break;
+            }
+            sum += cr * (double)m.x - ci * (double)m.y;
+        }
+    }
+    if ((xr + yr) & 1) sum = -sum;
+    const long long ax = xr < 0 ? -xr : xr, ay = yr < 0 ? -yr : yr;
+    const double value = fabs(sum * (double)corr[ax] * (double)corr[ay]) * inv_n;
+    if (presplat) {  // slab batches add up (the reference also sums |partial| per batch)
+        out[y * N + x] += (float)value;
+        return;
+    }
+
+    const SplatTarget tg = reprojection == SVDI_REPROJ_FIPK ? reproject_fipk(x, y, N, cell, V)
+                                                            : reproject_sii(x, y, N, cell, V);
+    if (!tg.ok) return;
+    const double LL = tg.LL, MM = tg.MM;
+    if (!(fabs(LL) < (double)(half - 1) && fabs(MM) < (double)(half - 1))) return;
+    const double Lf = floor(LL), Mf = floor(MM), Lc = ceil(LL), Mc = ceil(MM);
+    float* d = out + half * N + half;
+    atomicAdd(&d[(long long)Mf * N + (long long)Lf], (float)((1 - LL + Lf) * (1 - MM + Mf) * value));
+    atomicAdd(&d[(long long)Mc * N + (long long)Lf], (float)((1 - LL + Lf) * (0 + MM - Mf) * value));
+    atomicAdd(&d[(long long)Mf * N + (long long)Lc], (float)((0 + LL - Lf) * (1 - MM + Mf) * value));
+    atomicAdd(&d[(long long)Mc * N + (long long)Lc], (float)((0 + LL - Lf) * (0 + MM - Mf) * value));
+}
+
+}  // namespace
+
+int launch_recombine(const float2* d_moments, const GridGeom& g, long long N, double cell,
+                     const double* d_vin64, const SlabParams& sp, const float* d_corr,
+                     double inv_n_total, int reprojection, int presplat, float* d_out,
+                     cudaStream_t st) {
+    const dim3 block(32, 8);
+    const dim3 grid((unsigned)((N + 31) / 32), (unsigned)((N + 7) / 8));
+    if (sp.K <= 1) k_recombine<1><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out);
+    else if (sp.K <= 8) k_recombine<8><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out);
+    else if (sp.K <= 16) k_recombine<16><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out);
+    else if (sp.K <= 32) k_recombine<32><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out);
+    else if (sp.K <= kMaxTerms) k_recombine<kMaxTerms><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out);
+    else {
+        set_error("recombine: too many Chebyshev terms");
+        return SVDI_ERR_UNSUPPORTED;
+    }
+    SVDI_LAUNCHED();
+    return SVDI_OK;
+}
+
+}  // namespace svdi

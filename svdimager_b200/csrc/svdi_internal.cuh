@@ -1,0 +1,150 @@
+// Internal declarations shared by the svdimager_b200 CUDA translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "../../include/svdimager_b200.h"
+
+namespace svdi {
+
+constexpr double kCLight = 299792458.0;  // SVDIntegratedImager.cu:382
+constexpr double kPi = 3.14159265358979323846;
+constexpr int kMaxTerms = 64;            // Chebyshev terms the kernels support
+constexpr int kMaxSupport = 16;          // ES support the kernels support
+constexpr int kPolyDeg = 11;             // degree of the piecewise ES polynomials
+constexpr int kQuantBits = 24;           // grid positions are quantised to 2^-24 cells
+
+// Record of one binned sample (16 bytes). xq/yq: quantised position relative to the tile origin,
+// (cell offset << 24) | frac24; vre/vim: visibility / |det(Vin[0:2,0:2])| as float bits.
+struct __align__(16) SampleRec {
+    int xq, yq;
+    float vre, vim;
+};
+
+// Device-resident scalar statistics (double slots, one D2H copy per snapshot).
+enum StatSlot {
+    ST_R3_MIN = 0, ST_R3_MAX, ST_MAX_T3, ST_VALID_PIX, ST_S_MIN, ST_S_MAX, ST_NUM_GRIDDED,
+    ST_NUM_DROPPED, ST_EIG0, ST_EIG1, ST_EIG2, ST_COUNT = 16
+};
+
+// Geometry of one imaging call (passed by value to kernels).
+struct GridGeom {
+    long long G;          // grid side
+    long long gmin, gmax; // first/last cell index relative to the centre: -G/2 .. (G-1)/2
+    int W;                // ES support (even)
+    int T;                // tile side
+    int ntile;            // ceil(G / T)
+    int edge_mode;
+    int coord_mode;
+    double scale;         // cell_size * G  (grid position = r * scale)
+    float scale32;        // float(cell_size * G) of the reference (coord_mode 1)
+};
+
+struct SlabParams {
+    int nslab;
+    int K;
+    double r3_min;
+    double slab_width;
+    double inv_half;      // 1 / slab half width
+    double slab_half;
+};
+
+// ES kernel as W polynomial pieces in the fractional position: piece i evaluates
+// psi((i - (W/2 - 1) - f) / (W/2)) for f in [0, 1).
+struct EsPoly {
+    float c[kMaxSupport][kPolyDeg + 1];
+    float edge;           // psi(+-1) = exp(-beta), weight of the extra cell when frac == 0
+    int W;
+};
+
+// ---- launch accounting -------------------------------------------------------------------
+void note_launch(int n = 1);
+
+// ---- status helpers ------------------------------------------------------------------------
+void set_error(const std::string& msg);
+
+#define SVDI_CUDA(call)                                                                       \
+    do {                                                                                      \
+        cudaError_t e__ = (call);                                                             \
+        if (e__ != cudaSuccess) {                                                             \
+            ::svdi::set_error(std::string("CUDA error ") + cudaGetErrorString(e__) + " at " + \
+                              __FILE__ + ":" + std::to_string(__LINE__));                     \
+            return SVDI_ERR_CUDA;                                                             \
+        }                                                                                     \
+    } while (0)
+
+#define SVDI_LAUNCHED()                                                                       \
+    do {                                                                                      \
+        ::svdi::note_launch();                                                                \
+        cudaError_t e__ = cudaGetLastError();                                                 \
+        if (e__ != cudaSuccess) {                                                             \
+            ::svdi::set_error(std::string("kernel launch failed: ") + cudaGetErrorString(e__) \
+                              + " at " + __FILE__ + ":" + std::to_string(__LINE__));          \
+            return SVDI_ERR_CUDA;                                                             \
+        }                                                                                     \
+    } while (0)
+
+#define SVDI_TRY(call)                  \
+    do {                                \
+        int s__ = (call);               \
+        if (s__ != SVDI_OK) return s__; \
+    } while (0)
+
+// ---- kernel launchers (stream-ordered, no synchronisation) ---------------------------------
+// preprocess.cu
+int launch_preprocess(const float* d_uvw, const float* d_freq, long long R, long long C,
+                      float array_center_x, double* d_partial, int partial_cap, double* d_vin64,
+                      float* d_vin32, double* d_q, double* d_s, double* d_stats, cudaStream_t st);
+int launch_collapse(const float* v0r, const float* v0i, const float* v3r, const float* v3i,
+                    const uint8_t* f0, const uint8_t* f3, const float* w0, const float* w3,
+                    float* outr, float* outi, long long n, cudaStream_t st);
+int launch_expand_bin(const double* d_q, const double* d_s, long long R, long long C, float* d_bin,
+                      cudaStream_t st);
+int launch_bin_stats(const float* d_bin, long long n, double* d_partial, int partial_cap,
+                     double* d_stats, cudaStream_t st);
+int launch_vin_from_float(const float* d_vin32, double* d_vin64, cudaStream_t st);
+int launch_t3_stats(const double* d_vin64, long long N, double cell, double* d_partial,
+                    int partial_cap, double* d_stats, cudaStream_t st);
+int launch_cheb_errors(double amax, int na, int ns, int kmax, unsigned long long* d_err,
+                       cudaStream_t st);
+
+// binning.cu
+struct SampleSource {
+    // separable (main path): r = s[chan] * q[row], idx = row + chan * R
+    const double* q;
+    const double* s;
+    long long R;
+    // explicit (archive path): r = bin[idx]
+    const float* bin;
+    // collapsed visibilities
+    const float* vr;
+    const float* vi;
+    long long n;
+    float inv_det;
+};
+int launch_histogram(const SampleSource& src, const GridGeom& g, const SlabParams& sp,
+                     unsigned int* d_counts, int n_keys, unsigned long long* d_dropped,
+                     cudaStream_t st);
+int launch_scan(const unsigned int* d_counts, int n_keys, unsigned int* d_offsets,
+                unsigned int* d_cursor, cudaStream_t st);
+int launch_scatter(const SampleSource& src, const GridGeom& g, const SlabParams& sp,
+                   unsigned int* d_cursor, int n_keys, SampleRec* d_rec, float* d_rec_s,
+                   cudaStream_t st);
+
+// gridder.cu
+int launch_grid_fp32(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d_offsets,
+                     int n_keys, int key_lo, int key_hi, int slab_lo, const GridGeom& g,
+                     const SlabParams& sp, const EsPoly& poly, float2* d_planes, int sm_count,
+                     cudaStream_t st);
+void build_es_poly(int W, double beta, EsPoly* out);
+
+// image.cu
+int launch_recombine(const float2* d_moments, const GridGeom& g, long long N, double cell,
+                     const double* d_vin64, const SlabParams& sp, const float* d_corr,
+                     double inv_n_total, int reprojection, int presplat, float* d_out,
+                     cudaStream_t st);
+
+}  // namespace svdi

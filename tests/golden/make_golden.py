@@ -1,0 +1,57 @@
+"""Generate golden outputs of the REFERENCE archive imager on a B200.
+
+The reference's archive/FIPkernels.cu is compiled unmodified for sm_100a by `make -C oracle ref`
+(oracle/_ref/libfipk_ref.so, needs the reference sources to build; the built library travels with
+the tree). This script runs its FIpipe on the small configuration's FITS-quartet inputs and writes
+
+    tests/golden/fipk_small.npz   image [256][256] float32, input sha256, K chosen by the oracle rule
+
+Usage (GPU):  python -m tests.golden.make_golden [out_dir]
+"""
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def quartet():
+    """Visreal, Visimag, Bin [N_s][3], Vin [3][3] (float32), N, cell of the small configuration:
+    the collapse and FP64 rotation of the synthetic snapshot, cast to float like the reference's
+    FITS inputs (archive/SVD_MFS.py writes them from the same quantities)."""
+    from oracle import oracle as O
+    from svdimager_b200 import synth
+    s = synth.make_snapshot("small")
+    vr, vi = O.collapse(s)
+    vin, q, sv, _ = O.preprocess64(s)
+    b = O.expand_coords(q, sv).astype(np.float32)
+    return vr, vi, b, vin.astype(np.float32), s.image_size, s.cell_size
+
+
+def digest(*arrays):
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def main(out_dir):
+    from oracle import oracle as O
+    visr, visi, b, v, N, cell = quartet()
+    img = O.run_reference_fipipe(visr, visi, b, v, N, cell)
+    img2 = O.run_reference_fipipe(visr, visi, b, v, N, cell)
+    sc = O.slab_config_fipk(b[:, 2], v.astype(np.float64), N, cell)
+    os.makedirs(out_dir, exist_ok=True)
+    path = os.path.join(out_dir, "fipk_small.npz")
+    np.savez_compressed(path, image=img, image_rerun=img2, input_sha256=digest(visr, visi, b, v),
+                        K=sc.K, N=N, cell=cell)
+    print("wrote", path, "K", sc.K, "rerun rel diff",
+          float(np.linalg.norm(img - img2) / np.linalg.norm(img)))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden"))

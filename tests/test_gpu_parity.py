@@ -1,0 +1,355 @@
+"""Parity of the B200 path with the oracle (CPU restatement of the reference), with the reference's
+own archive imager compiled for sm_100a, and with the FP64 direct DFT. Every call goes through the
+C ABI (svdimager_b200.api -> libsvdimager_b200.so).
+
+Tolerances: integer/byte work (flag collapse, tile binning) is bit-exact; images are compared by
+relative RMS, sqrt(sum (a-b)^2 / sum b^2), against 1e-5 (FP32 gridding and FFT)."""
+import math
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from svdimager_b200 import api, synth
+from tests.conftest import snapshot
+
+pytestmark = pytest.mark.gpu
+
+IMG_TOL = 1e-5
+
+
+def _scale(cell, G):
+    return float(np.float32(cell)) * G
+
+
+def _slab_config_from_stats(st):
+    return O.SlabConfig(st["slab_r3_min"], st["r3_max"], st["max_abs_t3"], st["alpha_max"],
+                        st["num_slabs"], st["slab_width"], st["slab_half"], 1.0 / st["slab_half"],
+                        st["slab_alpha_max"], st["num_terms"])
+
+
+@pytest.fixture(scope="module")
+def small_run(cuda_device, small_snapshot):
+    s = small_snapshot
+    e = api.Engine(keep_grid=1)
+    img = e.image(s)
+    return dict(engine=e, image=img, stats=e.stats(), snap=s)
+
+
+def test_collapse_bit_exact(small_run):
+    s, e = small_run["snap"], small_run["engine"]
+    ovr, ovi = O.collapse(s)
+    assert np.array_equal(e.buffer(api.BUF_VIS_REAL), ovr)
+    assert np.array_equal(e.buffer(api.BUF_VIS_IMAG), ovi)
+    both = (s.flag0 != 0) & (s.flag3 != 0)
+    assert both.any() and np.all(e.buffer(api.BUF_VIS_REAL)[both] == 0)
+
+
+def test_rotation_matches_oracle(small_run):
+    s, e = small_run["snap"], small_run["engine"]
+    vin, q, sv, _ = O.preprocess64(s)
+    assert np.array_equal(e.buffer(api.BUF_S), sv)
+    assert np.allclose(e.buffer(api.BUF_VIN).reshape(3, 3), vin, atol=1e-12)
+    assert np.allclose(e.buffer(api.BUF_Q).reshape(-1, 3), q, rtol=1e-12, atol=1e-9)
+
+
+def _check_binning(e, st, r, vr, vi, cell, coord_mode=0, edge_mode=0, W=8):
+    G, T = st["grid_size"], st["tile"]
+    sc = _slab_config_from_stats(st)
+    keys, xq, yq, sa = O.tile_keys(r, _scale(cell, G), G, W, T, edge_mode, sc, coord_mode, records=True)
+    n_keys = st["num_keys"]
+    off = e.buffer(api.BUF_OFFSETS).astype(np.int64)
+    kept = keys >= 0
+    assert st["num_gridded"] == int(kept.sum())
+    assert np.array_equal(np.diff(off), np.bincount(keys[kept], minlength=n_keys))
+    rec = e.buffer(api.BUF_RECORDS)
+    vin = np.array(st["vin"]).reshape(3, 3)
+    inv_det = np.float32(1.0 / abs(vin[0, 0] * vin[1, 1] - vin[0, 1] * vin[1, 0]))
+    orec = np.zeros(int(kept.sum()), rec.dtype)
+    order = np.argsort(keys[kept], kind="stable")
+    orec["xq"] = xq[kept][order]
+    orec["yq"] = yq[kept][order]
+    orec["vre"] = (vr[kept] * inv_det).astype(np.float32)[order]
+    orec["vim"] = (vi[kept] * inv_det).astype(np.float32)[order]
+    # records within one key may come in any order: compare per-key sorted
+    kk = np.repeat(np.arange(n_keys), np.diff(off))
+    a = np.lexsort((rec["vim"], rec["vre"], rec["yq"], rec["xq"], kk))
+    b = np.lexsort((orec["vim"], orec["vre"], orec["yq"], orec["xq"], kk))
+    assert np.array_equal(rec[a], orec[b])
+
+
+def test_tile_binning_bit_exact_main(small_run):
+    s, e, st = small_run["snap"], small_run["engine"], small_run["stats"]
+    r = O.expand_coords(e.buffer(api.BUF_Q).reshape(-1, 3), e.buffer(api.BUF_S))
+    _check_binning(e, st, r, e.buffer(api.BUF_VIS_REAL), e.buffer(api.BUF_VIS_IMAG), s.cell_size)
+
+
+def test_grid_planes_match_oracle(small_run):
+    s, e, st = small_run["snap"], small_run["engine"], small_run["stats"]
+    G = st["grid_size"]
+    r = O.expand_coords(e.buffer(api.BUF_Q).reshape(-1, 3), e.buffer(api.BUF_S))
+    vin = np.array(st["vin"]).reshape(3, 3)
+    inv_det = 1.0 / abs(vin[0, 0] * vin[1, 1] - vin[0, 1] * vin[1, 0])
+    sc = _slab_config_from_stats(st)
+    og = O.grid(r, e.buffer(api.BUF_VIS_REAL), e.buffer(api.BUF_VIS_IMAG), _scale(s.cell_size, G), G, sc,
+                inv_det)
+    grid = e.buffer(api.BUF_GRID).reshape(-1, G, G)
+    assert grid.shape == og.shape
+    for p in range(og.shape[0]):
+        num = np.linalg.norm(grid[p] - og[p])
+        den = np.linalg.norm(og[p])
+        if den > 0:
+            assert num / den < 2e-6, (p, num / den)
+
+
+def test_main_path_image_matches_oracle(small_run):
+    s = small_run["snap"]
+    oimg = O.image_sii(s)
+    assert small_run["stats"]["num_terms"] == oimg.sc.K == 8
+    assert O.rel_rms(small_run["image"], oimg.image) < IMG_TOL
+
+
+def test_main_path_presplat_and_dft_accuracy(cuda_device, small_snapshot):
+    """Rotated-frame image before reprojection against the oracle and against the FP64 direct
+    DFT of the same samples (strict inclusion at the grid edge), at every pixel."""
+    s = small_snapshot
+    with api.Engine(edge_mode=api.EDGE_STRICT, presplat=1) as e:
+        R = e.image(s)
+    o = O.image_sii(s, edge_mode=1)
+    assert O.rel_rms(R, o.pre) < IMG_TOL
+    N = s.image_size
+    yy, xx = np.mgrid[0:N, 0:N]
+    px, py = xx.ravel(), yy.ravel()
+    scale = _scale(s.cell_size, o.G)
+    inc = O.inclusion_mask(o.r, scale, o.G, edge_mode=1)
+    vin, q, sv, _ = O.preprocess64(s)
+    inv_det = 1 / abs(o.vin[0, 0] * o.vin[1, 1] - o.vin[0, 1] * o.vin[1, 0])
+    d = O.dft_pixels_sep(q, sv, o.vr, o.vi, inv_det, s.num_samples, o.vin, N, float(np.float32(s.cell_size)),
+                         px, py, inc).reshape(N, N)
+    err = O.rel_rms(R, d)
+    print("small: rel RMS vs FP64 DFT", err)
+    assert err < IMG_TOL
+
+
+def test_fipipe_device_path_equals_engine(cuda_device, small_snapshot, small_run):
+    s = small_snapshot
+    buf = api.preprocess_measurement_set_gpu(s, want_bin=True)
+    img = api.FIpipeDevice(buf, s.image_size, s.cell_size)
+    api.free_device_preprocess_buffers(buf)
+    assert O.rel_rms(img, small_run["image"]) < 1e-6
+
+
+def _quartet():
+    from tests.golden.make_golden import quartet
+    return quartet()
+
+
+def test_fipipe_matches_oracle(cuda_device):
+    visr, visi, b, v, N, cell = _quartet()
+    img = api.FIpipe(visr, visi, b, v, N, cell)
+    o = O.image_fipk(visr, visi, b, v, N, cell, coord_mode=0)
+    assert O.rel_rms(img, o.image) < IMG_TOL
+    with api.Engine(api.archive_options(coord_mode=api.COORD_REF32)) as e:
+        img32 = e.fipipe(visr, visi, b, v, N, cell)
+        assert e.stats()["num_terms"] == o.sc.K
+    o32 = O.image_fipk(visr, visi, b, v, N, cell, coord_mode=1)
+    assert O.rel_rms(img32, o32.image) < IMG_TOL
+
+
+def test_fipipe_binning_bit_exact(cuda_device):
+    visr, visi, b, v, N, cell = _quartet()
+    for cm in (0, 1):
+        with api.Engine(api.archive_options(coord_mode=cm)) as e:
+            e.fipipe(visr, visi, b, v, N, cell)
+            _check_binning(e, e.stats(), b.astype(np.float64), visr, visi, cell, coord_mode=cm)
+
+
+@pytest.mark.skipif(O.load_reference_fipipe() is None, reason="reference library not built")
+def test_fipipe_matches_reference_binary(cuda_device):
+    """The reference's own archive imager, compiled unmodified for sm_100a, on the same inputs."""
+    visr, visi, b, v, N, cell = _quartet()
+    ref = O.run_reference_fipipe(visr, visi, b, v, N, cell)
+    ref2 = O.run_reference_fipipe(visr, visi, b, v, N, cell)
+    noise = O.rel_rms(ref2, ref)
+    with api.Engine(api.archive_options(coord_mode=api.COORD_REF32)) as e:
+        img32 = e.fipipe(visr, visi, b, v, N, cell)
+    img64 = api.FIpipe(visr, visi, b, v, N, cell)
+    e32, e64 = O.rel_rms(img32, ref), O.rel_rms(img64, ref)
+    print(f"vs reference binary: ref32 {e32:.3e} fp64 {e64:.3e} reference rerun noise {noise:.3e}")
+    assert e32 < IMG_TOL
+    assert e64 < IMG_TOL
+
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "fipk_small.npz")
+
+
+@pytest.mark.skipif(not os.path.exists(GOLDEN), reason="golden output absent")
+def test_fipipe_matches_reference_golden(cuda_device):
+    visr, visi, b, v, N, cell = _quartet()
+    z = np.load(GOLDEN)
+    with api.Engine(api.archive_options(coord_mode=api.COORD_REF32)) as e:
+        img = e.fipipe(visr, visi, b, v, N, cell)
+    assert O.rel_rms(img, z["image"]) < IMG_TOL
+
+
+def test_all_flagged_gives_zero_image(cuda_device):
+    s = synth.make_snapshot("small", n_rows_limit=400, nchan=4)
+    s.flag0[:] = 1
+    s.flag3[:] = 1
+    with api.Engine() as e:
+        img = e.image(s)
+    assert np.all(img == 0)
+
+
+def test_empty_input_is_an_error(cuda_device):
+    s = synth.make_snapshot("small", n_rows_limit=10, nchan=2)
+    s.num_rows = 0
+    with api.Engine() as e:
+        with pytest.raises(api.SvdiError) as ei:
+            e.image(s)
+    assert ei.value.status == 2
+
+
+def test_edge_clipping_and_integer_positions(cuda_device):
+    """Samples whose footprints cross the grid edge (clipped, reference rule) or lie exactly on a
+    grid cell (W+1-cell footprint carrying exp(-beta) at both ends) match the oracle."""
+    N, cell = 64, 2e-3
+    G = 96
+    scale = float(np.float32(cell)) * G
+    rng = np.random.default_rng(5)
+    n = 3000
+    b = rng.uniform(-1.0, 1.0, (n, 3)) * (G / 2 + 3) / scale
+    b[:, 2] *= 1e-3
+    # exact integer grid positions (scale * b integral): fraction 0 in both, one, other axis
+    ints = rng.integers(-G // 2 + 5, G // 2 - 5, (300, 2)).astype(np.float64)
+    b[:300, :2] = ints / scale
+    b[300:400, 0] = ints[:100, 0] / scale
+    b[400:500, 1] = ints[100:200, 1] / scale
+    b = b.astype(np.float32)
+    visr = rng.normal(size=n).astype(np.float32)
+    visi = rng.normal(size=n).astype(np.float32)
+    v = np.eye(3, dtype=np.float32)
+    v[0] = [0.8, 0.6, 0.0]
+    v[1] = [-0.6, 0.8, 0.0]
+    with api.Engine(api.archive_options(coord_mode=api.COORD_REF32, keep_grid=1)) as e:
+        img = e.fipipe(visr, visi, b, v, N, cell)
+        st = e.stats()
+        _check_binning(e, st, b.astype(np.float64), visr, visi, cell, coord_mode=1)
+        grid = e.buffer(api.BUF_GRID).reshape(-1, G, G)
+    o = O.image_fipk(visr, visi, b, v, N, cell, coord_mode=1)
+    inv_det = 1.0 / abs(0.8 * 0.8 + 0.6 * 0.6)
+    og = O.grid(b.astype(np.float64), visr, visi, scale, G, o.sc, inv_det, coord_mode=1)
+    assert np.linalg.norm(grid - og) / np.linalg.norm(og) < 2e-6
+    assert O.rel_rms(img, o.image) < IMG_TOL
+
+
+@pytest.mark.parametrize("N", [255, 100, 64])
+def test_odd_and_small_image_sizes(cuda_device, N):
+    s = synth.make_snapshot("small", n_rows_limit=3000, nchan=8)
+    cell = 4e-4 * 256 / N
+    with api.Engine() as e:
+        img = e.image(s, N, cell)
+    o = O.image_sii(s, N, cell)
+    assert O.rel_rms(img, o.image) < IMG_TOL
+
+
+def test_wterm_multi_slab_matches_oracle_and_dft(cuda_device):
+    """Non-coplanar snapshot: several w-slabs x Chebyshev terms (tile 32 gridder, K > 1)."""
+    s = snapshot("widefield", nchan=4, n_rows_limit=6000, image_size=128, cell_size=6e-4)
+    with api.Engine(k_rule=api.KRULE_FIXED, fixed_k=12, target_alpha=2.0, edge_mode=api.EDGE_STRICT,
+                    presplat=1) as e:
+        R = e.image(s)
+        st = e.stats()
+    o = O.image_sii(s, edge_mode=1, k_rule=12, target_alpha=2.0)
+    assert st["num_slabs"] == o.sc.num_slabs > 1 and st["num_terms"] == 12
+    assert O.rel_rms(R, o.pre) < IMG_TOL
+    rng = np.random.default_rng(2)
+    N = s.image_size
+    px, py = rng.integers(0, N, 300), rng.integers(0, N, 300)
+    inc = O.inclusion_mask(o.r, _scale(s.cell_size, o.G), o.G, edge_mode=1)
+    inv_det = 1 / abs(o.vin[0, 0] * o.vin[1, 1] - o.vin[0, 1] * o.vin[1, 0])
+    d = O.dft_pixels(o.r, o.vr, o.vi, inv_det, s.num_samples, o.vin, N, float(np.float32(s.cell_size)), px, py,
+                     inc)
+    m = np.isfinite(d)
+    assert O.rel_rms(R[py, px][m], d[m]) < IMG_TOL
+
+
+def test_slab_batching_matches_single_batch_when_one_slab(cuda_device, small_snapshot):
+    with api.Engine(max_batch_slabs=1) as e:
+        a = e.image(small_snapshot)
+    with api.Engine() as e:
+        b = e.image(small_snapshot)
+    assert O.rel_rms(a, b) < 1e-6
+
+
+def test_repeat_calls_are_stable(cuda_device, small_snapshot):
+    with api.Engine() as e:
+        a = e.image(small_snapshot)
+        b = e.image(small_snapshot)
+    assert O.rel_rms(a, b) < 1e-6
+
+
+def test_archive_cli_round_trip(cuda_device, tmp_path):
+    """sharedlibrary_gpu with FITS inputs (archive/pipe_interface.cpp argv) equals api.FIpipe."""
+    from svdimager_b200 import fits
+    visr, visi, b, v, N, cell = _quartet()
+    paths = {}
+    for name, arr in (("Visreal", visr), ("Visimag", visi), ("B", b), ("V", v)):
+        paths[name] = str(tmp_path / f"{name}.fits")
+        fits.write_fits(paths[name], arr.astype(np.float64))  # SVD_MFS.py writes float64
+    out = str(tmp_path / "out.fits")
+    exe = os.path.join(os.path.dirname(api.HERE), "svdimager_b200", "bin", "sharedlibrary_gpu")
+    r = subprocess.run([exe, paths["Visreal"], paths["Visimag"], paths["B"], paths["V"], str(N), str(len(visr)),
+                        repr(cell), out], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    img = fits.read_fits(out)
+    ref = api.FIpipe(visr, visi, b, v, N, np.float32(cell))
+    assert O.rel_rms(img, ref) < 1e-6
+
+
+def test_integrated_cli_round_trip(cuda_device, tmp_path):
+    """svd_integrated_imager_gpu on a snapshot bundle equals the engine on the same snapshot."""
+    from svdimager_b200 import bundle, fits
+    s0 = synth.make_snapshot("small", n_rows_limit=2000, nchan=8, snapshot_index=0)
+    s1 = synth.make_snapshot("small", n_rows_limit=2000, nchan=8, snapshot_index=1)
+    p = str(tmp_path / "obs.ms")
+    bundle.write_bundle(p, [s1, s0])
+    out = str(tmp_path / "img.fits")
+    exe = os.path.join(os.path.dirname(api.HERE), "svdimager_b200", "bin", "svd_integrated_imager_gpu")
+    r = subprocess.run([exe, p, "128", "8e-4", "1", out], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert "Found 2 TIME snapshot(s)" in r.stderr
+    img = fits.read_fits(out)
+    with api.Engine() as e:
+        ref = e.image(s1, 128, 8e-4)
+    assert O.rel_rms(img, ref) < 1e-6
+
+
+def test_precision_config_properties(cuda_device):
+    """The headline configuration (8.4M samples, 2048^2): flag mask, sample accounting and
+    accuracy against the FP64 DFT at random pixels (strict inclusion)."""
+    s = snapshot("precision")
+    with api.Engine(edge_mode=api.EDGE_STRICT, presplat=1, k_rule=api.KRULE_TARGET,
+                    target_error=1e-7) as e:
+        R = e.image(s)
+        st = e.stats()
+        vr, vi = e.buffer(api.BUF_VIS_REAL), e.buffer(api.BUF_VIS_IMAG)
+        q, sv = e.buffer(api.BUF_Q).reshape(-1, 3), e.buffer(api.BUF_S)
+    ovr, ovi = O.collapse(s)
+    assert np.array_equal(vr, ovr) and np.array_equal(vi, ovi)
+    vin = np.array(st["vin"]).reshape(3, 3)
+    r = O.expand_coords(q, sv)
+    G = st["grid_size"]
+    inc = O.inclusion_mask(r, _scale(s.cell_size, G), G, edge_mode=1)
+    assert st["num_gridded"] == int(inc.sum())
+    rng = np.random.default_rng(7)
+    N = s.image_size
+    npix = 256
+    px, py = rng.integers(0, N, npix), rng.integers(0, N, npix)
+    inv_det = 1 / abs(vin[0, 0] * vin[1, 1] - vin[0, 1] * vin[1, 0])
+    d = O.dft_pixels_sep(q, sv, vr, vi, inv_det, s.num_samples, vin, N, float(np.float32(s.cell_size)), px, py, inc)
+    err = O.rel_rms(R[py, px], d)
+    print("precision: K", st["num_terms"], "slabs", st["num_slabs"], "rel RMS vs FP64 DFT", err)
+    assert err < IMG_TOL
