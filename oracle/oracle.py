@@ -325,20 +325,25 @@ def image_sii(snap, N=None, cell=None, edge_mode=0, k_rule="bucket", target_alph
     return OracleImage(img, R, vin, sc, G, r, vr, vi)
 
 
-def load_reference_fipipe():
+REF_PRECISE_LIB_PATH = os.path.join(HERE, "_ref", "libfipk_ref_precise.so")
+
+
+def load_reference_fipipe(precise=False):
     """The reference's own archive FIpipe (compiled from archive/FIPkernels.cu for sm_100a by
-    oracle/Makefile) or None when it was not built. Runs on the GPU only."""
-    if not os.path.exists(REF_LIB_PATH):
+    oracle/Makefile; precise=True: the build without --use_fast_math) or None when it was not
+    built. Runs on the GPU only."""
+    path = REF_PRECISE_LIB_PATH if precise else REF_LIB_PATH
+    if not os.path.exists(path):
         return None
-    L = ctypes.CDLL(REF_LIB_PATH)
+    L = ctypes.CDLL(path)
     fn = getattr(L, "_Z6FIpipePfS_S_S_S_mmf")  # int FIpipe(float*,float*,float*,float*,float*,size_t,size_t,float)
     fn.restype = ctypes.c_int
     fn.argtypes = [ctypes.c_void_p] * 5 + [ctypes.c_size_t, ctypes.c_size_t, ctypes.c_float]
     return fn
 
 
-def run_reference_fipipe(visr, visi, bin_, vin, N, cell):
-    fn = load_reference_fipipe()
+def run_reference_fipipe(visr, visi, bin_, vin, N, cell, precise=False):
+    fn = load_reference_fipipe(precise)
     if fn is None:
         raise RuntimeError("reference library not built (make -C oracle ref)")
     vr = _c(visr, np.float32).copy()

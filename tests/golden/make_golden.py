@@ -44,13 +44,18 @@ def main(out_dir):
     visr, visi, b, v, N, cell = quartet()
     img = O.run_reference_fipipe(visr, visi, b, v, N, cell)
     img2 = O.run_reference_fipipe(visr, visi, b, v, N, cell)
+    imgp = O.run_reference_fipipe(visr, visi, b, v, N, cell, precise=True)
+    assert np.any(img != 0) and np.any(imgp != 0), "reference FIpipe returned an empty image"
     sc = O.slab_config_fipk(b[:, 2], v.astype(np.float64), N, cell)
     os.makedirs(out_dir, exist_ok=True)
     path = os.path.join(out_dir, "fipk_small.npz")
-    np.savez_compressed(path, image=img, image_rerun=img2, input_sha256=digest(visr, visi, b, v),
-                        K=sc.K, N=N, cell=cell)
+    # image: the reference as its own Makefile builds it (--use_fast_math);
+    # image_precise: the same source built without --use_fast_math.
+    np.savez_compressed(path, image=img, image_rerun=img2, image_precise=imgp,
+                        input_sha256=digest(visr, visi, b, v), K=sc.K, N=N, cell=cell)
     print("wrote", path, "K", sc.K, "rerun rel diff",
-          float(np.linalg.norm(img - img2) / np.linalg.norm(img)))
+          float(np.linalg.norm(img - img2) / np.linalg.norm(img)),
+          "fast-math vs precise", float(np.linalg.norm(img - imgp) / np.linalg.norm(imgp)))
 
 
 if __name__ == "__main__":

@@ -172,14 +172,61 @@ def test_fipipe_matches_reference_binary(cuda_device):
     visr, visi, b, v, N, cell = _quartet()
     ref = O.run_reference_fipipe(visr, visi, b, v, N, cell)
     ref2 = O.run_reference_fipipe(visr, visi, b, v, N, cell)
+    assert np.any(ref != 0), "reference FIpipe returned an empty image (kernel launch failed?)"
     noise = O.rel_rms(ref2, ref)
     with api.Engine(api.archive_options(coord_mode=api.COORD_REF32)) as e:
         img32 = e.fipipe(visr, visi, b, v, N, cell)
     img64 = api.FIpipe(visr, visi, b, v, N, cell)
     e32, e64 = O.rel_rms(img32, ref), O.rel_rms(img64, ref)
-    print(f"vs reference binary: ref32 {e32:.3e} fp64 {e64:.3e} reference rerun noise {noise:.3e}")
-    assert e32 < IMG_TOL
-    assert e64 < IMG_TOL
+    print(f"vs reference binary (--use_fast_math): ref32 {e32:.3e} fp64 {e64:.3e} "
+          f"reference rerun noise {noise:.3e}")
+    # The reference's own build approximates the degree-based trigonometry of its SIN
+    # reprojection (fast-math cos near 90 deg), moving splat positions by up to ~1e-3 pixel; the
+    # same source built with IEEE math functions is the parity target at 1e-5.
+    assert e32 < 1e-3 and e64 < 1e-3
+    refp = O.run_reference_fipipe(visr, visi, b, v, N, cell, precise=True)
+    p32, p64 = O.rel_rms(img32, refp), O.rel_rms(img64, refp)
+    print(f"vs reference binary (IEEE math): ref32 {p32:.3e} fp64 {p64:.3e}")
+    assert p32 < IMG_TOL
+    assert p64 < IMG_TOL
+
+
+def _wide_cell_inputs():
+    """Samples inside the grid of a 128^2 image at cell 8e-3 rad, a 5-source sky. At this cell the
+    reference's FP32 degree-based reprojection is accurate to ~1e-5 pixel (its rounding error
+    scales as 1/cell), so the whole archive path can be compared at 1e-5."""
+    rng = np.random.default_rng(11)
+    N, cell = 128, 8e-3
+    n = 40000
+    r = np.zeros((n, 3))
+    r[:, :2] = rng.uniform(-58.0, 58.0, (n, 2))
+    r[:, 2] = rng.normal(0, 1e-3, n)
+    src = np.array([[3.0, 0.1, -0.2], [1.0, -0.3, 0.05], [0.5, 0.25, 0.3], [2.0, 0.0, 0.0],
+                    [0.7, -0.1, -0.35]])
+    ph = -2 * np.pi * (np.outer(r[:, 0], src[:, 1]) + np.outer(r[:, 1], src[:, 2]))
+    vis = (np.exp(1j * ph) @ src[:, 0]) + rng.normal(0, 0.05, n) + 1j * rng.normal(0, 0.05, n)
+    th = 0.4
+    v = np.array([[np.cos(th), np.sin(th), 0.0], [-np.sin(th), np.cos(th), 0.0], [0.0, 0.0, 1.0]])
+    return (vis.real.astype(np.float32), vis.imag.astype(np.float32), r.astype(np.float32),
+            v.astype(np.float32), N, cell)
+
+
+@pytest.mark.skipif(O.load_reference_fipipe() is None, reason="reference library not built")
+def test_fipipe_matches_reference_binary_wide_cell(cuda_device):
+    visr, visi, b, v, N, cell = _wide_cell_inputs()
+    refp = O.run_reference_fipipe(visr, visi, b, v, N, cell, precise=True)
+    ref = O.run_reference_fipipe(visr, visi, b, v, N, cell)
+    assert np.any(refp != 0)
+    with api.Engine(api.archive_options(coord_mode=api.COORD_REF32)) as e:
+        img32 = e.fipipe(visr, visi, b, v, N, cell)
+    img64 = api.FIpipe(visr, visi, b, v, N, cell)
+    o = O.image_fipk(visr, visi, b, v, N, cell, coord_mode=1)
+    vals = {"ref32/ieee": O.rel_rms(img32, refp), "fp64/ieee": O.rel_rms(img64, refp),
+            "ref32/fast": O.rel_rms(img32, ref), "oracle/ieee": O.rel_rms(o.image, refp),
+            "fast/ieee": O.rel_rms(ref, refp)}
+    print("wide cell vs reference binary:", {k: f"{x:.2e}" for k, x in vals.items()})
+    assert vals["ref32/ieee"] < IMG_TOL and vals["oracle/ieee"] < IMG_TOL
+    assert vals["fp64/ieee"] < IMG_TOL
 
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "fipk_small.npz")
@@ -191,7 +238,8 @@ def test_fipipe_matches_reference_golden(cuda_device):
     z = np.load(GOLDEN)
     with api.Engine(api.archive_options(coord_mode=api.COORD_REF32)) as e:
         img = e.fipipe(visr, visi, b, v, N, cell)
-    assert O.rel_rms(img, z["image"]) < IMG_TOL
+    assert O.rel_rms(img, z["image_precise"]) < IMG_TOL
+    assert O.rel_rms(img, z["image"]) < 1e-3
 
 
 def test_all_flagged_gives_zero_image(cuda_device):

@@ -162,5 +162,9 @@ def test_oracle_matches_reference_binary_golden():
     visr, visi, b, v, N, cell = quartet()
     assert str(z["input_sha256"]) == digest(visr, visi, b, v)
     img = O.image_fipk(visr, visi, b, v, N, cell, coord_mode=1)
-    assert O.rel_rms(img.image, z["image"]) < 1e-5
+    # the reference source built with IEEE math functions: parity at 1e-5
+    assert O.rel_rms(img.image, z["image_precise"]) < 1e-5
+    # the reference as its Makefile builds it (--use_fast_math): its approximate trigonometry in
+    # the SIN reprojection moves splat positions by up to ~1e-3 pixel
+    assert O.rel_rms(img.image, z["image"]) < 1e-3
     assert int(z["K"]) == img.sc.K
