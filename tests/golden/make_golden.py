@@ -32,6 +32,27 @@ def quartet():
     return vr, vi, b, vin.astype(np.float32), s.image_size, s.cell_size
 
 
+def wide_cell_quartet():
+    """Samples inside the grid of a 128^2 image at cell 8e-3 rad (40,000 samples, a 5-source sky
+    plus noise, Vin an in-plane rotation). At this cell the reference's FP32 degree-based SIN
+    reprojection is accurate to ~1e-5 pixel (its rounding error scales as 1/cell), so the whole
+    archive path can be compared at 1e-5."""
+    rng = np.random.default_rng(11)
+    N, cell = 128, 8e-3
+    n = 40000
+    r = np.zeros((n, 3))
+    r[:, :2] = rng.uniform(-58.0, 58.0, (n, 2))
+    r[:, 2] = rng.normal(0, 1e-3, n)
+    src = np.array([[3.0, 0.1, -0.2], [1.0, -0.3, 0.05], [0.5, 0.25, 0.3], [2.0, 0.0, 0.0],
+                    [0.7, -0.1, -0.35]])
+    ph = -2 * np.pi * (np.outer(r[:, 0], src[:, 1]) + np.outer(r[:, 1], src[:, 2]))
+    vis = (np.exp(1j * ph) @ src[:, 0]) + rng.normal(0, 0.05, n) + 1j * rng.normal(0, 0.05, n)
+    th = 0.4
+    v = np.array([[np.cos(th), np.sin(th), 0.0], [-np.sin(th), np.cos(th), 0.0], [0.0, 0.0, 1.0]])
+    return (vis.real.astype(np.float32), vis.imag.astype(np.float32), r.astype(np.float32),
+            v.astype(np.float32), N, cell)
+
+
 def digest(*arrays):
     h = hashlib.sha256()
     for a in arrays:
@@ -56,6 +77,16 @@ def main(out_dir):
     print("wrote", path, "K", sc.K, "rerun rel diff",
           float(np.linalg.norm(img - img2) / np.linalg.norm(img)),
           "fast-math vs precise", float(np.linalg.norm(img - imgp) / np.linalg.norm(imgp)))
+    visr, visi, b, v, N, cell = wide_cell_quartet()
+    img = O.run_reference_fipipe(visr, visi, b, v, N, cell)
+    imgp = O.run_reference_fipipe(visr, visi, b, v, N, cell, precise=True)
+    assert np.any(img != 0) and np.any(imgp != 0), "reference FIpipe returned an empty image"
+    sc = O.slab_config_fipk(b[:, 2], v.astype(np.float64), N, cell)
+    path = os.path.join(out_dir, "fipk_widecell.npz")
+    np.savez_compressed(path, image=img, image_precise=imgp, input_sha256=digest(visr, visi, b, v),
+                        K=sc.K, N=N, cell=cell)
+    print("wrote", path, "K", sc.K, "fast-math vs precise",
+          float(np.linalg.norm(img - imgp) / np.linalg.norm(imgp)))
 
 
 if __name__ == "__main__":

@@ -162,9 +162,27 @@ def test_oracle_matches_reference_binary_golden():
     visr, visi, b, v, N, cell = quartet()
     assert str(z["input_sha256"]) == digest(visr, visi, b, v)
     img = O.image_fipk(visr, visi, b, v, N, cell, coord_mode=1)
-    # the reference source built with IEEE math functions: parity at 1e-5
-    assert O.rel_rms(img.image, z["image_precise"]) < 1e-5
-    # the reference as its Makefile builds it (--use_fast_math): its approximate trigonometry in
-    # the SIN reprojection moves splat positions by up to ~1e-3 pixel
+    # At cell 4e-4 rad the reference's reprojection (FP32, degrees, theta ~ 87 deg where one ulp
+    # is 7.6e-6 deg) moves splat positions by ~3e-4 pixel, so its image carries ~3e-4 relative
+    # rounding noise; the FP64 restatement agrees with both of its builds at that level.
+    assert O.rel_rms(img.image, z["image_precise"]) < 1e-3
     assert O.rel_rms(img.image, z["image"]) < 1e-3
+    assert int(z["K"]) == img.sc.K
+
+
+GOLDEN_WIDE = os.path.join(os.path.dirname(__file__), "golden", "fipk_widecell.npz")
+
+
+@pytest.mark.skipif(not os.path.exists(GOLDEN_WIDE), reason="golden output of the reference binary absent")
+def test_oracle_matches_reference_binary_golden_wide_cell():
+    """Pins the oracle at 1e-5: at cell 8e-3 rad the reference's FP32 reprojection noise is
+    negligible, so the reference binary (IEEE-math build) and the restatement agree over the
+    whole archive path (gridding, FFT, recombination, correction, reprojection, splat)."""
+    from tests.golden.make_golden import digest, wide_cell_quartet
+    z = np.load(GOLDEN_WIDE)
+    visr, visi, b, v, N, cell = wide_cell_quartet()
+    assert str(z["input_sha256"]) == digest(visr, visi, b, v)
+    img = O.image_fipk(visr, visi, b, v, N, cell, coord_mode=1)
+    assert O.rel_rms(img.image, z["image_precise"]) < 1e-5
+    assert O.rel_rms(img.image, z["image"]) < 1e-4
     assert int(z["K"]) == img.sc.K
