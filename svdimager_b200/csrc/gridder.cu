@@ -23,6 +23,12 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 
+// Exact ES kernel psi(x) = exp(beta (sqrt(1 - x^2) - 1)) written without cancellation (rare path).
+__device__ __forceinline__ float es_exact(float beta, float x) {
+    if (fabsf(x) > 1.0f) return 0.0f;
+    return expf(-beta * x * x / (1.0f + sqrtf((1.0f - x) * (1.0f + x))));
+}
+
 __device__ __forceinline__ void red_add_v2(float2* addr, float a, float b) {
     asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(addr), "f"(a), "f"(b) : "memory");
 }
@@ -45,22 +51,25 @@ __global__ void __launch_bounds__(kThreads) k_grid_fp32(
     extern __shared__ float tile[];  // [KC][2][R][RS]
     __shared__ int bbox[4];          // row min, row max, col min, col max
     __shared__ int seg_key;
+    // per-warp staging of the decoded batch: {u_x, u_y, vre, vim} and {fast-path base, s}
+    __shared__ float4 st_f[kWarps][32];
+    __shared__ int2 st_i[kWarps][32];
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int HW = W / 2;
-    constexpr int RPP = 32 / W;                // footprint rows per pass
+    constexpr int RPP = 32 / W;                  // footprint rows per pass
     constexpr int PASSES = (W + RPP - 1) / RPP;
+    constexpr bool PAIR = 2 * W <= 16;           // two samples per polynomial pass
     const int la = lane / W, lb = lane % W;
     const bool lane_cell = lane < RPP * W;
-
-    // this lane's polynomial piece (lanes 0..2W-1)
+    const int lane_off = la * C::RS + lb;
+    // polynomial piece of this lane: x-piece (local < W) or y-piece (W <= local < 2W)
+    const int local = PAIR ? (lane & 15) : lane;
+    const bool is_x = local < W;
+    const int piece = is_x ? local : (local < 2 * W ? local - W : 0);
     float coef[kPolyDeg + 1];
-    {
-        const int piece = lane % W;
 #pragma unroll
-        for (int d = 0; d <= kPolyDeg; ++d) coef[d] = poly.c[piece][d];
-    }
-    const float edge_w = poly.edge;
+    for (int d = 0; d <= kPolyDeg; ++d) coef[d] = poly.c[piece][d];
 
     for (int i = threadIdx.x; i < KC * 2 * C::PLANE; i += kThreads) tile[i] = 0.0f;
     if (threadIdx.x == 0) {
@@ -72,6 +81,7 @@ __global__ void __launch_bounds__(kThreads) k_grid_fp32(
     const unsigned int n_chunks = (rec_hi - rec_lo + chunk - 1) / chunk;
     const long long GG = g.G * g.G;
     const int tiles2 = g.ntile * g.ntile;
+    const bool need_s = !(KC == 1 && term0 == 0);
 
     for (unsigned int ch = blockIdx.x; ch < n_chunks; ch += gridDim.x) {
         const unsigned int c_beg = rec_lo + ch * chunk;
@@ -92,98 +102,124 @@ __global__ void __launch_bounds__(kThreads) k_grid_fp32(
             if (s_beg < s_end) {
                 const int slab = key / tiles2;
                 const int t1 = (key / g.ntile) % g.ntile, t2 = key % g.ntile;
-                int rmin = C::R, rmax = -1, cmin = C::R, cmax = -1;
                 for (unsigned int b0 = s_beg + warp * 32; b0 < s_end; b0 += kWarps * 32) {
+                    // ---- decode this lane's record once per batch
                     const unsigned int my = b0 + lane;
+                    const bool valid = my < s_end;
                     SampleRec r = {0, 0, 0.0f, 0.0f};
                     float sv = 0.0f;
-                    if (my < s_end) {
+                    if (valid) {
                         r = rec[my];
-                        if (rec_s) sv = rec_s[my];
+                        if (need_s) sv = rec_s[my];
                     }
+                    const int cx = r.xq >> 24, cy = r.yq >> 24;
+                    const int fxq = r.xq & 0xFFFFFF, fyq = r.yq & 0xFFFFFF;
+                    const int r0 = cx - (HW - 1), c0 = cy - (HW - 1);
+                    const bool rare = valid && (fxq == 0 || fyq == 0 || r0 < 0 || c0 < 0);
+                    st_f[warp][lane] = make_float4(fmaf(2.0f, (float)fxq * (1.0f / 16777216.0f), -1.0f),
+                                                   fmaf(2.0f, (float)fyq * (1.0f / 16777216.0f), -1.0f),
+                                                   r.vre, r.vim);
+                    st_i[warp][lane] = make_int2(r0 * C::RS + c0, __float_as_int(sv));
+                    // bounding box of the batch (one warp reduction per 32 samples)
+                    const int rlo = valid ? max(0, fxq ? r0 : r0 - 1) : C::R;
+                    const int rhi = valid ? cx + HW : -1;
+                    const int clo = valid ? max(0, fyq ? c0 : c0 - 1) : C::R;
+                    const int chi = valid ? cy + HW : -1;
+                    const int brlo = __reduce_min_sync(0xffffffffu, rlo);
+                    const int brhi = __reduce_max_sync(0xffffffffu, rhi);
+                    const int bclo = __reduce_min_sync(0xffffffffu, clo);
+                    const int bchi = __reduce_max_sync(0xffffffffu, chi);
+                    if (lane == 0 && brhi >= 0) {
+                        atomicMin(&bbox[0], brlo); atomicMax(&bbox[1], brhi);
+                        atomicMin(&bbox[2], bclo); atomicMax(&bbox[3], bchi);
+                    }
+                    unsigned int rare_mask = __ballot_sync(0xffffffffu, rare);
+                    __syncwarp();
                     const int nb = min(32u, s_end - b0);
-                    for (int j = 0; j < nb; ++j) {
-                        const int xq = __shfl_sync(0xffffffffu, r.xq, j);
-                        const int yq = __shfl_sync(0xffffffffu, r.yq, j);
-                        const float vre = __shfl_sync(0xffffffffu, r.vre, j);
-                        const float vim = __shfl_sync(0xffffffffu, r.vim, j);
-                        const int cx = xq >> 24, cy = yq >> 24;
-                        const int fxq = xq & 0xFFFFFF, fyq = yq & 0xFFFFFF;
-                        // weight of this lane's piece
-                        const float f = (float)(lane < W ? fxq : fyq) * (1.0f / 16777216.0f);
-                        const float u = fmaf(2.0f, f, -1.0f);
+                    // ---- fast path: W x W footprint, polynomial weights, no bounds checks
+                    constexpr int STEP = PAIR ? 2 : 1;
+                    for (int j = 0; j < nb; j += STEP) {
+                        const int jw = PAIR ? min(j + (lane >> 4), 31) : j;
+                        const float4 su = st_f[warp][jw];
+                        const float u = is_x ? su.x : su.y;
                         float w = coef[kPolyDeg];
 #pragma unroll
                         for (int d = kPolyDeg - 1; d >= 0; --d) w = fmaf(w, u, coef[d]);
-                        const float wy = __shfl_sync(0xffffffffu, w, W + lb);
-                        float tv[KC];
-                        if (KC == 1 && term0 == 0) {
-                            tv[0] = 1.0f;
-                        } else {
-                            const float s = __shfl_sync(0xffffffffu, sv, j);
-                            float tm2 = 1.0f, tm1 = s;
-                            for (int t = 0; t < term0 + KC; ++t) {
-                                float tn = t == 0 ? 1.0f : (t == 1 ? s : 2.0f * s * tm1 - tm2);
-                                if (t >= 2) { tm2 = tm1; tm1 = tn; }
-                                if (t >= term0) tv[t - term0] = tn;
-                            }
-                        }
-                        const int r0 = cx - (HW - 1), c0 = cy - (HW - 1);
 #pragma unroll
-                        for (int p = 0; p < PASSES; ++p) {
-                            const int i = la + p * RPP;
-                            const float wx = __shfl_sync(0xffffffffu, w, (i < W ? i : 0));
-                            const int rr = r0 + i, cc = c0 + lb;
-                            if (lane_cell && i < W && rr >= 0 && cc >= 0) {
-                                const float kv = wx * wy;
-                                const float ar = kv * vre, ai = kv * vim;
-#pragma unroll
-                                for (int t = 0; t < KC; ++t) {
-                                    float* pl = tile + (size_t)t * 2 * C::PLANE + rr * C::RS + cc;
-                                    atomicAdd(pl, ar * tv[t]);
-                                    atomicAdd(pl + C::PLANE, ai * tv[t]);
+                        for (int h = 0; h < STEP; ++h) {
+                            const int js = j + h;
+                            if (js >= nb || ((rare_mask >> js) & 1u)) continue;  // warp-uniform
+                            const float4 sf = st_f[warp][js];
+                            const int2 si = st_i[warp][js];
+                            const int src = PAIR ? 16 * h : 0;
+                            const float wy = __shfl_sync(0xffffffffu, w, src + W + lb);
+                            float tv[KC];
+                            if (!need_s) {
+                                tv[0] = 1.0f;
+                            } else {
+                                const float s = __int_as_float(si.y);
+                                float tm2 = 1.0f, tm1 = s;
+                                for (int t = 0; t < term0 + KC; ++t) {
+                                    const float tn = t == 0 ? 1.0f : (t == 1 ? s : 2.0f * s * tm1 - tm2);
+                                    if (t >= 2) { tm2 = tm1; tm1 = tn; }
+                                    if (t >= term0) tv[t - term0] = tn;
                                 }
                             }
-                        }
-                        // frac == 0: the footprint has W+1 cells; the extra one sits at offset -W/2
-                        // and carries psi(-1) = exp(-beta).
-                        if ((fxq == 0) | (fyq == 0)) {
-                            const float wxe = __shfl_sync(0xffffffffu, w, lane < W ? lane : 0);
-                            float wy_l = __shfl_sync(0xffffffffu, w, W + (lane < W ? lane : 0));
-                            for (int e = 0; e < 3; ++e) {
-                                int rr, cc;
-                                float kv;
-                                bool act;
-                                if (e == 0) {        // extra row x normal columns
-                                    act = (fxq == 0) && lane < W;
-                                    rr = cx - HW; cc = c0 + lane; kv = edge_w * wy_l;
-                                } else if (e == 1) { // normal rows x extra column
-                                    act = (fyq == 0) && lane < W;
-                                    rr = r0 + lane; cc = cy - HW; kv = wxe * edge_w;
-                                } else {             // corner
-                                    act = (fxq == 0) && (fyq == 0) && lane == 0;
-                                    rr = cx - HW; cc = cy - HW; kv = edge_w * edge_w;
-                                }
-                                if (act && rr >= 0 && cc >= 0) {
-                                    const float ar = kv * vre, ai = kv * vim;
+                            const int base = si.x + lane_off;
+#pragma unroll
+                            for (int p = 0; p < PASSES; ++p) {
+                                const int i = la + p * RPP;
+                                const float wx = __shfl_sync(0xffffffffu, w, src + (i < W ? i : 0));
+                                if (lane_cell && i < W) {
+                                    const float kv = wx * wy;
+                                    const float ar = kv * sf.z, ai = kv * sf.w;
+#pragma unroll
                                     for (int t = 0; t < KC; ++t) {
-                                        float* pl = tile + (size_t)t * 2 * C::PLANE + rr * C::RS + cc;
+                                        float* pl = tile + (size_t)t * 2 * C::PLANE + base + p * RPP * C::RS;
                                         atomicAdd(pl, ar * tv[t]);
                                         atomicAdd(pl + C::PLANE, ai * tv[t]);
                                     }
                                 }
                             }
                         }
-                        // bounding box of touched cells
-                        const int rlo = max(0, fxq ? r0 : r0 - 1), rhi = cx + HW;
-                        const int clo = max(0, fyq ? c0 : c0 - 1), chi = cy + HW;
-                        rmin = min(rmin, rlo); rmax = max(rmax, rhi);
-                        cmin = min(cmin, clo); cmax = max(cmax, chi);
                     }
-                }
-                if (lane == 0 && rmax >= 0) {
-                    atomicMin(&bbox[0], rmin); atomicMax(&bbox[1], rmax);
-                    atomicMin(&bbox[2], cmin); atomicMax(&bbox[3], cmax);
+                    // ---- rare path: exactly-integer positions (W+1 cells, psi(-1) at the ends) and
+                    // footprints clipped at the low grid edge; exact ES formula, lanes over cells
+                    while (rare_mask) {
+                        const int js = __ffs(rare_mask) - 1;
+                        rare_mask &= rare_mask - 1;
+                        const SampleRec rr_ = rec[b0 + js];
+                        const float s = need_s ? rec_s[b0 + js] : 0.0f;
+                        const int rcx = rr_.xq >> 24, rcy = rr_.yq >> 24;
+                        const int rfx = rr_.xq & 0xFFFFFF, rfy = rr_.yq & 0xFFFFFF;
+                        const int lo_r = rfx ? rcx - (HW - 1) : rcx - HW, nr = rfx ? W : W + 1;
+                        const int lo_c = rfy ? rcy - (HW - 1) : rcy - HW, nc = rfy ? W : W + 1;
+                        const float px = (float)rfx * (1.0f / 16777216.0f), py = (float)rfy * (1.0f / 16777216.0f);
+                        float tv[KC];
+                        {
+                            float tm2 = 1.0f, tm1 = s;
+                            for (int t = 0; t < term0 + KC; ++t) {
+                                const float tn = t == 0 ? 1.0f : (t == 1 ? s : 2.0f * s * tm1 - tm2);
+                                if (t >= 2) { tm2 = tm1; tm1 = tn; }
+                                if (t >= term0) tv[t - term0] = tn;
+                            }
+                        }
+                        for (int c = lane; c < nr * nc; c += 32) {
+                            const int i = c / nc, jj = c % nc;
+                            const int rr = lo_r + i, cc = lo_c + jj;
+                            if (rr < 0 || cc < 0) continue;
+                            const float x = ((float)(lo_r + i - rcx) - px) / (float)HW;
+                            const float y = ((float)(lo_c + jj - rcy) - py) / (float)HW;
+                            const float kv = es_exact(poly.beta, x) * es_exact(poly.beta, y);
+                            const float ar = kv * rr_.vre, ai = kv * rr_.vim;
+                            for (int t = 0; t < KC; ++t) {
+                                float* pl = tile + (size_t)t * 2 * C::PLANE + rr * C::RS + cc;
+                                atomicAdd(pl, ar * tv[t]);
+                                atomicAdd(pl + C::PLANE, ai * tv[t]);
+                            }
+                        }
+                    }
+                    __syncwarp();
                 }
                 __syncthreads();
                 // flush the bounding box: checkerboard sign, clip to the grid, zero behind
@@ -223,7 +259,6 @@ __global__ void __launch_bounds__(kThreads) k_grid_fp32(
         }
     }
 }
-
 template <int W, int T, int KC>
 int launch_variant(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d_offsets,
                    int key_lo, int key_hi, int slab_lo, const GridGeom& g, const SlabParams& sp,
@@ -309,6 +344,7 @@ void build_es_poly(int W, double beta, EsPoly* out) {
     for (int k = 0; k < n; ++k) nodes[k] = cos(kPi * (k + 0.5) / n);
     out->W = W;
     out->edge = (float)exp(-beta);
+    out->beta = (float)beta;
     for (int i = 0; i < kMaxSupport; ++i)
         for (int d = 0; d <= D; ++d) out->c[i][d] = 0.0f;
     for (int i = 0; i < W; ++i) {

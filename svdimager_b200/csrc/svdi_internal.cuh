@@ -57,6 +57,7 @@ struct SlabParams {
 struct EsPoly {
     float c[kMaxSupport][kPolyDeg + 1];
     float edge;           // psi(+-1) = exp(-beta), weight of the extra cell when frac == 0
+    float beta;           // ES beta (exact evaluation on the rare path)
     int W;
 };
 
