@@ -204,6 +204,31 @@ int svdi_engine_last_stats(const svdi_engine* e, svdi_stats* out);
 int svdi_engine_buffer_size(const svdi_engine* e, int which, size_t* bytes);
 int svdi_engine_copy_buffer(svdi_engine* e, int which, void* host_dst, size_t bytes);
 
+/* ---- allocation-free binning --------------------------------------------------------------- */
+/* No counterpart in the reference. For callers that must not allocate device memory once they
+ * run: a correlator's real-time loop that reserves all of its device memory at start-up and
+ * cannot stall on the allocator, or a host framework that owns the device's memory pool.
+ * Bins num_samples samples (archive layout: d_bin [num_samples][3] in wavelengths, collapsed
+ * d_vis_real / d_vis_imag) into tile records exactly like the engine's binning with one w-slab,
+ * one Chebyshev term, ES support 8, clipping at the grid edge and FP64 grid coordinates, on a
+ * grid of side ceil(1.5 image_size); vre/vim of each record are the visibility times inv_det.
+ * All pointers are DEVICE pointers owned by the caller: d_records receives up to num_samples
+ * 16-byte records {int xq, int yq, float vre, float vim}; d_offsets receives
+ * ceil(1.5 image_size / tile)^2 + 1 record offsets per tile key (offsets_capacity entries).
+ * The scratch (per-key counters and cursors, the dropped count) is a static device array of
+ * 2 * SVDI_NOALLOC_MAX_KEYS + 4 words (128 KiB) that every GPU loading this library holds until
+ * the process exits; more tile keys than SVDI_NOALLOC_MAX_KEYS are rejected with
+ * SVDI_ERR_UNSUPPORTED. The first call on a device looks the array's address up
+ * (cudaGetSymbolAddress): make it before any stream capture. Every call shares the array, so
+ * calls whose work overlaps on the GPU (other streams, threads or processes on the same device)
+ * race; serialise them. Asynchronous on cuda_stream (NULL = legacy default stream); allocates
+ * no device memory. */
+#define SVDI_NOALLOC_MAX_KEYS 16384
+int svdi_bin_samples_noalloc(const float* d_bin, const float* d_vis_real, const float* d_vis_imag,
+                             size_t num_samples, size_t image_size, float cell_size, int tile,
+                             float inv_det, void* d_records, uint32_t* d_offsets,
+                             size_t offsets_capacity, void* cuda_stream);
+
 /* Number of kernel launches this library has issued in the calling process. */
 uint64_t svdi_kernel_launch_count(void);
 

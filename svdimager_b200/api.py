@@ -34,8 +34,9 @@ EXPORTED_SYMBOLS = (
     "svdi_free_device_buffers", "svdi_default_options", "svdi_engine_create", "svdi_engine_destroy",
     "svdi_engine_image_host", "svdi_engine_image_device", "svdi_engine_fipipe_host",
     "svdi_engine_last_stats", "svdi_engine_buffer_size", "svdi_engine_copy_buffer",
-    "svdi_kernel_launch_count", "_Z6FIpipePfS_S_S_S_mmf",
+    "svdi_kernel_launch_count", "svdi_bin_samples_noalloc", "_Z6FIpipePfS_S_S_S_mmf",
 )
+NOALLOC_MAX_KEYS = 16384
 
 BUF_VIS_REAL, BUF_VIS_IMAG, BUF_Q, BUF_S, BUF_VIN, BUF_OFFSETS, BUF_RECORDS, BUF_RECORDS_S, \
     BUF_GRID, BUF_MOMENTS = range(10)
@@ -136,6 +137,7 @@ def lib():
         L.svdi_engine_buffer_size.argtypes = [P, i, ctypes.POINTER(sz)]
         L.svdi_engine_copy_buffer.argtypes = [P, i, P, sz]
         L.svdi_kernel_launch_count.restype = ctypes.c_uint64
+        L.svdi_bin_samples_noalloc.argtypes = [P, P, P, sz, sz, f, i, f, P, P, sz, P]
         _lib = L
     return _lib
 
@@ -322,3 +324,16 @@ def FIpipeDevice(buffers: PreprocessBuffers, image_size: int, cell_size: float) 
 
 def free_device_preprocess_buffers(buffers: PreprocessBuffers):
     buffers.free()
+
+
+def bin_samples_noalloc(d_bin: int, d_vis_real: int, d_vis_imag: int, num_samples: int,
+                        image_size: int, cell_size: float, tile: int, inv_det: float,
+                        d_records: int, d_offsets: int, offsets_capacity: int, stream: int = 0):
+    """Allocation-free tile binning on DEVICE pointers (svdi_bin_samples_noalloc): for callers
+    that may not allocate device memory while they run. Scratch lives in a fixed static device
+    array (at most NOALLOC_MAX_KEYS tile keys); overlapping calls on one device race."""
+    _check(lib().svdi_bin_samples_noalloc(
+        ctypes.c_void_p(d_bin), ctypes.c_void_p(d_vis_real), ctypes.c_void_p(d_vis_imag),
+        int(num_samples), int(image_size), float(cell_size), int(tile), float(inv_det),
+        ctypes.c_void_p(d_records), ctypes.c_void_p(d_offsets), int(offsets_capacity),
+        ctypes.c_void_p(stream)))
