@@ -66,7 +66,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -108,17 +108,50 @@ class ClockSampler:
 
 
 def dist_init():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    if ws <= 1:
-        return 0, 1, 0, None
+    from svdimager_b200 import replicas
+    return replicas.init_from_env("nccl", timeout_s=120)
+
+
+def serving_phase(api, big, n_requests, rate, device, seed=5):
+    """Poisson stream (rate/s) of mixed requests through a 4-slot server: the 512-station
+    headline snapshot at 2048^2, a 256-station 32-channel snapshot at 1024^2 and a 128-station
+    16-channel snapshot at 512^2. Returns latency percentiles and sustained throughput."""
+    from svdimager_b200 import synth
+    mix = [(big, big.image_size, big.cell_size),
+           (synth.make_snapshot("batching", nchan=32, flag_fraction_rows=0.0, flag_fraction_samples=0.15,
+                                snapshot_index=7), 1024, 1e-4),
+           (synth.make_snapshot("small", snapshot_index=8), 512, 2e-4)]
     import torch
-    import torch.distributed as dist
-    from datetime import timedelta
-    rank = int(os.environ["RANK"])
-    local = int(os.environ.get("LOCAL_RANK", rank))
-    torch.cuda.set_device(local)
-    dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    return rank, ws, local, dist
+    for s, _, _ in mix:  # host arrays in pinned memory, as a correlator's receive buffers would be
+        for k, v in s.arrays().items():
+            setattr(s, k, torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy())
+    rng = np.random.default_rng(seed)
+    lat, queue, run = [], [], []
+    with api.Server(num_slots=4, device=device, edge_mode=api.EDGE_STRICT, k_rule=api.KRULE_TARGET,
+                    target_error=1e-6) as srv:
+        for s, N, cell in mix:  # warm every slot's plans and buffers
+            for t in [srv.submit(s, N, cell) for _ in range(4)]:
+                srv.wait(t, 120)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
+        t0 = time.perf_counter()
+        tickets = []
+        for a in arrivals:
+            while time.perf_counter() - t0 < a:
+                time.sleep(0.0002)
+            s, N, cell = mix[int(rng.integers(len(mix)))]
+            tickets.append(srv.submit(s, N, cell))
+        for t in tickets:
+            _, info = srv.wait(t, 120)
+            lat.append(info["latency_ms"])
+            queue.append(info["queue_ms"])
+            run.append(info["run_ms"])
+        wall = time.perf_counter() - t0
+    return {"requests": n_requests, "offered_rate_per_s": rate, "slots": 4,
+            "mix": "512 st x 64 ch @2048^2, 256 st x 32 ch @1024^2, 128 st x 16 ch @512^2",
+            "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+            "queue_p99_ms": round(float(np.percentile(queue, 99)), 3),
+            "run_p50_ms": round(float(np.percentile(run, 50)), 3),
+            "sustained_snapshots_per_s": round(n_requests / wall, 2)}
 
 
 def algorithmic_bytes(n_samples, n_rows, n_chan, planes, G, N):
@@ -185,13 +218,10 @@ def run_ours(args):
         ev1.record(stream)
         torch.cuda.synchronize(dev)
     launches = api.kernel_launch_count() - n_launch0
-    ms_total = ev0.elapsed_time(ev1)
-    if dist:
-        t = torch.tensor([ms_total], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    from svdimager_b200 import replicas
+    ms_total = replicas.max_over_ranks(ev0.elapsed_time(ev1), dist, dev)
     ms_step = ms_total / args.steps
-    value = ws * args.steps / (ms_total / 1e3)
+    value = replicas.aggregate_rate(args.steps, ws, ms_total / 1e3)
 
     # end-to-end through the host API (pinned host buffers, upload + image read per step)
     pinned = {k: torch.from_numpy(v).pin_memory() for k, v in host.items()}
@@ -210,12 +240,9 @@ def run_ours(args):
         t1 = time.perf_counter()
         eng.image(psnap, out=himg)
         e2e_lat.append((time.perf_counter() - t1) * 1e3)
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = ws * args.steps / e2e_s
+    e2e_s = replicas.max_over_ranks(time.perf_counter() - t0, dist, dev)
+    e2e_value = replicas.aggregate_rate(args.steps, ws, e2e_s)
+    serving = None if args.no_serving else serving_phase(api, snap, args.serving_requests, 50.0, local)
     h2d = int(sum(v.nbytes for v in host.values()))
     d2h = int(N * N * 4)
 
@@ -294,6 +321,8 @@ def run_ours(args):
         "clocks": clk.summary(),
         "gpu_launches": int(launches),
     }
+    if serving:
+        line["serving"] = serving
     if cpu:
         line["cpu_baseline"] = cpu["baseline"]
         line["accuracy"] = cpu["accuracy"]
@@ -409,6 +438,8 @@ def main():
     ap.add_argument("--cpu-pixels", type=int, default=48)
     ap.add_argument("--ref-fraction", type=float, default=1.0 / 32)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=150)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

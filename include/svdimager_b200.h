@@ -204,6 +204,40 @@ int svdi_engine_last_stats(const svdi_engine* e, svdi_stats* out);
 int svdi_engine_buffer_size(const svdi_engine* e, int which, size_t* bytes);
 int svdi_engine_copy_buffer(svdi_engine* e, int which, void* host_dst, size_t bytes);
 
+/* ---- serving: continuous batching ---------------------------------------------------------- */
+/* New export (the reference images one snapshot per process, SVDIntegratedImager.cu:1773-1854).
+ * A server keeps num_slots engines resident (own stream, grids, cuFFT plans, tile bins) and one
+ * worker thread per slot. Requests queue in arrival order; a request is admitted when a slot is
+ * free and its device-memory estimate fits in the HBM budget beside the running ones (a smaller
+ * request may overtake a larger one that waits for memory); admitted requests overlap on the GPU.
+ * Requests that can never fit the budget are refused at submit (SVDI_ERR_OUT_OF_MEMORY). The host
+ * arrays of a request and its output image must stay valid until svdi_server_wait returns. */
+typedef struct svdi_server svdi_server;
+
+typedef struct svdi_request_info {
+    int status;                  /* SVDI_OK or the request's error status                      */
+    int slot;                    /* slot that ran it                                           */
+    size_t num_samples;
+    double queue_ms;             /* submit -> start (host wall clock)                          */
+    double run_ms;               /* start -> completion                                        */
+    double latency_ms;           /* submit -> completion                                       */
+} svdi_request_info;
+
+/* hbm_budget_bytes = 0: 80 % of the free device memory. fault_every > 0 makes every
+ * fault_every-th request fail on the host before any device work (failure-path testing). */
+int svdi_server_create(const svdi_options* opt, int num_slots, size_t hbm_budget_bytes,
+                       int fault_every, svdi_server** out);
+/* Queue a main-path request (host snapshot, host output [N][N]); returns its ticket. */
+int svdi_server_submit(svdi_server* s, const svdi_host_ms* ms, size_t image_size, float cell_size,
+                       float* dirty_image, uint64_t* ticket);
+/* Block until the request finishes (timeout_s <= 0: no limit); returns the request's status. */
+int svdi_server_wait(svdi_server* s, uint64_t ticket, double timeout_s, svdi_request_info* info);
+int svdi_server_poll(svdi_server* s, uint64_t ticket, int* done);
+int svdi_server_stats(svdi_server* s, size_t* queued, size_t* hbm_in_use, size_t* hbm_budget,
+                      uint64_t* admitted);
+/* Drains the queue, joins the workers, frees the engines. */
+void svdi_server_destroy(svdi_server* s);
+
 /* ---- allocation-free binning --------------------------------------------------------------- */
 /* No counterpart in the reference. For callers that must not allocate device memory once they
  * run: a correlator's real-time loop that reserves all of its device memory at start-up and

@@ -34,7 +34,9 @@ EXPORTED_SYMBOLS = (
     "svdi_free_device_buffers", "svdi_default_options", "svdi_engine_create", "svdi_engine_destroy",
     "svdi_engine_image_host", "svdi_engine_image_device", "svdi_engine_fipipe_host",
     "svdi_engine_last_stats", "svdi_engine_buffer_size", "svdi_engine_copy_buffer",
-    "svdi_kernel_launch_count", "svdi_bin_samples_noalloc", "_Z6FIpipePfS_S_S_S_mmf",
+    "svdi_kernel_launch_count", "svdi_bin_samples_noalloc", "svdi_server_create",
+    "svdi_server_submit", "svdi_server_wait", "svdi_server_poll", "svdi_server_stats",
+    "svdi_server_destroy", "_Z6FIpipePfS_S_S_S_mmf",
 )
 NOALLOC_MAX_KEYS = 16384
 
@@ -107,6 +109,15 @@ class Stats(ctypes.Structure):
         return d
 
 
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("slot", ctypes.c_int), ("num_samples", ctypes.c_size_t),
+                ("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double),
+                ("latency_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -138,6 +149,14 @@ def lib():
         L.svdi_engine_copy_buffer.argtypes = [P, i, P, sz]
         L.svdi_kernel_launch_count.restype = ctypes.c_uint64
         L.svdi_bin_samples_noalloc.argtypes = [P, P, P, sz, sz, f, i, f, P, P, sz, P]
+        L.svdi_server_create.argtypes = [ctypes.POINTER(Options), i, sz, i, ctypes.POINTER(P)]
+        L.svdi_server_submit.argtypes = [P, ctypes.POINTER(HostMS), sz, f, P, ctypes.POINTER(ctypes.c_uint64)]
+        L.svdi_server_wait.argtypes = [P, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(RequestInfo)]
+        L.svdi_server_poll.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(i)]
+        L.svdi_server_stats.argtypes = [P, ctypes.POINTER(sz), ctypes.POINTER(sz), ctypes.POINTER(sz),
+                                        ctypes.POINTER(ctypes.c_uint64)]
+        L.svdi_server_destroy.argtypes = [P]
+        L.svdi_server_destroy.restype = None
         _lib = L
     return _lib
 
@@ -233,8 +252,8 @@ class Engine:
     def image(self, snap, image_size: Optional[int] = None, cell_size: Optional[float] = None,
               out: Optional[np.ndarray] = None) -> np.ndarray:
         """Main path from host snapshot arrays to a host image [N][N] float32."""
-        N = int(image_size or snap.image_size)
-        cell = float(cell_size or snap.cell_size)
+        N = int(snap.image_size if image_size is None else image_size)
+        cell = float(snap.cell_size if cell_size is None else cell_size)
         h, keep = host_ms(snap)
         if out is None:
             out = np.zeros((N, N), np.float32)
@@ -324,6 +343,62 @@ def FIpipeDevice(buffers: PreprocessBuffers, image_size: int, cell_size: float) 
 
 def free_device_preprocess_buffers(buffers: PreprocessBuffers):
     buffers.free()
+
+
+class Server:
+    """Continuous-batching imaging server (svdi_server_*): `num_slots` resident engines, one
+    worker thread each; requests are admitted by free slot and HBM budget and overlap on the GPU.
+    submit() keeps the snapshot's arrays and the output image alive until wait() returns."""
+
+    def __init__(self, options: Optional[Options] = None, num_slots: int = 4, hbm_budget: int = 0,
+                 fault_every: int = 0, **kw):
+        o = options if options is not None else default_options(**kw)
+        h = ctypes.c_void_p()
+        _check(lib().svdi_server_create(ctypes.byref(o), int(num_slots), int(hbm_budget), int(fault_every),
+                                        ctypes.byref(h)))
+        self._h = h
+        self._pending = {}
+
+    def submit(self, snap, image_size: Optional[int] = None, cell_size: Optional[float] = None) -> int:
+        N = int(snap.image_size if image_size is None else image_size)
+        cell = float(snap.cell_size if cell_size is None else cell_size)
+        h, keep = host_ms(snap)
+        out = np.zeros((N, N), np.float32)
+        t = ctypes.c_uint64()
+        _check(lib().svdi_server_submit(self._h, ctypes.byref(h), N, cell, _ptr(out), ctypes.byref(t)))
+        self._pending[t.value] = (h, keep, out)
+        return t.value
+
+    def wait(self, ticket: int, timeout_s: float = 0.0):
+        """(image, info dict); raises SvdiError when the request failed."""
+        info = RequestInfo()
+        st = lib().svdi_server_wait(self._h, ctypes.c_uint64(ticket), float(timeout_s), ctypes.byref(info))
+        _, _, out = self._pending.pop(ticket, (None, None, None))
+        _check(st)
+        return out, info.as_dict()
+
+    def stats(self) -> dict:
+        q, u, b, a = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_uint64()
+        _check(lib().svdi_server_stats(self._h, ctypes.byref(q), ctypes.byref(u), ctypes.byref(b),
+                                       ctypes.byref(a)))
+        return {"queued": q.value, "hbm_in_use": u.value, "hbm_budget": b.value, "admitted": a.value}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().svdi_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def bin_samples_noalloc(d_bin: int, d_vis_real: int, d_vis_imag: int, num_samples: int,

@@ -7,10 +7,19 @@
 // bounding box to the moment planes with 8-byte vector reductions (red.global.add.v2.f32) --
 // one per cell, instead of one per sample-cell.
 //
+// Accumulation is 32-bit fixed point: on sm_100a a float atomicAdd to shared memory executes as a
+// load + compare-and-swap loop (~3 clk per warp instruction, ~6 under inter-warp overlap, measured),
+// whereas red.shared.add.u32 is native (~1 clk). Each tile segment holds <= 512 samples and gets
+// the scale 0.999 * 2^(22 - e) (max|v| < 2^e), so every contribution stays below 2^22 and no cell
+// can overflow (512 * 2^22 = 2^31); each contribution is rounded to an integer by one FMA against
+// 1.5 * 2^23. The quantisation step is <= 2^-21 max|v| of the segment. Integer sums are
+// order-independent, so a tile segment's contribution is deterministic.
+//
 // Inner loop: one warp per sample. Lanes 0..W-1 evaluate the W x-weights and lanes W..2W-1 the
 // W y-weights from a piecewise polynomial of the ES kernel (degree kPolyDeg in the fractional
-// grid position, FP32 Horner); lane (a, b) then owns footprint cells (a + p * 32/W, b), whose
-// shared-memory addresses are bank-conflict free because the row stride is == W (mod 32).
+// grid position, FP32 Horner), two samples per polynomial pass when 2W <= 16; lane (a, b) then
+// owns footprint cells (a + p * 32/W, b), whose shared-memory addresses are bank-conflict free
+// because the row stride is == W (mod 32).
 #include "svdi_internal.cuh"
 
 #include <cmath>
@@ -27,6 +36,14 @@ constexpr int kWarps = kThreads / 32;
 __device__ __forceinline__ float es_exact(float beta, float x) {
     if (fabsf(x) > 1.0f) return 0.0f;
     return expf(-beta * x * x / (1.0f + sqrtf((1.0f - x) * (1.0f + x))));
+}
+
+// Round-to-nearest integer of x for |x| < 2^22: fmaf(a, b, kMagic) rounds a*b + 1.5 2^23 once into
+// [2^23, 2^24), whose ulp is 1, and the low mantissa bits are then the integer.
+constexpr float kMagic = 12582912.0f;   // 1.5 * 2^23
+constexpr int kMagicBits = 0x4B400000;  // bit pattern of kMagic
+__device__ __forceinline__ int fx_round(float x_plus_magic) {
+    return __float_as_int(x_plus_magic) - kMagicBits;
 }
 
 __device__ __forceinline__ void red_add_v2(float2* addr, float a, float b) {
@@ -48,7 +65,8 @@ __global__ void __launch_bounds__(kThreads) k_grid_fp32(
     const unsigned int* __restrict__ offsets, int key_lo, int key_hi, int slab_lo, GridGeom g,
     SlabParams sp, EsPoly poly, float2* __restrict__ planes, int term0, unsigned int chunk) {
     using C = TileCfg<W, T, KC>;
-    extern __shared__ float tile[];  // [KC][2][R][RS]
+    extern __shared__ int tile[];    // [KC][2][R][RS] 32-bit fixed-point accumulators
+    __shared__ unsigned int seg_max; // max |v| of the segment (float bits; non-negative)
     __shared__ int bbox[4];          // row min, row max, col min, col max
     __shared__ int seg_key;
     // per-warp staging of the decoded batch: {u_x, u_y, vre, vim} and {fast-path base, s}
@@ -71,7 +89,7 @@ __global__ void __launch_bounds__(kThreads) k_grid_fp32(
 #pragma unroll
     for (int d = 0; d <= kPolyDeg; ++d) coef[d] = poly.c[piece][d];
 
-    for (int i = threadIdx.x; i < KC * 2 * C::PLANE; i += kThreads) tile[i] = 0.0f;
+    for (int i = threadIdx.x; i < KC * 2 * C::PLANE; i += kThreads) tile[i] = 0;
     if (threadIdx.x == 0) {
         bbox[0] = C::R; bbox[1] = -1; bbox[2] = C::R; bbox[3] = -1;
     }
@@ -102,6 +120,32 @@ __global__ void __launch_bounds__(kThreads) k_grid_fp32(
             if (s_beg < s_end) {
                 const int slab = key / tiles2;
                 const int t1 = (key / g.ntile) % g.ntile, t2 = key % g.ntile;
+                // Fixed-point scale of the segment: 0.999 * 2^(22 - e) with max|v| < 2^e, so every
+                // contribution (|psi psi T_n| <= 1 up to the polynomial's 1e-7) stays inside the
+                // exact-rounding range |x| < 2^22 and the <= 512 samples of a segment cannot
+                // overflow a 32-bit cell (512 * 2^22 = 2^31).
+                if (threadIdx.x == 0) seg_max = 0u;
+                __syncthreads();
+                {
+                    float m = 0.0f;
+                    for (unsigned int k = s_beg + threadIdx.x; k < s_end; k += kThreads) {
+                        const SampleRec q = rec[k];
+                        m = fmaxf(m, fmaxf(fabsf(q.vre), fabsf(q.vim)));
+                    }
+                    const unsigned int mb = __reduce_max_sync(0xffffffffu, __float_as_uint(m));
+                    if (lane == 0) atomicMax(&seg_max, mb);
+                }
+                __syncthreads();
+                float scale = 0.0f, inv_scale = 0.0f;
+                {
+                    const float vmax = __uint_as_float(seg_max);
+                    if (vmax > 0.0f && vmax < 3.0e38f) {
+                        int ex;
+                        frexpf(vmax, &ex);  // vmax = f 2^ex, f in [0.5, 1)
+                        scale = ldexpf(0.999f, 22 - ex);
+                        inv_scale = 1.0f / scale;
+                    }
+                }
                 for (unsigned int b0 = s_beg + warp * 32; b0 < s_end; b0 += kWarps * 32) {
                     // ---- decode this lane's record once per batch
                     const unsigned int my = b0 + lane;
@@ -118,7 +162,7 @@ __global__ void __launch_bounds__(kThreads) k_grid_fp32(
                     const bool rare = valid && (fxq == 0 || fyq == 0 || r0 < 0 || c0 < 0);
                     st_f[warp][lane] = make_float4(fmaf(2.0f, (float)fxq * (1.0f / 16777216.0f), -1.0f),
                                                    fmaf(2.0f, (float)fyq * (1.0f / 16777216.0f), -1.0f),
-                                                   r.vre, r.vim);
+                                                   r.vre * scale, r.vim * scale);
                     st_i[warp][lane] = make_int2(r0 * C::RS + c0, __float_as_int(sv));
                     // bounding box of the batch (one warp reduction per 32 samples)
                     const int rlo = valid ? max(0, fxq ? r0 : r0 - 1) : C::R;
@@ -172,12 +216,18 @@ __global__ void __launch_bounds__(kThreads) k_grid_fp32(
                                 const float wx = __shfl_sync(0xffffffffu, w, src + (i < W ? i : 0));
                                 if (lane_cell && i < W) {
                                     const float kv = wx * wy;
-                                    const float ar = kv * sf.z, ai = kv * sf.w;
+                                    int* pl = tile + base + p * RPP * C::RS;
+                                    if (!need_s) {
+                                        atomicAdd(pl, fx_round(fmaf(kv, sf.z, kMagic)));
+                                        atomicAdd(pl + C::PLANE, fx_round(fmaf(kv, sf.w, kMagic)));
+                                    } else {
+                                        const float ar = kv * sf.z, ai = kv * sf.w;
 #pragma unroll
-                                    for (int t = 0; t < KC; ++t) {
-                                        float* pl = tile + (size_t)t * 2 * C::PLANE + base + p * RPP * C::RS;
-                                        atomicAdd(pl, ar * tv[t]);
-                                        atomicAdd(pl + C::PLANE, ai * tv[t]);
+                                        for (int t = 0; t < KC; ++t) {
+                                            atomicAdd(pl + (size_t)t * 2 * C::PLANE, fx_round(fmaf(ar, tv[t], kMagic)));
+                                            atomicAdd(pl + (size_t)t * 2 * C::PLANE + C::PLANE,
+                                                      fx_round(fmaf(ai, tv[t], kMagic)));
+                                        }
                                     }
                                 }
                             }
@@ -211,11 +261,11 @@ __global__ void __launch_bounds__(kThreads) k_grid_fp32(
                             const float x = ((float)(lo_r + i - rcx) - px) / (float)HW;
                             const float y = ((float)(lo_c + jj - rcy) - py) / (float)HW;
                             const float kv = es_exact(poly.beta, x) * es_exact(poly.beta, y);
-                            const float ar = kv * rr_.vre, ai = kv * rr_.vim;
+                            const float ar = kv * (rr_.vre * scale), ai = kv * (rr_.vim * scale);
                             for (int t = 0; t < KC; ++t) {
-                                float* pl = tile + (size_t)t * 2 * C::PLANE + rr * C::RS + cc;
-                                atomicAdd(pl, ar * tv[t]);
-                                atomicAdd(pl + C::PLANE, ai * tv[t]);
+                                int* pl = tile + (size_t)t * 2 * C::PLANE + rr * C::RS + cc;
+                                atomicAdd(pl, fx_round(fmaf(ar, tv[t], kMagic)));
+                                atomicAdd(pl + C::PLANE, fx_round(fmaf(ai, tv[t], kMagic)));
                             }
                         }
                     }
@@ -238,14 +288,15 @@ __global__ void __launch_bounds__(kThreads) k_grid_fp32(
                         const long long cell = (g1 - g.gmin) * g.G + (g2 - g.gmin);
 #pragma unroll
                         for (int t = 0; t < KC; ++t) {
-                            float* pl = tile + (size_t)t * 2 * C::PLANE + rr * C::RS + cc;
-                            const float re = pl[0], im = pl[C::PLANE];
-                            if (on_grid && (re != 0.0f || im != 0.0f)) {
+                            int* pl = tile + (size_t)t * 2 * C::PLANE + rr * C::RS + cc;
+                            const int ire = pl[0], iim = pl[C::PLANE];
+                            if (on_grid && (ire | iim)) {
                                 const long long plane = (long long)(slab - slab_lo) * sp.K + term0 + t;
-                                red_add_v2(planes + plane * GG + cell, sgn * re, sgn * im);
+                                const float s = sgn * inv_scale;
+                                red_add_v2(planes + plane * GG + cell, s * (float)ire, s * (float)iim);
                             }
-                            pl[0] = 0.0f;
-                            pl[C::PLANE] = 0.0f;
+                            pl[0] = 0;
+                            pl[C::PLANE] = 0;
                         }
                     }
                 }
@@ -284,7 +335,7 @@ template <int W>
 int launch_w(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d_offsets, int key_lo,
              int key_hi, int slab_lo, const GridGeom& g, const SlabParams& sp, const EsPoly& poly,
              float2* d_planes, int sm_count, cudaStream_t st) {
-    const unsigned int chunk = 4096;
+    const unsigned int chunk = 512;  // <= 512 samples per tile segment: no 32-bit overflow
     if (g.T == 64) {
         for (int t0 = 0; t0 < sp.K; ++t0)
             SVDI_TRY((launch_variant<W, 64, 1>(d_rec, d_rec_s, d_offsets, key_lo, key_hi, slab_lo, g, sp,

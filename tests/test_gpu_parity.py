@@ -18,6 +18,9 @@ from tests.conftest import snapshot
 pytestmark = pytest.mark.gpu
 
 IMG_TOL = 1e-5
+# Grid planes against the FP64 oracle grid: FP32 ES weights (polynomial, <= 1e-7) and the tile
+# accumulator's fixed-point step (<= 2^-21 of the tile segment's max |v| per contribution).
+GRID_TOL = 4e-6
 
 
 def _scale(cell, G):
@@ -101,7 +104,7 @@ def test_grid_planes_match_oracle(small_run):
         num = np.linalg.norm(grid[p] - og[p])
         den = np.linalg.norm(og[p])
         if den > 0:
-            assert num / den < 2e-6, (p, num / den)
+            assert num / den < GRID_TOL, (p, num / den)
 
 
 def test_main_path_image_matches_oracle(small_run):
@@ -281,7 +284,7 @@ def test_edge_clipping_and_integer_positions(cuda_device):
     o = O.image_fipk(visr, visi, b, v, N, cell, coord_mode=1)
     inv_det = 1.0 / abs(0.8 * 0.8 + 0.6 * 0.6)
     og = O.grid(b.astype(np.float64), visr, visi, scale, G, o.sc, inv_det, coord_mode=1)
-    assert np.linalg.norm(grid - og) / np.linalg.norm(og) < 2e-6
+    assert np.linalg.norm(grid - og) / np.linalg.norm(og) < GRID_TOL
     assert O.rel_rms(img, o.image) < IMG_TOL
 
 
