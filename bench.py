@@ -112,7 +112,7 @@ def dist_init():
     return replicas.init_from_env("nccl", timeout_s=120)
 
 
-def serving_phase(api, big, n_requests, rate, device, seed=5):
+def serving_phase(api, big, n_requests, rate, device, seed=5, gridder=0):
     """Poisson stream (rate/s) of mixed requests through a 4-slot server: the 512-station
     headline snapshot at 2048^2, a 256-station 32-channel snapshot at 1024^2 and a 128-station
     16-channel snapshot at 512^2. Returns latency percentiles and sustained throughput."""
@@ -128,7 +128,7 @@ def serving_phase(api, big, n_requests, rate, device, seed=5):
     rng = np.random.default_rng(seed)
     lat, queue, run = [], [], []
     with api.Server(num_slots=4, device=device, edge_mode=api.EDGE_STRICT, k_rule=api.KRULE_TARGET,
-                    target_error=1e-6) as srv:
+                    target_error=1e-6, gridder=gridder) as srv:
         for s, N, cell in mix:  # warm every slot's plans and buffers
             for t in [srv.submit(s, N, cell) for _ in range(4)]:
                 srv.wait(t, 120)
@@ -180,7 +180,9 @@ def run_ours(args):
     dev = torch.device("cuda", local)
     snap = make_workload(args.config, rank)
     N, cell = snap.image_size, snap.cell_size
-    opts = dict(device=local, edge_mode=api.EDGE_STRICT, k_rule=api.KRULE_TARGET, target_error=1e-6)
+    gridder = api.GRIDDER_TC if args.gridder == "tc" else api.GRIDDER_FP32
+    opts = dict(device=local, edge_mode=api.EDGE_STRICT, k_rule=api.KRULE_TARGET, target_error=1e-6,
+                gridder=gridder)
     eng = api.Engine(**opts)
     # device-resident inputs
     host = {k: np.ascontiguousarray(v) for k, v in snap.arrays().items()}
@@ -242,7 +244,8 @@ def run_ours(args):
         e2e_lat.append((time.perf_counter() - t1) * 1e3)
     e2e_s = replicas.max_over_ranks(time.perf_counter() - t0, dist, dev)
     e2e_value = replicas.aggregate_rate(args.steps, ws, e2e_s)
-    serving = None if args.no_serving else serving_phase(api, snap, args.serving_requests, 50.0, local)
+    serving = None if args.no_serving else serving_phase(api, snap, args.serving_requests, 50.0, local,
+                                                         gridder=gridder)
     h2d = int(sum(v.nbytes for v in host.values()))
     d2h = int(N * N * 4)
 
@@ -261,7 +264,7 @@ def run_ours(args):
     dom = max(ours, key=ours.get)
     if dom == "ms_grid":
         alg = grid_kernel_bytes(st["num_gridded"], planes, G)
-        name = "k_grid_fp32 (+ plane zeroing)"
+        name = ("k_grid_tc" if st["used_tc"] else "k_grid_fp32") + " (+ plane zeroing)"
     elif dom == "ms_bin":
         alg = (26 + 8) * snap.num_samples + 16 * st["num_gridded"]
         name = "k_histogram + k_scan + k_scatter"
@@ -292,11 +295,12 @@ def run_ours(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32",
+        "dtype": "f16 hi+lo operands, f32 accumulation" if st["used_tc"] else "f32",
         "data": "synthetic (seeded; 512-station layout, 220-source sky, noise, flags, weights)",
         "config": {
             "workload": f"{args.config}: {snap.num_rows} baselines x {snap.num_channels} channels = "
                         f"{snap.num_samples} vis, one snapshot, {N}^2 image, cell {cell} rad",
+            "gridder": "tcgen05 split-precision" if st["used_tc"] else "fp32 fixed-point",
             "grid": G, "planes": planes, "num_slabs": st["num_slabs"], "chebyshev_terms": st["num_terms"],
             "support": 8, "beta": 15.3704324328, "oversampling": 1.5, "tile": st["tile"],
             "k_rule": "target 1e-6", "edges": "strict (samples whose footprint leaves the grid are dropped)",
@@ -338,7 +342,7 @@ def cpu_baseline(snap, eng, api, st, args):
     from oracle import oracle as O
     N, cell = snap.image_size, snap.cell_size
     with api.Engine(device=eng.options.device, edge_mode=api.EDGE_STRICT, k_rule=api.KRULE_TARGET,
-                    target_error=1e-6, presplat=1) as e2:
+                    target_error=1e-6, presplat=1, gridder=eng.options.gridder) as e2:
         R = e2.image(snap)
         vr, vi = e2.buffer(api.BUF_VIS_REAL), e2.buffer(api.BUF_VIS_IMAG)
         q, sv = e2.buffer(api.BUF_Q).reshape(-1, 3), e2.buffer(api.BUF_S)
@@ -440,6 +444,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=150)
+    ap.add_argument("--gridder", default="fp32", choices=["tc", "fp32"],
+                    help="tc: split-precision tcgen05 gridder; fp32: CUDA-core fixed-point gridder")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -181,7 +181,9 @@ typedef struct svdi_stats {
     double alpha_max;            /* 2 pi max|t3| (r3 range / 2)                                */
     double slab_alpha_max;
     double vin[9];               /* FP64 basis used                                            */
-    int tile;                    /* gridder tile side T                                        */
+    int tile;                    /* gridder tile rows                                          */
+    int tile_cols;               /* gridder tile columns                                       */
+    int used_tc;                 /* 1 when the tensor-core gridder ran                         */
     int num_keys;                /* tile keys: num_slabs * ceil(G/T)^2                         */
     double slab_r3_min, slab_width, slab_half;  /* slab geometry used by the gridder           */
     float ms_total;              /* device time of the call (CUDA events)                      */

@@ -257,14 +257,15 @@ static void orc_slab(double r3, int nslab, double r3_min, double slab_width, dou
 /* Tile binning keys. For every sample: the grid position p = r * scale (FP64, scale =        */
 /* cell_size * G, or the reference's FP32 rounding), its clipped footprint origin (lo1, lo2),  */
 /* and the key                                                                                  */
-/*   key = (slab * ntile + (lo1 + G/2) / T) * ntile + (lo2 + G/2) / T,  ntile = ceil(G / T)   */
+/*   key = (slab * ntile + (lo1 + G/2) / T) * ntile2 + (lo2 + G/2) / T2,  ntile = ceil(G / T)  */
+/* (square tiles: T2 = T, ntile2 = ntile; the tensor-core gridder uses tall narrow tiles)      */
 /* or -1 when the sample touches no cell. xq/yq (optional) receive the record coordinates of   */
 /* the B200 path: Q - (tile origin) * 2^24 with Q = floor(p 2^24). This is the binning         */
 /* contract of the B200 path (bit-exact); the reference grids unsorted (SII:1218-1293).         */
 /* ------------------------------------------------------------------------------------------ */
 void orc_tile_keys(long n, const double* r, double scale, int coord_mode, long G, int W, int T,
-                   int edge_mode, int nslab, double r3_min, double slab_width, double inv_half,
-                   int64_t* keys, int32_t* xq, int32_t* yq, float* sarg) {
+                   int T2, long ntile2, int edge_mode, int nslab, double r3_min, double slab_width,
+                   double inv_half, int64_t* keys, int32_t* xq, int32_t* yq, float* sarg) {
     const long ntile = (G + T - 1) / T;
     const long gmin = -(G / 2);
     for (long k = 0; k < n; ++k) {
@@ -280,10 +281,10 @@ void orc_tile_keys(long n, const double* r, double scale, int coord_mode, long G
         int slab;
         double s;
         orc_slab(r[k * 3 + 2], nslab, r3_min, slab_width, inv_half, &slab, &s);
-        const long t1 = (a1 - gmin) / T, t2 = (a2 - gmin) / T;
-        keys[k] = ((int64_t)slab * ntile + t1) * ntile + t2;
+        const long t1 = (a1 - gmin) / T, t2 = (a2 - gmin) / T2;
+        keys[k] = ((int64_t)slab * ntile + t1) * ntile2 + t2;
         if (xq) xq[k] = (int32_t)((long long)floor(p1 * 16777216.0) - (gmin + t1 * T) * 16777216LL);
-        if (yq) yq[k] = (int32_t)((long long)floor(p2 * 16777216.0) - (gmin + t2 * T) * 16777216LL);
+        if (yq) yq[k] = (int32_t)((long long)floor(p2 * 16777216.0) - (gmin + t2 * T2) * 16777216LL);
         if (sarg) sarg[k] = (float)s;
     }
 }

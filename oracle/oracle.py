@@ -53,7 +53,7 @@ def lib():
         L.orc_es.restype = d
         L.orc_es.argtypes = [d, d]
         L.orc_es_correction.argtypes = [l, l, i, d, P]
-        L.orc_tile_keys.argtypes = [l, P, d, i, l, i, i, i, i, d, d, d, P, P, P, P]
+        L.orc_tile_keys.argtypes = [l, P, d, i, l, i, i, i, l, i, i, d, d, d, P, P, P, P]
         L.orc_grid.argtypes = [l, P, P, P, d, i, l, i, d, i, i, d, d, d, d, i, P]
         L.orc_bessel_j.argtypes = [d, i, P]
         L.orc_bessel_series_f32.argtypes = [f, i, P]
@@ -199,16 +199,20 @@ def es_correction(N, G, W=REF_SUPPORT, beta=REF_BETA):
     return phi
 
 
-def tile_keys(r, scale, G, W, T, edge_mode, sc: SlabConfig, coord_mode=0, records=False):
+def tile_keys(r, scale, G, W, T, edge_mode, sc: SlabConfig, coord_mode=0, records=False,
+              T2=None, ntile2=None):
     """Per-sample tile key (-1 = dropped); with records=True also the record coordinates
-    (xq, yq) and the Chebyshev argument of the B200 binning contract."""
+    (xq, yq) and the Chebyshev argument of the B200 binning contract. Tiles are T rows by
+    T2 columns (default square) with ntile2 tile columns per tile row (default ceil(G / T2))."""
     n = r.shape[0]
+    T2 = T if T2 is None else T2
+    ntile2 = (G + T2 - 1) // T2 if ntile2 is None else ntile2
     keys = np.empty(n, np.int64)
     xq = np.zeros(n, np.int32) if records else None
     yq = np.zeros(n, np.int32) if records else None
     sa = np.zeros(n, np.float32) if records else None
     lib().orc_tile_keys(n, _p(_c(r, np.float64)), float(scale), coord_mode, G, W, T,
-                        edge_mode, sc.num_slabs, sc.r3_min, sc.slab_width, sc.inv_half, _p(keys),
+                        T2, ntile2, edge_mode, sc.num_slabs, sc.r3_min, sc.slab_width, sc.inv_half, _p(keys),
                         _p(xq), _p(yq), _p(sa))
     return (keys, xq, yq, sa) if records else keys
 

@@ -96,7 +96,8 @@ class Stats(ctypes.Structure):
         ("num_planes", ctypes.c_int), ("r3_min", ctypes.c_double), ("r3_max", ctypes.c_double),
         ("max_abs_t3", ctypes.c_double), ("valid_pixels", ctypes.c_size_t),
         ("alpha_max", ctypes.c_double), ("slab_alpha_max", ctypes.c_double),
-        ("vin", ctypes.c_double * 9), ("tile", ctypes.c_int), ("num_keys", ctypes.c_int),
+        ("vin", ctypes.c_double * 9), ("tile", ctypes.c_int), ("tile_cols", ctypes.c_int),
+        ("used_tc", ctypes.c_int), ("num_keys", ctypes.c_int),
         ("slab_r3_min", ctypes.c_double), ("slab_width", ctypes.c_double),
         ("slab_half", ctypes.c_double), ("ms_total", ctypes.c_float),
         ("ms_preprocess", ctypes.c_float), ("ms_bin", ctypes.c_float), ("ms_grid", ctypes.c_float),

@@ -11,8 +11,9 @@
 //   lo     = frac ? cell - (W/2 - 1) : cell - W/2   (= ceil(p - W/2)),  hi = cell + W/2
 //   clip   lo, hi to [-G/2, (G-1)/2] (SVDIntegratedImager.cu:1261-1267); drop if lo > hi
 //          (strict mode: drop if the footprint leaves the grid)
-//   tile   = (lo + G/2) / T  per axis;  slab = clamp(floor((r3 - r3_min) / width), 0, nslab-1)
-//   key    = (slab * ntile + tile1) * ntile + tile2
+//   tile1  = (lo1 + G/2) / T1, tile2 = (lo2 + G/2) / T2 (tiles may be rectangular)
+//   slab   = clamp(floor((r3 - r3_min) / width), 0, nslab - 1)
+//   key    = (slab * ntile1 + tile1) * ntile2 + tile2
 #include "svdi_internal.cuh"
 
 namespace svdi {
@@ -30,7 +31,7 @@ struct KeyRec {
     float s;
 };
 
-__device__ inline bool quantise_axis(double p, const GridGeom& g, int& tile, int& qrel) {
+__device__ inline bool quantise_axis(double p, const GridGeom& g, int T, int& tile, int& qrel) {
     if (!(fabs(p) < 1e15)) return false;
     const long long Q = (long long)floor(p * 16777216.0);
     const long long cell = Q >> 24;
@@ -45,8 +46,8 @@ __device__ inline bool quantise_axis(double p, const GridGeom& g, int& tile, int
         if (hi > g.gmax) hi = g.gmax;
         if (lo > hi) return false;
     }
-    tile = (int)((lo - g.gmin) / g.T);
-    const long long origin = g.gmin + (long long)tile * g.T;
+    tile = (int)((lo - g.gmin) / T);
+    const long long origin = g.gmin + (long long)tile * T;
     qrel = (int)(Q - origin * 16777216LL);
     return true;
 }
@@ -78,7 +79,7 @@ __device__ inline KeyRec sample_key(const SampleSource& src, long long idx, cons
     double r1, r2, r3;
     sample_coords(src, idx, r1, r2, r3);
     int t1, t2;
-    if (!quantise_axis(grid_pos(r1, g), g, t1, k.xq) || !quantise_axis(grid_pos(r2, g), g, t2, k.yq))
+    if (!quantise_axis(grid_pos(r1, g), g, g.T, t1, k.xq) || !quantise_axis(grid_pos(r2, g), g, g.T2, t2, k.yq))
         return k;
     int j = 0;
     double sv = 0.0;
@@ -92,7 +93,7 @@ __device__ inline KeyRec sample_key(const SampleSource& src, long long idx, cons
         sv = fmin(1.0, fmax(-1.0, sv));
     }
     k.s = (float)sv;
-    k.key = (j * g.ntile + t1) * g.ntile + t2;
+    k.key = (j * g.ntile + t1) * g.ntile2 + t2;
     return k;
 }
 
@@ -164,13 +165,15 @@ __global__ void __launch_bounds__(1024) k_scan(const unsigned int* __restrict__ 
 // Scatter: block-aggregated reservation of output ranges per key, then 16-byte record writes.
 __global__ void __launch_bounds__(kThreads) k_scatter(SampleSource src, GridGeom g, SlabParams sp,
                                                      unsigned int* __restrict__ cursor, int n_keys,
-                                                     SampleRec* __restrict__ rec, float* __restrict__ rec_s) {
+                                                     SampleRec* __restrict__ rec, float* __restrict__ rec_s,
+                                                     unsigned int* __restrict__ vmax) {
     extern __shared__ unsigned int sh[];  // [n_keys] counts, then [n_keys] bases
     unsigned int* cnt = sh;
     unsigned int* base = sh + n_keys;
     const bool use_smem = n_keys <= kSmemKeyLimit / 2;
     const int lane = threadIdx.x & 31;
     const long long n = src.n;
+    float vm = 0.0f;  // max |record value| written by this thread
     for (long long c0 = (long long)blockIdx.x * kChunk; c0 < n; c0 += (long long)gridDim.x * kChunk) {
         KeyRec kr[kPerThread];
         unsigned int rank[kPerThread];
@@ -214,8 +217,13 @@ __global__ void __launch_bounds__(kThreads) k_scatter(SampleSource src, GridGeom
             r.vim = __fmul_rn(src.vi[idx], src.inv_det);
             rec[pos] = r;
             if (rec_s) rec_s[pos] = kr[i].s;
+            vm = fmaxf(vm, fmaxf(fabsf(r.vre), fabsf(r.vim)));
         }
         if (use_smem) __syncthreads();
+    }
+    if (vmax) {  // non-negative floats order like their bit patterns
+        const unsigned int mb = __reduce_max_sync(0xffffffffu, __float_as_uint(vm));
+        if (lane == 0 && mb) atomicMax(vmax, mb);
     }
 }
 
@@ -244,14 +252,14 @@ int launch_scan(const unsigned int* d_counts, int n_keys, unsigned int* d_offset
 
 int launch_scatter(const SampleSource& src, const GridGeom& g, const SlabParams& sp,
                    unsigned int* d_cursor, int n_keys, SampleRec* d_rec, float* d_rec_s,
-                   cudaStream_t st) {
+                   unsigned int* d_vmax, cudaStream_t st) {
     const size_t smem = n_keys <= kSmemKeyLimit / 2 ? (size_t)n_keys * 8 : 0;
     if (smem > 48 * 1024)
         SVDI_CUDA(cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     long long blocks = (src.n + kChunk - 1) / kChunk;
     if (blocks > 148 * 16) blocks = 148 * 16;
     if (blocks < 1) blocks = 1;
-    k_scatter<<<(int)blocks, kThreads, smem, st>>>(src, g, sp, d_cursor, n_keys, d_rec, d_rec_s);
+    k_scatter<<<(int)blocks, kThreads, smem, st>>>(src, g, sp, d_cursor, n_keys, d_rec, d_rec_s, d_vmax);
     SVDI_LAUNCHED();
     return SVDI_OK;
 }

@@ -105,7 +105,7 @@ struct svdi_engine {
     svdi::DevBuf in_bin, in_vin;
     // intermediates
     svdi::DevBuf vr, vi, q, s, vin64, vin32, stats, partial, counts, offsets, cursor, dropped, rec,
-        rec_s, planes, corr, image, cheb_err, bin_out, grid_keep;
+        rec_s, planes, corr, image, cheb_err, bin_out, grid_keep, tc_status;
     size_t sz_vr = 0, sz_q = 0, sz_s = 0, sz_off = 0, sz_rec = 0, sz_rec_s = 0, sz_grid = 0, sz_mom = 0;
     const float* cur_vr = nullptr;
     const float* cur_vi = nullptr;
@@ -403,13 +403,26 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     g.gmin = -(g.G / 2);
     g.gmax = (g.G - 1) / 2;
     g.W = o.support;
-    g.T = o.tile ? o.tile : (sp.K == 1 ? 64 : 32);
-    g.ntile = (int)((g.G + g.T - 1) / g.T);
+    // the tensor-core gridder accumulates one moment plane per CTA in TMEM (K == 1) and bins
+    // into 120 x 8 tiles, four of which share a 128-row accumulator (gridder_tc.cu)
+    const bool use_tc = o.gridder == SVDI_GRIDDER_TC && sp.K == 1 && g.W <= 8;
+    if (use_tc) {
+        g.T = kTcTileRows;
+        g.ntile = (int)((g.G + g.T - 1) / g.T);
+        g.T2 = kTcTileCols;
+        g.ntile2 = (int)((g.G + g.T2 - 1) / g.T2);
+        g.ntile2 = (g.ntile2 + kTcBlocks - 1) / kTcBlocks * kTcBlocks;
+    } else {
+        g.T = o.tile ? o.tile : (sp.K == 1 ? 64 : 32);
+        g.ntile = (int)((g.G + g.T - 1) / g.T);
+        g.T2 = g.T;
+        g.ntile2 = g.ntile;
+    }
     g.edge_mode = o.edge_mode;
     g.coord_mode = o.coord_mode;
     g.scale = cell * (double)g.G;
     g.scale32 = cell_f * (float)g.G;
-    const long long n_keys_ll = (long long)sp.nslab * g.ntile * g.ntile;
+    const long long n_keys_ll = (long long)sp.nslab * g.ntile * g.ntile2;
     if (n_keys_ll > (1LL << 26)) {
         set_error("too many tile keys");
         return SVDI_ERR_UNSUPPORTED;
@@ -437,8 +450,14 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
                               e->dropped.as<unsigned long long>(), st));
     SVDI_TRY(launch_scan(e->counts.as<unsigned int>(), n_keys, e->offsets.as<unsigned int>(),
                          e->cursor.as<unsigned int>(), st));
+    // tensor-core gridder: [0] give-up status, [1] max |record value| (float bits) from the scatter
+    if (use_tc) {
+        SVDI_TRY(e->tc_status.ensure(4 * sizeof(unsigned int)));
+        SVDI_CUDA(cudaMemsetAsync(e->tc_status.p, 0, 4 * sizeof(unsigned int), st));
+    }
     SVDI_TRY(launch_scatter(src, g, sp, e->cursor.as<unsigned int>(), n_keys, e->rec.as<SampleRec>(),
-                            need_s ? e->rec_s.as<float>() : nullptr, st));
+                            need_s ? e->rec_s.as<float>() : nullptr,
+                            use_tc ? e->tc_status.as<unsigned int>() + 1 : nullptr, st));
     SVDI_CUDA(cudaEventRecord(e->ev[2], st));
 
     // slab batches: grid -> FFT -> recombine
@@ -456,10 +475,17 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
         SlabParams bp = sp;
         SVDI_CUDA(cudaEventRecord(e->ev[3], st));
         SVDI_CUDA(cudaMemsetAsync(e->planes.p, 0, plane_bytes * planes_per_batch, st));
-        const int tiles2 = g.ntile * g.ntile;
-        SVDI_TRY(launch_grid_fp32(e->rec.as<SampleRec>(), need_s ? e->rec_s.as<float>() : nullptr,
-                                  e->offsets.as<unsigned int>(), n_keys, s0 * tiles2, s1 * tiles2, s0, g, sp,
-                                  e->poly, e->planes.as<float2>(), e->sm_count, st));
+        const int tiles2 = g.ntile * g.ntile2;
+        if (use_tc) {
+            SVDI_TRY(launch_grid_tc(e->rec.as<SampleRec>(), e->offsets.as<unsigned int>(), n_keys, s0 * tiles2,
+                                    s1 * tiles2, s0, g, e->poly, e->planes.as<float2>(),
+                                    e->tc_status.as<unsigned int>() + 1, e->tc_status.as<unsigned int>(),
+                                    e->sm_count, st));
+        } else {
+            SVDI_TRY(launch_grid_fp32(e->rec.as<SampleRec>(), need_s ? e->rec_s.as<float>() : nullptr,
+                                      e->offsets.as<unsigned int>(), n_keys, s0 * tiles2, s1 * tiles2, s0, g,
+                                      sp, e->poly, e->planes.as<float2>(), e->sm_count, st));
+        }
         if (o.keep_grid && s0 == 0) {
             SVDI_TRY(e->grid_keep.ensure(plane_bytes * planes_per_batch));
             SVDI_CUDA(cudaMemcpyAsync(e->grid_keep.p, e->planes.p, plane_bytes * planes_per_batch,
@@ -486,8 +512,15 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
         ms_img += c;
     }
     unsigned long long ndrop = 0;
+    unsigned int tc_status = 0;
     SVDI_CUDA(cudaMemcpyAsync(&ndrop, e->dropped.p, 8, cudaMemcpyDeviceToHost, st));
+    if (use_tc) SVDI_CUDA(cudaMemcpyAsync(&tc_status, e->tc_status.p, 4, cudaMemcpyDeviceToHost, st));
     SVDI_CUDA(cudaStreamSynchronize(st));
+    if (tc_status != 0) {
+        set_error("tensor-core gridder gave up waiting for an MMA completion (status " +
+                  std::to_string(tc_status) + "); the grid is incomplete");
+        return SVDI_ERR_INTERNAL;
+    }
 
     e->sz_off = (size_t)(n_keys + 1) * 4;
     e->sz_rec = (size_t)(n - (long long)ndrop) * sizeof(SampleRec);
@@ -500,6 +533,8 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     e->cur_s = src.s;
     svdi_stats& L = e->last;
     L.tile = g.T;
+    L.tile_cols = g.T2;
+    L.used_tc = use_tc ? 1 : 0;
     L.num_keys = n_keys;
     L.slab_r3_min = sp.r3_min;
     L.slab_width = sp.slab_width;

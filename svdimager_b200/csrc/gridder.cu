@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(kThreads) k_grid_fp32(
     const unsigned int rec_lo = offsets[key_lo], rec_hi = offsets[key_hi];
     const unsigned int n_chunks = (rec_hi - rec_lo + chunk - 1) / chunk;
     const long long GG = g.G * g.G;
-    const int tiles2 = g.ntile * g.ntile;
+    const int tiles2 = g.ntile * g.ntile2;
     const bool need_s = !(KC == 1 && term0 == 0);
 
     for (unsigned int ch = blockIdx.x; ch < n_chunks; ch += gridDim.x) {
@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(kThreads) k_grid_fp32(
             const unsigned int s_end = min(c_end, offsets[key + 1]);
             if (s_beg < s_end) {
                 const int slab = key / tiles2;
-                const int t1 = (key / g.ntile) % g.ntile, t2 = key % g.ntile;
+                const int t1 = (key / g.ntile2) % g.ntile, t2 = key % g.ntile2;
                 // Fixed-point scale of the segment: 0.999 * 2^(22 - e) with max|v| < 2^e, so every
                 // contribution (|psi psi T_n| <= 1 up to the polynomial's 1e-7) stays inside the
                 // exact-rounding range |x| < 2^22 and the <= 512 samples of a segment cannot

@@ -76,6 +76,8 @@ extern "C" int svdi_bin_samples_noalloc(const float* d_bin, const float* d_vis_r
     g.W = 8;
     g.T = tile;
     g.ntile = (int)((g.G + g.T - 1) / g.T);
+    g.T2 = tile;
+    g.ntile2 = g.ntile;
     g.edge_mode = SVDI_EDGE_CLIP;
     g.coord_mode = SVDI_COORD_FP64;
     g.scale = (double)cell_size * (double)g.G;
@@ -114,6 +116,6 @@ extern "C" int svdi_bin_samples_noalloc(const float* d_bin, const float* d_vis_r
     SVDI_CUDA(cudaMemsetAsync(dropped, 0, sizeof(unsigned long long), st));
     SVDI_TRY(launch_histogram(src, g, sp, counts, (int)n_keys, dropped, st));
     SVDI_TRY(launch_scan(counts, (int)n_keys, d_offsets, cursor, st));
-    SVDI_TRY(launch_scatter(src, g, sp, cursor, (int)n_keys, static_cast<SampleRec*>(d_records), nullptr, st));
+    SVDI_TRY(launch_scatter(src, g, sp, cursor, (int)n_keys, static_cast<SampleRec*>(d_records), nullptr, nullptr, st));
     return SVDI_OK;
 }

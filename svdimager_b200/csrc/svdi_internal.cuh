@@ -35,8 +35,10 @@ struct GridGeom {
     long long G;          // grid side
     long long gmin, gmax; // first/last cell index relative to the centre: -G/2 .. (G-1)/2
     int W;                // ES support (even)
-    int T;                // tile side
+    int T;                // tile rows (first grid axis)
     int ntile;            // ceil(G / T)
+    int T2;               // tile columns (second grid axis)
+    int ntile2;           // tiles along the second axis (>= ceil(G / T2))
     int edge_mode;
     int coord_mode;
     double scale;         // cell_size * G  (grid position = r * scale)
@@ -131,9 +133,18 @@ int launch_histogram(const SampleSource& src, const GridGeom& g, const SlabParam
                      cudaStream_t st);
 int launch_scan(const unsigned int* d_counts, int n_keys, unsigned int* d_offsets,
                 unsigned int* d_cursor, cudaStream_t st);
+// d_vmax (optional, zeroed by the caller): receives max(|vre|, |vim|) over the records as float bits
 int launch_scatter(const SampleSource& src, const GridGeom& g, const SlabParams& sp,
                    unsigned int* d_cursor, int n_keys, SampleRec* d_rec, float* d_rec_s,
-                   cudaStream_t st);
+                   unsigned int* d_vmax, cudaStream_t st);
+
+// gridder_tc.cu: split-precision tcgen05 gridder (one moment plane, support <= 8)
+constexpr int kTcTileRows = 120;   // tile rows: footprint origins; 128-row accumulator with halo
+constexpr int kTcTileCols = 8;     // tile columns: footprint origins of one column block
+constexpr int kTcBlocks = 4;       // column blocks per super-tile accumulator (4 x 32 TMEM columns)
+int launch_grid_tc(const SampleRec* d_rec, const unsigned int* d_offsets, int n_keys, int key_lo,
+                   int key_hi, int slab_lo, const GridGeom& g, const EsPoly& poly, float2* d_planes,
+                   const unsigned int* d_vmax, unsigned int* d_status, int sm_count, cudaStream_t st);
 
 // gridder.cu
 int launch_grid_fp32(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d_offsets,

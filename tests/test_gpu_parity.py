@@ -59,9 +59,11 @@ def test_rotation_matches_oracle(small_run):
 
 
 def _check_binning(e, st, r, vr, vi, cell, coord_mode=0, edge_mode=0, W=8):
-    G, T = st["grid_size"], st["tile"]
+    G, T, T2 = st["grid_size"], st["tile"], st["tile_cols"]
     sc = _slab_config_from_stats(st)
-    keys, xq, yq, sa = O.tile_keys(r, _scale(cell, G), G, W, T, edge_mode, sc, coord_mode, records=True)
+    ntile2 = st["num_keys"] // (sc.num_slabs * ((G + T - 1) // T))
+    keys, xq, yq, sa = O.tile_keys(r, _scale(cell, G), G, W, T, edge_mode, sc, coord_mode, records=True,
+                                   T2=T2, ntile2=ntile2)
     n_keys = st["num_keys"]
     off = e.buffer(api.BUF_OFFSETS).astype(np.int64)
     kept = keys >= 0
