@@ -135,31 +135,50 @@ __global__ void __launch_bounds__(kThreads) k_histogram(SampleSource src, GridGe
     }
 }
 
-// Exclusive scan of the key counts (one block): offsets[0..n_keys], cursor = offsets.
+// Exclusive scan of the key counts (one block): offsets[0..n_keys], cursor = offsets. With
+// kb_offsets, also the exclusive scan of ceil(count / kb_size): the K-blocks of kb_size records of
+// one key each that the tensor-core gridder splits evenly over its CTAs.
 __global__ void __launch_bounds__(1024) k_scan(const unsigned int* __restrict__ counts, int n_keys,
                                               unsigned int* __restrict__ offsets,
-                                              unsigned int* __restrict__ cursor) {
+                                              unsigned int* __restrict__ cursor,
+                                              unsigned int* __restrict__ kb_offsets, int kb_size) {
     __shared__ unsigned int part[1024];
+    __shared__ unsigned int kpart[1024];
     const int t = threadIdx.x;
     const int per = (n_keys + 1023) / 1024;
     const int b = t * per, e = min(n_keys, b + per);
-    unsigned int s = 0;
-    for (int k = b; k < e; ++k) s += counts[k];
+    unsigned int s = 0, ks = 0;
+    for (int k = b; k < e; ++k) {
+        const unsigned int c = counts[k];
+        s += c;
+        ks += (c + kb_size - 1) / kb_size;
+    }
     part[t] = s;
+    kpart[t] = ks;
     __syncthreads();
     for (int off = 1; off < 1024; off <<= 1) {
-        unsigned int v = (t >= off) ? part[t - off] : 0u;
+        const unsigned int v = (t >= off) ? part[t - off] : 0u;
+        const unsigned int kv = (t >= off) ? kpart[t - off] : 0u;
         __syncthreads();
         part[t] += v;
+        kpart[t] += kv;
         __syncthreads();
     }
-    unsigned int run = part[t] - s;
+    unsigned int run = part[t] - s, krun = kpart[t] - ks;
     for (int k = b; k < e; ++k) {
+        const unsigned int c = counts[k];
         offsets[k] = run;
         cursor[k] = run;
-        run += counts[k];
+        run += c;
+        if (kb_offsets) {
+            kb_offsets[k] = krun;
+            krun += (c + kb_size - 1) / kb_size;
+        }
     }
-    if (t == 1023) offsets[n_keys] = part[1023];
+    if (t == 1023) {
+        offsets[n_keys] = part[1023];
+        if (kb_offsets) kb_offsets[n_keys] = kpart[1023];
+    }
 }
 
 // Scatter: block-aggregated reservation of output ranges per key, then 16-byte record writes.
@@ -233,8 +252,11 @@ int launch_histogram(const SampleSource& src, const GridGeom& g, const SlabParam
                      unsigned int* d_counts, int n_keys, unsigned long long* d_dropped,
                      cudaStream_t st) {
     const size_t smem = n_keys <= kSmemKeyLimit ? (size_t)n_keys * 4 : 0;
-    if (smem > 48 * 1024)
+    static size_t configured = 48 * 1024;  // the attribute is raised once, to the largest size used
+    if (smem > configured) {
         SVDI_CUDA(cudaFuncSetAttribute(k_histogram, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured = smem;
+    }
     long long blocks = (src.n + kThreads - 1) / kThreads;
     if (blocks > 148 * 8) blocks = 148 * 8;
     if (blocks < 1) blocks = 1;
@@ -244,8 +266,8 @@ int launch_histogram(const SampleSource& src, const GridGeom& g, const SlabParam
 }
 
 int launch_scan(const unsigned int* d_counts, int n_keys, unsigned int* d_offsets,
-                unsigned int* d_cursor, cudaStream_t st) {
-    k_scan<<<1, 1024, 0, st>>>(d_counts, n_keys, d_offsets, d_cursor);
+                unsigned int* d_cursor, cudaStream_t st, unsigned int* d_kb_offsets, int kb_size) {
+    k_scan<<<1, 1024, 0, st>>>(d_counts, n_keys, d_offsets, d_cursor, d_kb_offsets, kb_size);
     SVDI_LAUNCHED();
     return SVDI_OK;
 }
@@ -254,8 +276,11 @@ int launch_scatter(const SampleSource& src, const GridGeom& g, const SlabParams&
                    unsigned int* d_cursor, int n_keys, SampleRec* d_rec, float* d_rec_s,
                    unsigned int* d_vmax, cudaStream_t st) {
     const size_t smem = n_keys <= kSmemKeyLimit / 2 ? (size_t)n_keys * 8 : 0;
-    if (smem > 48 * 1024)
+    static size_t configured = 48 * 1024;  // the attribute is raised once, to the largest size used
+    if (smem > configured) {
         SVDI_CUDA(cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured = smem;
+    }
     long long blocks = (src.n + kChunk - 1) / kChunk;
     if (blocks > 148 * 16) blocks = 148 * 16;
     if (blocks < 1) blocks = 1;

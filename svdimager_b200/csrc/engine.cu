@@ -105,7 +105,7 @@ struct svdi_engine {
     svdi::DevBuf in_bin, in_vin;
     // intermediates
     svdi::DevBuf vr, vi, q, s, vin64, vin32, stats, partial, counts, offsets, cursor, dropped, rec,
-        rec_s, planes, corr, image, cheb_err, bin_out, grid_keep, tc_status;
+        rec_s, planes, corr, image, cheb_err, bin_out, grid_keep, tc_status, kb_offsets;
     size_t sz_vr = 0, sz_q = 0, sz_s = 0, sz_off = 0, sz_rec = 0, sz_rec_s = 0, sz_grid = 0, sz_mom = 0;
     const float* cur_vr = nullptr;
     const float* cur_vi = nullptr;
@@ -404,7 +404,7 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     g.gmax = (g.G - 1) / 2;
     g.W = o.support;
     // the tensor-core gridder accumulates one moment plane per CTA in TMEM (K == 1) and bins
-    // into 120 x 8 tiles, four of which share a 128-row accumulator (gridder_tc.cu)
+    // into 56 x 8 tiles, four of which share a 64-row accumulator (gridder_tc.cu)
     const bool use_tc = o.gridder == SVDI_GRIDDER_TC && sp.K == 1 && g.W <= 8;
     if (use_tc) {
         g.T = kTcTileRows;
@@ -448,8 +448,10 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     SVDI_CUDA(cudaMemsetAsync(e->dropped.p, 0, 8, st));
     SVDI_TRY(launch_histogram(src, g, sp, e->counts.as<unsigned int>(), n_keys,
                               e->dropped.as<unsigned long long>(), st));
+    if (use_tc) SVDI_TRY(e->kb_offsets.ensure((size_t)(n_keys + 1) * 4));
     SVDI_TRY(launch_scan(e->counts.as<unsigned int>(), n_keys, e->offsets.as<unsigned int>(),
-                         e->cursor.as<unsigned int>(), st));
+                         e->cursor.as<unsigned int>(), st,
+                         use_tc ? e->kb_offsets.as<unsigned int>() : nullptr, kTcKBlock));
     // tensor-core gridder: [0] give-up status, [1] max |record value| (float bits) from the scatter
     if (use_tc) {
         SVDI_TRY(e->tc_status.ensure(4 * sizeof(unsigned int)));
@@ -477,7 +479,8 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
         SVDI_CUDA(cudaMemsetAsync(e->planes.p, 0, plane_bytes * planes_per_batch, st));
         const int tiles2 = g.ntile * g.ntile2;
         if (use_tc) {
-            SVDI_TRY(launch_grid_tc(e->rec.as<SampleRec>(), e->offsets.as<unsigned int>(), n_keys, s0 * tiles2,
+            SVDI_TRY(launch_grid_tc(e->rec.as<SampleRec>(), e->offsets.as<unsigned int>(),
+                                    e->kb_offsets.as<unsigned int>(), n_keys, s0 * tiles2,
                                     s1 * tiles2, s0, g, e->poly, e->planes.as<float2>(),
                                     e->tc_status.as<unsigned int>() + 1, e->tc_status.as<unsigned int>(),
                                     e->sm_count, st));

@@ -5,34 +5,47 @@
 //
 // Gridding with a separable kernel is a sum of outer products. For the samples k of one tile,
 //   G[m][n] = sum_k  wx_k[m] * (wy_k[n] v_k)   =   (A B^T)[m][n],
-// where column k of A holds the ES weights of sample k on its W footprint rows and column k of B
-// its ES weights on its W footprint columns times the visibility (re and im as separate B rows).
-// Each K-block of 32 samples of one tile is written to shared memory as FP16 hi + lo pairs
+// where column k of A holds the ES weights of sample k on its footprint rows and column k of B its
+// ES weights on its footprint columns times the visibility (re and im as separate B rows). Each
+// K-block of 32 samples of one tile is written to shared memory as FP16 hi + lo pairs
 // (x = hi + lo + O(2^-22 x)) and accumulated in FP32 in tensor memory by
 //   D += A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T
-// (six tcgen05.mma kind::f16, M = 128, N = 32, K = 16; the lo*lo term is below 2^-22 relative).
+// (six tcgen05.mma kind::f16, M = 64, N = 32, K = 16; the lo*lo term is below 2^-22 relative).
 //
-// Tiles. Binning uses 120-row x 8-column tiles (footprint origins). Four consecutive tile keys
-// (the same tile row, 32 consecutive columns) form a super-tile. Its running sum lives in TMEM
-// columns [0, 128): block c = key % 4 owns columns [32c, 32c + 32), lanes = the 128 grid rows
-// origin1 .. origin1 + 127, columns 0..15 the real and 16..31 the imaginary part of grid columns
-// origin2 + 8c .. origin2 + 8c + 15. Neighbouring blocks overlap by 8 grid columns; the epilogue
-// adds the overlap while it reads TMEM, and flushes every non-zero cell once with a vector
-// reduction to the moment plane, checkerboard sign and 1 / scale applied.
+// Cost model (measured on B200): a tcgen05.mma of this skinny shape costs about its operand bytes
+// read from shared memory at ~117 B/clk (M = 128, N = 32: 43 clk; M = 64, N = 32: 26 clk), so the
+// accumulator is 64 rows and the operands are built with as few shared-memory wavefronts as
+// possible: both operands are MN-major (8 consecutive rows / columns of one sample form one
+// 16-byte row of a core matrix), and the eight threads of a sample hold the eight footprint
+// positions of its two 8-row chunks after a warp-shuffle rotation, so the stores are contiguous
+// 4-byte pairs and a sample's B column is rewritten in full (no clearing).
+//
+// Tiles. Binning uses 56-row x 8-column tiles (footprint origins). Four consecutive tile keys
+// (the same tile row, 32 consecutive columns) form a super-tile whose running sum lives in TMEM
+// columns [0, 128): block c = key % 4 owns columns [32c, 32c + 32) (0..15 real, 16..31 imaginary
+// part of grid columns origin2 + 8c .. + 15); row r of the 64-row accumulator sits in TMEM lane
+// 32 (r / 16) + r % 16. Neighbouring blocks overlap by 8 grid columns; the epilogue adds the
+// overlap and reduces every non-zero cell once into the moment plane (red.global.add.v2.f32),
+// checkerboard sign and 1 / scale applied.
 //
 // Two-level accumulation. The tensor core's FP32 accumulation is not round-to-nearest: summing
 // thousands of MMAs into one accumulator shrank dense grid cells by a relative 3.5e-5 on the 8.4M
-// sample snapshot (measured against the oracle). So the MMAs of at most 8 K-blocks of one key
-// (48 MMAs) go to one of three "fresh" 32-column accumulators (columns 128..223), which are then
-// added into the running block with FP32 round-to-nearest adds (tcgen05.ld / tcgen05.st, two
-// K-blocks later, when those MMAs are done).
+// sample snapshot (measured against the oracle). So the MMAs of at most 8 K-blocks of one key go
+// to one of four 32-column "fresh" accumulators (columns 128..255), which the epilogue warps add
+// into the running block with FP32 round-to-nearest adds once those MMAs are done.
 //
-// Work split. Every CTA takes an equal share of the binned records (a contiguous range, which can
-// start and end inside a tile) and walks it in K-blocks; a super-tile change flushes the
-// accumulator. Warp 0 prefetches the records of the K-block four steps ahead into a shared-memory
-// ring with cp.async; all 256 threads build the operands of the current K-block (thread = one
-// footprint row/column of one sample) into one of four stages, whose reuse waits on the mbarrier
-// that tcgen05.commit signals when the stage's MMAs are done; thread 0 issues the MMAs.
+// Roles (two CTAs per SM, 14 warps, 256 TMEM columns each):
+//   warps 0-7   producers, two groups of 128 threads filling alternate K-blocks (a thread owns two
+//               taps and two footprint positions of one sample); stage s is reused once the MMAs of
+//               its previous K-block commit to empty[s]; every thread arrives on full[s].
+//   warp 8      scheduler: walks the CTA's share of the K-blocks (runs of up to 32 records of one
+//               key) and publishes their descriptors to a ring.
+//   warp 9      MMA issuer: issues the MMAs, opens and closes fresh intervals and posts merge /
+//               flush / exit events.
+//   warps 10-13 epilogue: TMEM lane quarter (warp % 4); merge fresh intervals into the running sum
+//               and flush super-tiles to the moment plane, in event order.
+// Every CTA takes an equal share of the binned records (a contiguous range that can start and end
+// inside a tile).
 //
 // Scaling. The B values are wy * v * 2^(14 - e) with max|v| < 2^e over all records (the scatter
 // kernel's max reduction) and the A values 256 * wx, so every FP16 operand is below 65504 and the
@@ -42,9 +55,10 @@
 // clipped at the low grid edge) skip the matrices: the eight threads of the sample add their
 // exact ES weights to the moment plane directly.
 //
-// Every wait is bounded (about one second of global time); a wait that runs out sets *status,
-// the CTA stops, waits (bounded) for its MMAs, frees its tensor memory and returns, and the host
-// reports the grid as incomplete.
+// Every wait is bounded (about one second of global time); a wait that runs out sets *status and
+// a CTA-wide abort flag that every other wait also watches, so all roles leave their loops, the
+// MMA warp waits (bounded) for its last commit, the tensor memory is freed and the host reports
+// the grid as incomplete.
 #include "svdi_internal.cuh"
 
 #include <cuda_fp16.h>
@@ -53,50 +67,56 @@ namespace svdi {
 
 namespace {
 
-constexpr int kThreads = 256;
-constexpr int kKB = 32;          // samples per K-block
-constexpr int kStages = 4;       // operand stages in shared memory
-constexpr int kRing = 8;         // record ring slots (K-blocks)
-constexpr int kAhead = 4;        // K-blocks of records in flight
-constexpr int kAccRows = 128;    // M
-constexpr int kBlockCols = 32;   // N per column block (16 re + 16 im)
-constexpr int kFreshBufs = 3;    // fresh accumulators: one open interval + two awaiting their merge
-constexpr int kFreshKB = 8;      // K-blocks (48 MMAs) per fresh interval at most
-constexpr int kFreshCol0 = kTcBlocks * kBlockCols;  // running blocks first, then the fresh buffers
+constexpr int kKB = kTcKBlock;          // samples per K-block
+constexpr int kM = 64;                  // accumulator rows: tile rows + footprint halo
+constexpr int kN = 32;                  // columns per block: 16 real + 16 imaginary
+constexpr int kLanesPerSample = 4;      // a thread owns two taps / two footprint positions
+constexpr int kGroupThreads = kKB * kLanesPerSample;       // one K-block: 128 threads
+constexpr int kGroups = 2;              // producer groups fill alternate K-blocks
+constexpr int kProdWarps = kGroups * kGroupThreads / 32;  // 8
+constexpr int kSchedWarp = kProdWarps;                     // 8
+constexpr int kMmaWarp = kProdWarps + 1;                   // 9
+constexpr int kEpiWarp0 = kProdWarps + 2;                  // 10..13
+constexpr int kWarps = kProdWarps + 2 + 4;
+constexpr int kThreads = kWarps * 32;                      // 448
+constexpr int kStages = 8;              // operand sub-stages: one K-block each
+constexpr int kPairs = kStages / 2;     // pipeline stages: two consecutive K-blocks (one per group)
+constexpr int kFreshBufs = 4;
+constexpr int kFreshKB = 8;             // K-blocks (48 MMAs) per fresh interval at most
+constexpr int kFreshCol0 = kTcBlocks * kN;  // running blocks first, then the fresh buffers
 constexpr int kTmemCols = 256;
-static_assert(kFreshCol0 + kFreshBufs * kBlockCols <= kTmemCols, "TMEM plan exceeds the allocation");
+constexpr int kMetaRing = 128;          // published K-block descriptors
+constexpr int kEventRing = 64;
 
-constexpr int kABytes = kAccRows * kKB * 2;     // 8 KB per FP16 A operand
-constexpr int kBBytes = kBlockCols * kKB * 2;   // 2 KB per FP16 B operand
-constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;
-constexpr int kRingBytes = kRing * kKB * (int)sizeof(SampleRec);
-constexpr int kOldBytes = kStages * kThreads * 4;
-constexpr int kSmemUsed = kStages * kStageBytes + kRingBytes + kOldBytes;
-// Requested dynamic shared memory: above a third of the SM's 228 KB, so that at most two CTAs of
-// this kernel are resident on an SM and their 2 x 256 TMEM columns always fit in its 512.
-constexpr int kSmemBytes = 96 * 1024;
+constexpr int kABytes = kM * kKB * 2;                    // 4 KB per FP16 A operand
+constexpr int kBBytes = kN * kKB * 2;                    // 2 KB per FP16 B operand
+constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;   // 12 KB
+constexpr int kOldBytes = kStages * kGroupThreads;       // last A chunk written, per stage and thread
+constexpr int kSmemUsed = kStages * kStageBytes + kOldBytes;
+// Requested dynamic shared memory: more than a third of the SM's 228 KB, so at most two CTAs share
+// an SM and their 2 x 256 TMEM columns always fit in its 512.
+constexpr int kSmemBytes = 100 * 1024;
 static_assert(kSmemUsed <= kSmemBytes, "shared-memory plan exceeds the request");
-static_assert(kRing >= kAhead + 1, "record ring too small for the prefetch distance");
-static_assert(kTcTileRows + 8 <= kAccRows && kTcTileCols + 8 <= 16, "tile + footprint must fit the accumulator");
+static_assert(kFreshCol0 + kFreshBufs * kN <= kTmemCols, "TMEM plan exceeds the allocation");
+static_assert(kTcTileRows + 8 <= kM && kTcTileCols + 8 <= 16, "tile + footprint must fit the accumulator");
+static_assert(kGroups == 2 && kStages % 2 == 0, "a pipeline stage holds one K-block of each producer group");
+static_assert(kEpiWarp0 + 4 == kWarps, "four epilogue warps (one per TMEM lane quarter) come last");
 
-// K-major, no-swizzle canonical layout of an FP16 operand with kKB columns: core matrices of
-// 8 rows x 16 bytes; the next 8 K-elements at +128 bytes (LBO), the next 8 rows at +512 (SBO).
-__device__ __forceinline__ int op_off(int row, int k) {
-    return (row & 7) * 16 + (row >> 3) * 512 + (k >> 3) * 128 + (k & 7) * 2;
+// MN-major, no-swizzle canonical layout of an FP16 operand with kKB K-columns: a core matrix is
+// 8 K-rows x 16 bytes (8 consecutive M or N elements); the next 8 K at +128 bytes (LBO), the next
+// 8 M / N elements at +512 bytes (SBO).
+__device__ __forceinline__ int op_off(int mn, int k) {
+    return (mn & 7) * 2 + (k & 7) * 16 + (k >> 3) * 128 + (mn >> 3) * 512;
 }
-constexpr unsigned long long kDescHi = (512ull >> 4) << 32 | (1ull << 46);  // SBO, version 1
-constexpr unsigned long long kDescLbo = (128ull >> 4) << 16;                // LBO
-
+constexpr unsigned long long kDescFixed = ((128ull >> 4) << 16) | ((512ull >> 4) << 32) | (1ull << 46);
 __device__ __forceinline__ unsigned long long smem_desc(uint32_t addr) {
-    return (unsigned long long)((addr >> 4) & 0x3FFFu) | kDescLbo | kDescHi;
+    return (unsigned long long)((addr >> 4) & 0x3FFFu) | kDescFixed;
 }
+// Instruction descriptor: FP32 accumulator, FP16 A and B, both MN-major, N = 32, M = 64.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 15) | (1u << 16) | ((uint32_t)(kN >> 3) << 17) |
+                            ((uint32_t)(kM >> 4) << 24);
 
-// Instruction descriptor: FP32 accumulator, FP16 A and B, both K-major, N = 32, M = 128.
-constexpr uint32_t kIdesc = (1u << 4) | ((uint32_t)(kBlockCols >> 3) << 17) | ((uint32_t)(kAccRows >> 4) << 24);
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -116,13 +136,40 @@ __device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait for the completion of the phase with the given parity: about one second.
-__device__ bool mbar_wait(uint32_t addr, uint32_t parity) {
+__device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(addr), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t addr) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(addr) : "memory");
+}
+
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.cta.shared::cta.u32 %0, [%1];" : "=r"(v) : "r"(smem_u32(p)) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(unsigned int* p, unsigned int v) {
+    asm volatile("st.release.cta.shared::cta.u32 [%0], %1;" ::"r"(smem_u32(p)), "r"(v) : "memory");
+}
+
+// Bounded waits (about one second of global time) that also give up when another thread of the
+// CTA has given up (*abort != 0). They return false on either.
+__device__ bool mbar_wait(uint32_t addr, uint32_t parity, const volatile int* abort) {
     if (mbar_try(addr, parity)) return true;
     const unsigned long long t0 = global_ns();
     for (unsigned int it = 1; it < (1u << 28); ++it) {
         if (mbar_try(addr, parity)) return true;
-        if ((it & 63u) == 0 && global_ns() - t0 > 1000000000ull) return false;
+        if ((it & 63u) == 0 && (*abort || global_ns() - t0 > 1000000000ull)) return false;
+    }
+    return false;
+}
+__device__ bool wait_at_least(const unsigned int* p, unsigned int target, const volatile int* abort) {
+    if (ld_acquire(p) >= target) return true;
+    const unsigned long long t0 = global_ns();
+    for (unsigned int it = 1; it < (1u << 28); ++it) {
+        __nanosleep(64);
+        if (ld_acquire(p) >= target) return true;
+        if ((it & 15u) == 0 && (*abort || global_ns() - t0 > 1000000000ull)) return false;
     }
     return false;
 }
@@ -139,7 +186,6 @@ __device__ __forceinline__ void mma_f16(uint32_t d_tmem, unsigned long long a, u
         : "r"(d_tmem), "l"(a), "l"(b), "r"(kIdesc), "r"(accum)
         : "memory");
 }
-
 __device__ __forceinline__ void mma_commit(uint32_t mbar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
                  : "memory");
@@ -162,39 +208,25 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-    uint32_t r[16];
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float (&v)[32]) {
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
-}
-
-__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float (&v)[16]) {
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
-        "{%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16};" ::"r"(taddr),
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+        "{%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, "
+        "%17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(taddr),
         "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
         "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
         "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
         "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
         "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
-        "r"(__float_as_uint(v[15]))
+        "r"(__float_as_uint(v[15])), "r"(__float_as_uint(v[16])), "r"(__float_as_uint(v[17])),
+        "r"(__float_as_uint(v[18])), "r"(__float_as_uint(v[19])), "r"(__float_as_uint(v[20])),
+        "r"(__float_as_uint(v[21])), "r"(__float_as_uint(v[22])), "r"(__float_as_uint(v[23])),
+        "r"(__float_as_uint(v[24])), "r"(__float_as_uint(v[25])), "r"(__float_as_uint(v[26])),
+        "r"(__float_as_uint(v[27])), "r"(__float_as_uint(v[28])), "r"(__float_as_uint(v[29])),
+        "r"(__float_as_uint(v[30])), "r"(__float_as_uint(v[31]))
         : "memory");
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
-
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 __device__ __forceinline__ void red_add_v2(float2* addr, float a, float b) {
     asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(addr), "f"(a), "f"(b) : "memory");
@@ -206,92 +238,108 @@ __device__ __forceinline__ float es_exact(float beta, float x) {
     return expf(-beta * x * x / (1.0f + sqrtf((1.0f - x) * (1.0f + x))));
 }
 
-__device__ __forceinline__ void split_store(unsigned char* hi, unsigned char* lo, int off, float x) {
-    const __half h = __float2half_rn(x);
-    *reinterpret_cast<__half*>(hi + off) = h;
-    *reinterpret_cast<__half*>(lo + off) = __float2half_rn(x - __half2float(h));
+// x0, x1 as FP16 hi + lo pairs packed into two 32-bit words (x0 in the low halves).
+__device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_t& lo) {
+    const __half2 h = __floats2half2_rn(x0, x1);
+    const float2 f = __half22float2(h);
+    const __half2 l = __floats2half2_rn(x0 - f.x, x1 - f.y);
+    hi = *reinterpret_cast<const uint32_t*>(&h);
+    lo = *reinterpret_cast<const uint32_t*>(&l);
 }
 
 struct KBMeta {
-    int key;   // tile key of the K-block
-    int cnt;   // samples in it (0 = no more K-blocks)
+    int key;            // tile key of the K-block
+    unsigned int pos;   // first record
+    int cnt;            // records (1..32)
 };
 
-// Walks the CTA's record range [rbeg, rend) in K-blocks of one key each.
-struct KIter {
-    int key;
-    unsigned int pos, end;
-    bool ok;
-    __device__ void next_key(const unsigned int* off, int key_hi, unsigned int rend) {
-        for (;;) {
-            ++key;
-            if (key >= key_hi) { ok = false; return; }
-            const unsigned int b = off[key];
-            if (b >= rend) { ok = false; return; }
-            const unsigned int e = min(rend, off[key + 1]);
-            if (b < e) { pos = b; end = e; return; }
-        }
-    }
-    __device__ void advance(const unsigned int* off, int key_hi, unsigned int rend) {
-        pos += kKB;
-        if (pos >= end) next_key(off, key_hi, rend);
-    }
+enum EventType : int { kEvMerge = 0, kEvFlush = 1, kEvExit = 2 };
+struct Event {
+    int type;
+    int buf;     // merge: fresh buffer
+    int blk;     // merge: running block
+    int key;     // flush: a key of the super-tile
+    int parity;  // merge: phase parity of the fresh buffer's MMAs-done barrier
 };
 
 struct TcParams {
     const SampleRec* rec;
     const unsigned int* offsets;
+    const unsigned int* kb_offsets;  // exclusive scan of ceil(count / kKB) per key
     const unsigned int* vmax;
     float2* planes;
     unsigned int* status;
     int key_lo, key_hi, slab_lo;
 };
 
+struct __align__(8) TcShared {
+    unsigned long long full[kPairs];      // producers -> MMA: both K-blocks of the stage written
+    unsigned long long empty[kPairs];     // MMA -> producers: stage read (tcgen05.commit)
+    unsigned long long fdone[kFreshBufs]; // MMA -> epilogue: fresh interval's MMAs done (commit)
+    unsigned long long ffree[kFreshBufs]; // epilogue -> MMA: fresh buffer merged (4 warp arrivals)
+    KBMeta meta[kMetaRing];
+    Event events[kEventRing];
+    unsigned int published;               // K-block descriptors published
+    unsigned int consumed;                // K-blocks whose descriptor the MMA warp and producers are done with
+    unsigned int sched_done;              // 1 + total K-blocks once the schedule is complete
+    unsigned int ev_published;
+    unsigned int ev_consumed[4];
+    int abort;
+    uint32_t tmem_base;
+    int start_key;         // key of the CTA's first K-block
+    unsigned int start_m;  // its K-block index within that key
+};
+
 __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g, EsPoly poly) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) unsigned long long mbar[kStages];
-    __shared__ KBMeta meta[kRing];
-    __shared__ uint32_t tmem_base_sh;
-    __shared__ int start_key_sh;
-
-    unsigned char* stage_base = smem;
-    SampleRec* ring = reinterpret_cast<SampleRec*>(smem + kStages * kStageBytes);
-    int* oldpos = reinterpret_cast<int*>(smem + kStages * kStageBytes + kRingBytes);
+    __shared__ TcShared S;
+    signed char* oldchunk = reinterpret_cast<signed char*>(smem + kStages * kStageBytes);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int slot = tid >> 3, fi = tid & 7;  // sample slot of the K-block, footprint row/col index
     const int W = g.W, HW = W / 2;
     const int tiles2 = g.ntile * g.ntile2;
     const long long GG = g.G * g.G;
+    volatile int* abort_flag = &S.abort;
 
     // ---- set-up: tensor memory, barriers, the CTA's record range
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+    if (warp == kMmaWarp) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem_base)),
                      "r"(kTmemCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
+    // equal shares of the K-blocks of keys [key_lo, key_hi) (sparse tiles cost a K-block per key)
+    const unsigned int kb_lo = P.kb_offsets[P.key_lo], kb_hi = P.kb_offsets[P.key_hi];
+    const unsigned long long kb_total = kb_hi - kb_lo;
+    const unsigned int kbb = kb_lo + (unsigned int)(kb_total * blockIdx.x / gridDim.x);
+    const unsigned int kbe = kb_lo + (unsigned int)(kb_total * (blockIdx.x + 1) / gridDim.x);
     if (tid == 0) {
-        for (int s = 0; s < kStages; ++s)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[s])) : "memory");
+        for (int s = 0; s < kPairs; ++s) {
+            mbar_init(smem_u32(&S.full[s]), kGroups * kGroupThreads);
+            mbar_init(smem_u32(&S.empty[s]), 1);
+        }
+        for (int b = 0; b < kFreshBufs; ++b) {
+            mbar_init(smem_u32(&S.fdone[b]), 1);
+            mbar_init(smem_u32(&S.ffree[b]), 4);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    for (int i = tid; i < kStages * kStageBytes / 16; i += kThreads)
-        reinterpret_cast<uint4*>(stage_base)[i] = make_uint4(0, 0, 0, 0);
-    for (int i = tid; i < kStages * kThreads; i += kThreads) oldpos[i] = -1;
-
-    const unsigned int rec_lo = P.offsets[P.key_lo], rec_hi = P.offsets[P.key_hi];
-    const unsigned long long total = rec_hi - rec_lo;
-    const unsigned int rbeg = rec_lo + (unsigned int)(total * blockIdx.x / gridDim.x);
-    const unsigned int rend = rec_lo + (unsigned int)(total * (blockIdx.x + 1) / gridDim.x);
-    if (tid == 0) {  // last key with offsets[key] <= rbeg
-        int lo = P.key_lo, hi = P.key_hi;
+        S.published = 0;
+        S.consumed = 0;
+        S.sched_done = 0;
+        S.ev_published = 0;
+        for (int q = 0; q < 4; ++q) S.ev_consumed[q] = 0;
+        S.abort = 0;
+        int lo = P.key_lo, hi = P.key_hi;  // last key with kb_offsets[key] <= kbb
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
-            if (P.offsets[mid] <= rbeg) lo = mid; else hi = mid;
+            if (P.kb_offsets[mid] <= kbb) lo = mid; else hi = mid;
         }
-        start_key_sh = lo;
+        S.start_key = lo;
+        S.start_m = kbb - P.kb_offsets[lo];
     }
+    for (int i = tid; i < kStages * kStageBytes / 16; i += kThreads)
+        reinterpret_cast<uint4*>(smem)[i] = make_uint4(0, 0, 0, 0);
+    for (int i = tid; i < kOldBytes; i += kThreads) oldchunk[i] = -1;
     // FP16 operand scale from max |v| over all records
     float vscale = 0.0f;
     {
@@ -303,287 +351,531 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
         }
     }
     const float inv_scale = vscale > 0.0f ? 1.0f / (256.0f * vscale) : 0.0f;
-    float coef[kPolyDeg + 1];
-#pragma unroll
-    for (int d = 0; d <= kPolyDeg; ++d) coef[d] = poly.c[fi][d];
-
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tmem = tmem_base_sh;
+    const uint32_t tmem = S.tmem_base;
 
-    // ---- record prefetch (warp 0): K-block j goes to ring slot j % kRing, one cp.async group each
-    KIter pf;
-    if (warp == 0) {
-        pf.key = start_key_sh;
-        pf.pos = rbeg;
-        pf.end = min(rend, P.offsets[pf.key + 1]);
-        pf.ok = rbeg < rend;
-        if (pf.ok && pf.pos >= pf.end) pf.next_key(P.offsets, P.key_hi, rend);
-    }
-    auto prefetch = [&](int j) {  // warp 0 only
-        const int cnt = pf.ok ? (int)min((unsigned int)kKB, pf.end - pf.pos) : 0;
-        if (lane < cnt) cp_async16(smem_u32(ring + (j % kRing) * kKB + lane), P.rec + pf.pos + lane);
-        cp_async_commit();
-        if (lane == 0) meta[j % kRing] = KBMeta{pf.ok ? pf.key : -1, cnt};
-        if (pf.ok) pf.advance(P.offsets, P.key_hi, rend);
-    };
-    if (warp == 0) {
-        for (int j = 0; j < kAhead; ++j) prefetch(j);
-        cp_async_wait<kAhead - 1>();
-    }
-    __syncthreads();
-
-    int cur_st = -1, cur_key = 0;
-    int kb = 0;
-    bool aborted = false;  // block-uniform (set from __syncthreads_or)
-    // Accumulation state, block-uniform. run_valid bit c: running block c holds data. Open interval:
-    // fresh buffer ob, block oc, on K-blocks so far (on == 0: none open). Closed intervals waiting
-    // for their merge, oldest first: pend[0..np), packed (last K-block << 8) | (block << 4) | buffer.
-    unsigned int run_valid = 0;
-    int ob = 0, oc = 0, on = 0;
-    int pend[3] = {0, 0, 0};
-    int np = 0;
-
-    const int q = warp & 3, h = warp >> 2;  // TMEM lane quarter, column half of this warp
-    const uint32_t lane_addr = (uint32_t)(32 * q) << 16;
-
-    auto wait_kb = [&](int j) -> bool {  // the MMAs of K-block j are complete (bounded wait)
-        return mbar_wait(smem_u32(&mbar[j % kStages]), (uint32_t)((j / kStages) & 1));
-    };
-    // running[blk] (+)= fresh[buf] with FP32 round-to-nearest adds: this thread's lane, columns
-    // [16h, 16h + 16) of the block (h = 0: real, h = 1: imaginary part).
-    auto merge = [&](int packed) {
-        const int buf = packed & 15, blk = (packed >> 4) & 15;
-        float f[16], r[16];
-        const uint32_t ra = tmem + lane_addr + (uint32_t)(kBlockCols * blk + 16 * h);
-        tmem_ld16(tmem + lane_addr + (uint32_t)(kFreshCol0 + kBlockCols * buf + 16 * h), f);
-        if ((run_valid >> blk) & 1u) {
-            tmem_ld16(ra, r);
+    if (warp < kProdWarps) {
+        // =========================== producers ===========================
+        const int grp = warp / (kGroupThreads / 32);
+        const int gtid = tid % kGroupThreads;
+        const int slot = gtid / kLanesPerSample, t = gtid % kLanesPerSample;
+        const int lane0 = lane & ~(kLanesPerSample - 1);  // first lane of this sample's four
+        const int q0 = 2 * t, q1 = 2 * t + 1;             // this thread's taps and positions
+        float cf0[kPolyDeg + 1], cf1[kPolyDeg + 1];
 #pragma unroll
-            for (int j = 0; j < 16; ++j) f[j] += r[j];
+        for (int d = 0; d <= kPolyDeg; ++d) {
+            cf0[d] = poly.c[q0][d];
+            cf1[d] = poly.c[q1][d];
         }
-        tmem_st16(ra, f);
-        run_valid |= 1u << blk;
-    };
-    auto close_interval = [&]() {
-        if (on > 0) {
-            pend[np] = ((kb - 1) << 8) | (oc << 4) | ob;
-            ++np;
-            on = 0;
-        }
-    };
-
-    // Flush the super-tile of cur_key: merge every fresh interval, read the running blocks (warp w:
-    // rows 32 (w % 4) + lane, blocks 2 (w / 4) and 2 (w / 4) + 1), add the column overlaps and reduce
-    // the non-zero on-grid cells into the moment plane.
-    auto flush = [&]() {
-        bool fail = false;
-        close_interval();
-        if (np > 0 && !wait_kb(pend[np - 1] >> 8)) {  // the newest commit covers the older MMAs
-            fail = true;
-            atomicOr(P.status, 2u);
-        }
-        tc_fence_after();
-        for (int k = 0; k < np; ++k) merge(pend[k]);
-        np = 0;
-        // the merges stored the real halves from warps 0-3 and the imaginary halves from warps 4-7;
-        // the epilogue below reads whole blocks across that split
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
-        const int slab = cur_key / tiles2;
-        const int t1 = (cur_key / g.ntile2) % g.ntile;
-        const int t2b = (cur_key % g.ntile2) / kTcBlocks * kTcBlocks;
-        const int row = 32 * q + lane;
-        const long long g1 = g.gmin + (long long)t1 * g.T + row;
-        const bool row_ok = g1 <= g.gmax;
-        const long long o2 = g.gmin + (long long)t2b * g.T2;  // grid column of block 0, column 0
-        float2* plane = P.planes + (long long)(slab - P.slab_lo) * GG + (g1 - g.gmin) * g.G;
-        float cre[8], cim[8];
+        // operand byte offset of positions (q0, q1) of chunk 0 in K-slot `slot`; chunk c adds 512 c
+        const int pbase = op_off(q0, slot);
+        // record prefetch queue: the records of this group's next two K-blocks (tag = K-block)
+        SampleRec preA = {0, 0, 0.0f, 0.0f}, preB = {0, 0, 0.0f, 0.0f};
+        int tagA = -1, tagB = -1;
+        int pub_seen = 0;  // lane 0: published count last read (acquire)
+        for (int it = 0;; ++it) {
+            const int j = it * kGroups + grp;
+            // wait until K-block j is published or the schedule ends before it (warp-uniform)
+            int state = 0, pub = 0;  // state 1: produce, 0: done, -1: abort
+            if (lane == 0) {
+                const unsigned long long t0 = global_ns();
+                for (unsigned int n = 0;; ++n) {
+                    if (pub_seen <= j + 2 * kGroups) pub_seen = (int)ld_acquire(&S.published);
+                    pub = pub_seen;
+                    if (pub > j) { state = 1; break; }
+                    const unsigned int sd = ld_acquire(&S.sched_done);
+                    if (sd && (unsigned int)j >= sd - 1) { state = 0; break; }
+                    if ((n & 63u) == 0 && (*abort_flag || global_ns() - t0 > 1000000000ull)) {
+                        state = -1;
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+            }
+            state = __shfl_sync(0xffffffffu, state, 0);
+            pub = __shfl_sync(0xffffffffu, pub, 0);
+            // pipeline stage of K-block j: pair j / 2 (the other group fills the other half)
+            const int pr = (j >> 1) % kPairs, u = (j >> 1) / kPairs;
+            const int s = 2 * pr + grp;  // this K-block's sub-stage
+            if (state == 0 && (j & 1)) {
+                // the schedule ends at K-block j - 1, the first half of this stage: complete the
+                // stage's arrival count (after the stage is free, so the arrivals count for this use)
+                unsigned int sd = 0;
+                if (lane == 0) sd = ld_acquire(&S.sched_done);
+                sd = __shfl_sync(0xffffffffu, sd, 0);
+                if (sd && (unsigned int)j == sd - 1) {
+                    bool ok = true;
+                    if (u > 0) ok = mbar_wait(smem_u32(&S.empty[pr]), (uint32_t)((u - 1) & 1), abort_flag);
+                    if (__all_sync(0xffffffffu, ok)) mbar_arrive(smem_u32(&S.full[pr]));
+                }
+            }
+            if (state <= 0) {
+                if (state < 0 && lane == 0 && !*abort_flag) {
+                    atomicOr(P.status, 1u);
+                    *abort_flag = 1;
+                }
+                break;
+            }
+            const KBMeta m = S.meta[j % kMetaRing];
+            // record of this thread's sample (the four threads of a sample load the same 16 bytes)
+            const bool valid = slot < m.cnt;
+            SampleRec r = {0, 0, 0.0f, 0.0f};
+            if (valid) r = (tagA == j) ? preA : P.rec[m.pos + slot];
+            {  // advance the queue; load the records of K-block j + 2 kGroups if it is published
+                preA = preB;
+                tagA = tagB;
+                const int jn = j + 2 * kGroups;
+                tagB = -1;
+                if (pub > jn) {
+                    const KBMeta mn = S.meta[jn % kMetaRing];
+                    if (slot < mn.cnt) preB = P.rec[mn.pos + slot];
+                    tagB = jn;
+                }
+            }
+            const int cx = r.xq >> 24, cy = r.yq >> 24;
+            const int fxq = r.xq & 0xFFFFFF, fyq = r.yq & 0xFFFFFF;
+            const int r0 = cx - (HW - 1), c0 = cy - (HW - 1);
+            const bool rare = valid && (fxq == 0 || fyq == 0 || r0 < 0 || c0 < 0 || r0 >= g.T || c0 >= g.T2);
+            const bool fast = valid && !rare;
+            float wx0, wx1, wy0, wy1;
+            {
+                const float ux = fmaf(2.0f, (float)fxq * (1.0f / 16777216.0f), -1.0f);
+                const float uy = fmaf(2.0f, (float)fyq * (1.0f / 16777216.0f), -1.0f);
+                wx0 = cf0[kPolyDeg]; wx1 = cf1[kPolyDeg];
+                wy0 = cf0[kPolyDeg]; wy1 = cf1[kPolyDeg];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) { cre[j] = 0.0f; cim[j] = 0.0f; }
-        auto emit = [&](long long g2, float re, float im) {
-            if (row_ok && g2 <= g.gmax && (re != 0.0f || im != 0.0f)) {
-                const float sg = ((g1 + g2) & 1) ? -inv_scale : inv_scale;
-                red_add_v2(plane + (g2 - g.gmin), sg * re, sg * im);
+                for (int d = kPolyDeg - 1; d >= 0; --d) {
+                    wx0 = fmaf(wx0, ux, cf0[d]);
+                    wx1 = fmaf(wx1, ux, cf1[d]);
+                    wy0 = fmaf(wy0, uy, cf0[d]);
+                    wy1 = fmaf(wy1, uy, cf1[d]);
+                }
+            }
+            // rotation: footprint position q of the 16 rows (columns) from the 8-aligned chunk below
+            // r0 (c0) holds tap (q - shift) & 7, in chunk 0 if q >= shift, else in chunk 1
+            const int sr = fast ? (r0 & 7) : 0, sc = fast ? c0 : 0;
+            float vx0, vx1, vy0, vy1;
+            {
+                auto rot = [&](float w0, float w1, int sh, float& v0, float& v1) {
+                    const int tau = (q0 - sh) & 7;  // tap at position q0; q1 holds tau + 1
+                    const bool odd = tau & 1;
+                    const int srcA = lane0 + (tau >> 1), srcB = lane0 + (((tau >> 1) + 1) & 3);
+                    const float p = __shfl_sync(0xffffffffu, w0, odd ? srcB : srcA);
+                    const float q = __shfl_sync(0xffffffffu, w1, srcA);
+                    v0 = odd ? q : p;
+                    v1 = odd ? p : q;
+                };
+                rot(wx0, wx1, sr, vx0, vx1);
+                rot(wy0, wy1, sc, vy0, vy1);
+            }
+            // stage reuse: the MMAs of K-block j - kStages must be done with it (warp-uniform)
+            bool ok = true;
+            if (u > 0) ok = mbar_wait(smem_u32(&S.empty[pr]), (uint32_t)((u - 1) & 1), abort_flag);
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok) {
+                if (lane == 0 && !*abort_flag) {
+                    atomicOr(P.status, 1u);
+                    *abort_flag = 1;
+                }
+                break;
+            }
+            unsigned char* A_hi = smem + s * kStageBytes;
+            unsigned char* A_lo = A_hi + kABytes;
+            unsigned char* B_hi = A_lo + kABytes;
+            unsigned char* B_lo = B_hi + kBBytes;
+            // A: clear this thread's pair in the previous sample's chunks the new one does not cover
+            const int j0 = fast ? (r0 >> 3) : -8;
+            const int oj = oldchunk[s * kGroupThreads + gtid];
+            if (oj >= 0) {
+#pragma unroll
+                for (int d = 0; d < 2; ++d) {
+                    const int cj = oj + d;
+                    if (cj != j0 && cj != j0 + 1) {
+                        *reinterpret_cast<uint32_t*>(A_hi + pbase + cj * 512) = 0u;
+                        *reinterpret_cast<uint32_t*>(A_lo + pbase + cj * 512) = 0u;
+                    }
+                }
+            }
+            oldchunk[s * kGroupThreads + gtid] = (signed char)(fast ? j0 : -1);
+            const bool up0 = q0 < sr, up1 = q1 < sr;  // position in chunk j0 + 1
+            if (fast) {
+                const float a0 = 256.0f * vx0, a1 = 256.0f * vx1;
+                uint32_t h, l;
+                split2(up0 ? 0.0f : a0, up1 ? 0.0f : a1, h, l);
+                *reinterpret_cast<uint32_t*>(A_hi + pbase + j0 * 512) = h;
+                *reinterpret_cast<uint32_t*>(A_lo + pbase + j0 * 512) = l;
+                split2(up0 ? a0 : 0.0f, up1 ? a1 : 0.0f, h, l);
+                *reinterpret_cast<uint32_t*>(A_hi + pbase + (j0 + 1) * 512) = h;
+                *reinterpret_cast<uint32_t*>(A_lo + pbase + (j0 + 1) * 512) = l;
+            }
+            {  // B: all four 8-column chunks of this sample's column, every time
+                const float wv0 = fast ? vy0 * vscale : 0.0f, wv1 = fast ? vy1 * vscale : 0.0f;
+                const bool cu0 = q0 < sc, cu1 = q1 < sc;  // column position in chunk 1
+                const float re0 = wv0 * r.vre, re1 = wv1 * r.vre, im0 = wv0 * r.vim, im1 = wv1 * r.vim;
+                uint32_t h, l;
+                split2(cu0 ? 0.0f : re0, cu1 ? 0.0f : re1, h, l);
+                *reinterpret_cast<uint32_t*>(B_hi + pbase) = h;
+                *reinterpret_cast<uint32_t*>(B_lo + pbase) = l;
+                split2(cu0 ? re0 : 0.0f, cu1 ? re1 : 0.0f, h, l);
+                *reinterpret_cast<uint32_t*>(B_hi + pbase + 512) = h;
+                *reinterpret_cast<uint32_t*>(B_lo + pbase + 512) = l;
+                split2(cu0 ? 0.0f : im0, cu1 ? 0.0f : im1, h, l);
+                *reinterpret_cast<uint32_t*>(B_hi + pbase + 1024) = h;
+                *reinterpret_cast<uint32_t*>(B_lo + pbase + 1024) = l;
+                split2(cu0 ? im0 : 0.0f, cu1 ? im1 : 0.0f, h, l);
+                *reinterpret_cast<uint32_t*>(B_hi + pbase + 1536) = h;
+                *reinterpret_cast<uint32_t*>(B_lo + pbase + 1536) = l;
+            }
+            if (rare) {  // exact ES weights straight to the moment plane; the 4 threads over cells
+                const int slab = m.key / tiles2;
+                const int t1 = (m.key / g.ntile2) % g.ntile, t2 = m.key % g.ntile2;
+                const long long o1 = g.gmin + (long long)t1 * g.T, o2 = g.gmin + (long long)t2 * g.T2;
+                const int lo_r = fxq ? r0 : cx - HW, nr = fxq ? W : W + 1;
+                const int lo_c = fyq ? c0 : cy - HW, nc = fyq ? W : W + 1;
+                const float px = (float)fxq * (1.0f / 16777216.0f), py = (float)fyq * (1.0f / 16777216.0f);
+                float2* plane = P.planes + (long long)(slab - P.slab_lo) * GG;
+                for (int cidx = t; cidx < nr * nc; cidx += kLanesPerSample) {
+                    const int rr = lo_r + cidx / nc, cc = lo_c + cidx % nc;
+                    const long long g1 = o1 + rr, g2 = o2 + cc;
+                    if (g1 < g.gmin || g2 < g.gmin || g1 > g.gmax || g2 > g.gmax) continue;
+                    const float x = ((float)(rr - cx) - px) / (float)HW;
+                    const float y = ((float)(cc - cy) - py) / (float)HW;
+                    const float kv = es_exact(poly.beta, x) * es_exact(poly.beta, y);
+                    const float sg = ((g1 + g2) & 1) ? -kv : kv;
+                    red_add_v2(plane + (g1 - g.gmin) * g.G + (g2 - g.gmin), sg * r.vre, sg * r.vim);
+                }
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive(smem_u32(&S.full[pr]));
+        }
+    } else if (warp == kSchedWarp) {
+        // ============================ scheduler ============================
+        // Schedule: K-blocks [kbb, kbe) in key order; K-block m of key k covers records
+        // [offsets[k] + 32 m, min(offsets[k + 1], offsets[k] + 32 (m + 1))). Lanes hold offsets and
+        // kb_offsets of the current 32-key chunk (x = 32 from the *_e registers); the next chunk's
+        // are loaded one chunk ahead.
+        int kc = S.start_key, ci = 0;
+        unsigned int m_in_key = S.start_m, remaining = kbe - kbb;
+        unsigned int off_l = 0, kbo_l = 0, off_e = 0, kbo_e = 0;
+        unsigned int noff_l = 0, nkbo_l = 0, noff_e = 0, nkbo_e = 0;
+        auto fetch = [&](int base, unsigned int& o, unsigned int& kb, unsigned int& oe, unsigned int& kbe_) {
+            const int k = min(base + lane, P.key_hi);
+            o = P.offsets[k];
+            kb = P.kb_offsets[k];
+            const int ke = min(base + 32, P.key_hi);
+            oe = P.offsets[ke];
+            kbe_ = P.kb_offsets[ke];
+        };
+        auto at = [&](unsigned int vl, unsigned int ve, int x) -> unsigned int {  // warp-uniform x in [0, 32]
+            const unsigned int v = __shfl_sync(0xffffffffu, vl, x & 31);
+            return x == 32 ? ve : v;
+        };
+        if (remaining) {
+            fetch(kc, off_l, kbo_l, off_e, kbo_e);
+            fetch(kc + 32, noff_l, nkbo_l, noff_e, nkbo_e);
+        }
+        unsigned int published = 0;
+        // current key: records [ka, kb_end_rec), K-blocks m_in_key .. nkb - 1
+        unsigned int ka = 0, kend = 0, nkb = 0;
+        bool have_key = false;
+        auto schedule_to = [&](unsigned int target) {  // publish K-blocks up to index target - 1
+            const unsigned int before = published;
+            while (remaining && published < target) {
+                if (!have_key || m_in_key >= nkb) {  // advance to the next key with K-blocks left
+                    if (have_key) {
+                        ++ci;
+                        m_in_key = 0;
+                    }
+                    for (;;) {
+                        if (kc + ci >= P.key_hi) {  // inconsistent K-block counts: stop scheduling
+                            remaining = 0;
+                            break;
+                        }
+                        if (ci == 32) {
+                            kc += 32;
+                            ci = 0;
+                            off_l = noff_l; kbo_l = nkbo_l; off_e = noff_e; kbo_e = nkbo_e;
+                            fetch(kc + 32, noff_l, nkbo_l, noff_e, nkbo_e);
+                        }
+                        nkb = at(kbo_l, kbo_e, ci + 1) - at(kbo_l, kbo_e, ci);
+                        if (m_in_key < nkb) break;
+                        ++ci;
+                        m_in_key = 0;
+                    }
+                    if (!remaining) break;
+                    ka = at(off_l, off_e, ci);
+                    kend = at(off_l, off_e, ci + 1);
+                    have_key = true;
+                }
+                // the K-blocks of this key, up to the target (no shuffles)
+                const int key = kc + ci;
+                while (remaining && published < target && m_in_key < nkb) {
+                    const unsigned int pos = ka + (unsigned int)kKB * m_in_key;
+                    if (lane == 0) S.meta[published % kMetaRing] = KBMeta{key, pos, (int)min((unsigned int)kKB, kend - pos)};
+                    ++published;
+                    ++m_in_key;
+                    --remaining;
+                }
+            }
+            if (published != before) {
+                __syncwarp();
+                if (lane == 0) st_release(&S.published, published);
+            }
+            if (!remaining && lane == 0 && ld_acquire(&S.sched_done) == 0) st_release(&S.sched_done, published + 1);
+        };
+        for (;;) {  // keep the ring full: up to kMetaRing descriptors ahead of the MMA warp
+            int cons = 0;
+            if (lane == 0) cons = (int)ld_acquire(&S.consumed);
+            cons = __shfl_sync(0xffffffffu, cons, 0);
+            schedule_to((unsigned int)cons + kMetaRing);
+            if (!remaining) break;
+            bool ok = true;
+            if (lane == 0) ok = wait_at_least(&S.consumed, (unsigned int)cons + 1, abort_flag);
+            if (!__shfl_sync(0xffffffffu, (int)ok, 0)) break;  // the waiting role reports the failure
+        }
+    } else if (warp == kMmaWarp) {
+        // ============================ MMA issuer ============================
+        // MMA / interval / event state (lane 0)
+        int cur_st = -1, cur_key = 0;
+        int ob = 0, oc = 0, on = 0, next_buf = 0;
+        unsigned int fuse[kFreshBufs];
+#pragma unroll
+        for (int b = 0; b < kFreshBufs; ++b) fuse[b] = 0;
+        unsigned int ev_n = 0;
+        int last_commit_stage = -1;
+        unsigned int last_commit_parity = 0;
+        int open_pair = -1;  // stage whose second K-block never came (end of the schedule)
+        unsigned int open_pair_parity = 0;
+        bool failed = false;
+        unsigned int ev_free_seen = 0;  // events consumed by every epilogue warp, last read
+        auto push_event = [&](Event ev) {  // lane 0
+            if (failed) return;
+            const unsigned long long t0 = global_ns();
+            for (unsigned int n = 0;; ++n) {
+                if (ev_n - ev_free_seen < (unsigned int)kEventRing) break;
+                unsigned int mn = 0xFFFFFFFFu;
+                for (int q = 0; q < 4; ++q) mn = min(mn, ld_acquire(&S.ev_consumed[q]));
+                ev_free_seen = mn;
+                if (ev_n - mn < (unsigned int)kEventRing) break;
+                if ((n & 63u) == 0 && (*abort_flag || global_ns() - t0 > 1000000000ull)) {
+                    failed = true;
+                    return;
+                }
+                __nanosleep(32);
+            }
+            S.events[ev_n % kEventRing] = ev;
+            ++ev_n;
+            st_release(&S.ev_published, ev_n);
+        };
+        auto close_interval = [&]() {  // lane 0
+            if (on > 0) {
+                mma_commit(smem_u32(&S.fdone[ob]));
+                push_event(Event{kEvMerge, ob, oc, 0, (int)(fuse[ob] & 1u)});
+                ++fuse[ob];
+                on = 0;
             }
         };
-#pragma unroll
-        for (int cc = 0; cc < 2; ++cc) {
-            const int c = 2 * h + cc;
-            float v[32];
-            if ((run_valid >> c) & 1u) {
-                tmem_ld32(tmem + lane_addr + (uint32_t)(kBlockCols * c), v);
-            } else {
-#pragma unroll
-                for (int j = 0; j < 32; ++j) v[j] = 0.0f;
-            }
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                emit(o2 + 8 * c + j, cre[j] + v[j], cim[j] + v[16 + j]);
-                cre[j] = v[8 + j];
-                cim[j] = v[24 + j];
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < 8; ++j) emit(o2 + 8 * (2 * h + 2) + j, cre[j], cim[j]);
-        run_valid = 0;
-        tc_fence_before();
-        if (__syncthreads_or(fail)) aborted = true;
-    };
 
-    for (;;) {
-        const KBMeta m = meta[kb % kRing];
-        if (m.cnt == 0) break;
-        const int st = m.key / kTcBlocks;  // ntile2 is a multiple of kTcBlocks
-        if (st != cur_st) {
-            if (cur_st >= 0) {
-                flush();
-                if (aborted) break;
+        unsigned int pub_seen = 0;  // published count last read (acquire): meta[< pub_seen] are visible
+        for (unsigned int i = 0;; ++i) {
+            // wait until K-block i is published or the schedule ends before it
+            int state = 0;
+            if (lane == 0) {
+                const unsigned long long t0 = global_ns();
+                for (unsigned int n = 0;; ++n) {
+                    if (pub_seen > i) { state = 1; break; }
+                    pub_seen = ld_acquire(&S.published);
+                    if (pub_seen > i) { state = 1; break; }
+                    const unsigned int sd = ld_acquire(&S.sched_done);
+                    if (sd && i >= sd - 1) { state = 0; break; }
+                    if ((n & 63u) == 0 && (*abort_flag || global_ns() - t0 > 1000000000ull)) {
+                        state = -1;
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+                if (state < 0) failed = true;
             }
-            cur_st = st;
-        }
-        cur_key = m.key;
-        const int c = m.key % kTcBlocks;
-        if (on > 0 && (c != oc || on == kFreshKB)) close_interval();
-        if (on == 0) {  // a fresh buffer that no closed interval still occupies
-            unsigned int used = 0;
-            for (int k = 0; k < np; ++k) used |= 1u << (pend[k] & 15);
-            ob = (used & 1u) == 0 ? 0 : ((used & 2u) == 0 ? 1 : 2);
-            oc = c;
-        }
-        if (warp == 0) prefetch(kb + kAhead);
-
-        // ---- this thread's sample slot and footprint index
-        const int s = kb % kStages;
-        unsigned char* A_hi = stage_base + s * kStageBytes;
-        unsigned char* A_lo = A_hi + kABytes;
-        unsigned char* B_hi = A_lo + kABytes;
-        unsigned char* B_lo = B_hi + kBBytes;
-        const bool valid = slot < m.cnt;
-        SampleRec r = {0, 0, 0.0f, 0.0f};
-        if (valid) r = ring[(kb % kRing) * kKB + slot];
-        const int cx = r.xq >> 24, cy = r.yq >> 24;
-        const int fxq = r.xq & 0xFFFFFF, fyq = r.yq & 0xFFFFFF;
-        const int r0 = cx - (HW - 1), c0 = cy - (HW - 1);
-        const bool rare = valid && (fxq == 0 || fyq == 0 || r0 < 0 || c0 < 0 || r0 >= g.T || c0 >= g.T2);
-        const bool fast = valid && !rare && fi < W;
-        float wx = 0.0f, wy = 0.0f;
-        if (fast) {
-            const float ux = fmaf(2.0f, (float)fxq * (1.0f / 16777216.0f), -1.0f);
-            const float uy = fmaf(2.0f, (float)fyq * (1.0f / 16777216.0f), -1.0f);
-            wx = coef[kPolyDeg];
-            wy = coef[kPolyDeg];
+            state = __shfl_sync(0xffffffffu, state, 0);
+            if (state <= 0) break;
+            if (lane == 0 && !failed) {
+                const KBMeta m = S.meta[i % kMetaRing];
+                const int st = m.key / kTcBlocks;  // ntile2 is a multiple of kTcBlocks
+                const int c = m.key % kTcBlocks;
+                if (st != cur_st) {
+                    if (cur_st >= 0) {
+                        close_interval();
+                        push_event(Event{kEvFlush, 0, 0, cur_key, 0});
+                    }
+                    cur_st = st;
+                }
+                cur_key = m.key;
+                if (on > 0 && (c != oc || on == kFreshKB)) close_interval();
+                if (on == 0) {  // open a fresh interval on the next buffer, once its last merge is done
+                    const int b = next_buf;
+                    next_buf = (next_buf + 1) % kFreshBufs;
+                    if (fuse[b] > 0 && !mbar_wait(smem_u32(&S.ffree[b]), (fuse[b] - 1) & 1u, abort_flag))
+                        failed = true;
+                    ob = b;
+                    oc = c;
+                }
+                const int pr = (int)((i >> 1) % kPairs);
+                const unsigned int u = (i >> 1) / kPairs;
+                const int s = 2 * pr + (int)(i & 1u);  // sub-stage of K-block i
+                // one wait per stage (two K-blocks): a try_wait costs the issuing thread ~200 clk
+                if (!failed && (i & 1u) == 0 && !mbar_wait(smem_u32(&S.full[pr]), u & 1u, abort_flag)) failed = true;
+                // producers and this warp are done with meta[<= i]; tell the scheduler every 8 K-blocks
+                if (!failed && (i & 7u) == 7u) st_release(&S.consumed, i + 1);
+                if (!failed) {
+                    tc_fence_after();
+                    const uint32_t d = tmem + (uint32_t)(kFreshCol0 + kN * ob);
+                    const uint32_t ah = smem_u32(smem + s * kStageBytes), al = ah + kABytes;
+                    const uint32_t bh = al + kABytes, bl = bh + kBBytes;
+                    uint32_t acc = on > 0 ? 1u : 0u;
 #pragma unroll
-            for (int d = kPolyDeg - 1; d >= 0; --d) {
-                wx = fmaf(wx, ux, coef[d]);
-                wy = fmaf(wy, uy, coef[d]);
+                    for (int k = 0; k < kKB / 16; ++k) {  // 16-element K steps: 2 K-groups = +256 bytes
+                        const uint32_t ko = (uint32_t)k * 256u;
+                        mma_f16(d, smem_desc(ah + ko), smem_desc(bh + ko), acc);
+                        acc = 1u;
+                        mma_f16(d, smem_desc(ah + ko), smem_desc(bl + ko), 1u);
+                        mma_f16(d, smem_desc(al + ko), smem_desc(bh + ko), 1u);
+                    }
+                    if (i & 1u) {  // both K-blocks of the stage issued
+                        mma_commit(smem_u32(&S.empty[pr]));
+                        last_commit_stage = pr;
+                        last_commit_parity = u & 1u;
+                        open_pair = -1;
+                    } else {
+                        open_pair = pr;
+                        open_pair_parity = u & 1u;
+                    }
+                    ++on;
+                }
+                if (failed && !*abort_flag) {
+                    atomicOr(P.status, 2u);
+                    *abort_flag = 1;
+                }
             }
+            if (__shfl_sync(0xffffffffu, (int)failed, 0) || *abort_flag) break;
         }
-        // ---- stage reuse: the MMAs of K-block kb - kStages must be done with it
-        bool fail = false;
-        if (kb >= kStages && !wait_kb(kb - kStages)) {
-            fail = true;
-            atomicOr(P.status, 1u);
-        }
-        {  // clear the entries this thread wrote into the stage last time
-            const int old = oldpos[s * kThreads + tid];
-            if (old >= 0) {
-                const int orow = old >> 8, ocol = old & 0xFF;
-                const int oa = op_off(orow, slot);
-                *reinterpret_cast<__half*>(A_hi + oa) = __float2half_rn(0.0f);
-                *reinterpret_cast<__half*>(A_lo + oa) = __float2half_rn(0.0f);
-                const int ob_ = op_off(ocol, slot), obi = op_off(16 + ocol, slot);
-                *reinterpret_cast<__half*>(B_hi + ob_) = __float2half_rn(0.0f);
-                *reinterpret_cast<__half*>(B_lo + ob_) = __float2half_rn(0.0f);
-                *reinterpret_cast<__half*>(B_hi + obi) = __float2half_rn(0.0f);
-                *reinterpret_cast<__half*>(B_lo + obi) = __float2half_rn(0.0f);
+        if (lane == 0) {
+            if (open_pair >= 0) {
+                mma_commit(smem_u32(&S.empty[open_pair]));
+                last_commit_stage = open_pair;
+                last_commit_parity = open_pair_parity;
+            }
+            if (!failed && !*abort_flag && cur_st >= 0) {
+                close_interval();
+                push_event(Event{kEvFlush, 0, 0, cur_key, 0});
+            }
+            push_event(Event{kEvExit, 0, 0, 0, 0});
+            if (failed && !*abort_flag) {
+                atomicOr(P.status, 2u);
+                *abort_flag = 1;
+            }
+            // no MMA of this CTA may still run when the tensor memory is freed
+            if (last_commit_stage >= 0) {
+                const volatile int never = 0;
+                if (!mbar_wait(smem_u32(&S.empty[last_commit_stage]), last_commit_parity, &never))
+                    atomicOr(P.status, 4u);
             }
         }
         __syncwarp();
-        if (fast) {
-            const int arow = r0 + fi, bcol = c0 + fi;
-            split_store(A_hi, A_lo, op_off(arow, slot), 256.0f * wx);
-            const float wv = wy * vscale;
-            split_store(B_hi, B_lo, op_off(bcol, slot), wv * r.vre);
-            split_store(B_hi, B_lo, op_off(16 + bcol, slot), wv * r.vim);
-            oldpos[s * kThreads + tid] = (arow << 8) | bcol;
-        } else {
-            oldpos[s * kThreads + tid] = -1;
-        }
-        if (rare) {  // exact ES weights straight to the moment plane; the slot's 8 threads over cells
-            const int slab = m.key / tiles2;
-            const int t1 = (m.key / g.ntile2) % g.ntile, t2 = m.key % g.ntile2;
-            const long long o1 = g.gmin + (long long)t1 * g.T, o2 = g.gmin + (long long)t2 * g.T2;
-            const int lo_r = fxq ? r0 : cx - HW, nr = fxq ? W : W + 1;
-            const int lo_c = fyq ? c0 : cy - HW, nc = fyq ? W : W + 1;
-            const float px = (float)fxq * (1.0f / 16777216.0f), py = (float)fyq * (1.0f / 16777216.0f);
-            float2* plane = P.planes + (long long)(slab - P.slab_lo) * GG;
-            for (int cidx = fi; cidx < nr * nc; cidx += 8) {
-                const int rr = lo_r + cidx / nc, cc = lo_c + cidx % nc;
-                const long long g1 = o1 + rr, g2 = o2 + cc;
-                if (g1 < g.gmin || g2 < g.gmin || g1 > g.gmax || g2 > g.gmax) continue;
-                const float x = ((float)(rr - cx) - px) / (float)HW;
-                const float y = ((float)(cc - cy) - py) / (float)HW;
-                const float kv = es_exact(poly.beta, x) * es_exact(poly.beta, y);
-                const float sg = ((g1 + g2) & 1) ? -kv : kv;
-                red_add_v2(plane + (g1 - g.gmin) * g.G + (g2 - g.gmin), sg * r.vre, sg * r.vim);
-            }
-        }
-        // ---- merge the intervals closed two or more K-blocks ago (their MMAs are done by now)
-        {
-            int k = 0;
-            while (k < np && (pend[k] >> 8) <= kb - 2) {
-                if (!wait_kb(pend[k] >> 8)) {
-                    fail = true;
+    } else {
+        // ============================ epilogue ============================
+        const int q = warp & 3;  // TMEM lane quarter: accumulator rows 16q .. 16q + 15 in lanes 0..15
+        const uint32_t lane_addr = (uint32_t)(32 * q) << 16;
+        unsigned int run_valid = 0;
+        for (unsigned int e = 0;; ++e) {
+            bool ok = true;
+            if (lane == 0) ok = wait_at_least(&S.ev_published, e + 1, abort_flag);
+            if (!__shfl_sync(0xffffffffu, (int)ok, 0)) {
+                if (lane == 0 && !*abort_flag) {
                     atomicOr(P.status, 8u);
+                    *abort_flag = 1;
+                }
+                break;
+            }
+            const Event ev = S.events[e % kEventRing];
+            if (ev.type == kEvExit) break;
+            if (ev.type == kEvMerge) {
+                bool dn = mbar_wait(smem_u32(&S.fdone[ev.buf]), (uint32_t)ev.parity, abort_flag);
+                dn = __all_sync(0xffffffffu, dn);
+                if (!dn) {
+                    if (lane == 0 && !*abort_flag) {
+                        atomicOr(P.status, 8u);
+                        *abort_flag = 1;
+                    }
+                    break;
                 }
                 tc_fence_after();
-                merge(pend[k]);
-                ++k;
-            }
-            if (k > 0) {
-                for (int i = k; i < np; ++i) pend[i - k] = pend[i];
-                np -= k;
+                float f[32];
+                tmem_ld32(tmem + lane_addr + (uint32_t)(kFreshCol0 + kN * ev.buf), f);
+                const uint32_t ra = tmem + lane_addr + (uint32_t)(kN * ev.blk);
+                if ((run_valid >> ev.blk) & 1u) {
+                    float rv[32];
+                    tmem_ld32(ra, rv);
+#pragma unroll
+                    for (int jj = 0; jj < 32; ++jj) f[jj] += rv[jj];  // FP32 round-to-nearest
+                }
+                tmem_st32(ra, f);
+                run_valid |= 1u << ev.blk;
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(smem_u32(&S.ffree[ev.buf]));
+            } else {  // flush the super-tile of ev.key
+                tc_fence_after();
+                const int slab = ev.key / tiles2;
+                const int t1 = (ev.key / g.ntile2) % g.ntile;
+                const int t2b = (ev.key % g.ntile2) / kTcBlocks * kTcBlocks;
+                const int row = 16 * q + (lane & 15);
+                const long long g1 = g.gmin + (long long)t1 * g.T + row;
+                const bool row_ok = lane < 16 && g1 <= g.gmax;
+                const long long o2 = g.gmin + (long long)t2b * g.T2;  // grid column of block 0, column 0
+                float2* plane = P.planes + (long long)(slab - P.slab_lo) * GG + (g1 - g.gmin) * g.G;
+                float cre[8], cim[8];
+#pragma unroll
+                for (int jj = 0; jj < 8; ++jj) { cre[jj] = 0.0f; cim[jj] = 0.0f; }
+                auto emit = [&](long long g2, float re, float im) {
+                    if (row_ok && g2 <= g.gmax && (re != 0.0f || im != 0.0f)) {
+                        const float sg = ((g1 + g2) & 1) ? -inv_scale : inv_scale;
+                        red_add_v2(plane + (g2 - g.gmin), sg * re, sg * im);
+                    }
+                };
+#pragma unroll 1
+                for (int c = 0; c < kTcBlocks; ++c) {
+                    float v[32];
+                    if ((run_valid >> c) & 1u) {
+                        tmem_ld32(tmem + lane_addr + (uint32_t)(kN * c), v);
+                    } else {
+#pragma unroll
+                        for (int jj = 0; jj < 32; ++jj) v[jj] = 0.0f;
+                    }
+#pragma unroll
+                    for (int jj = 0; jj < 8; ++jj) {
+                        emit(o2 + 8 * c + jj, cre[jj] + v[jj], cim[jj] + v[16 + jj]);
+                        cre[jj] = v[8 + jj];
+                        cim[jj] = v[24 + jj];
+                    }
+                }
+#pragma unroll
+                for (int jj = 0; jj < 8; ++jj) emit(o2 + 8 * kTcBlocks + jj, cre[jj], cim[jj]);
+                run_valid = 0;
                 tc_fence_before();
             }
+            __syncwarp();
+            if (lane == 0) st_release(&S.ev_consumed[q], e + 1);
         }
-        if (warp == 0) cp_async_wait<kAhead - 1>();  // records of K-block kb + 1 have landed
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        if (__syncthreads_or(fail)) {
-            aborted = true;
-            break;
-        }
-        if (tid == 0) {
-            tc_fence_after();
-            const uint32_t d = tmem + (uint32_t)(kFreshCol0 + kBlockCols * ob);
-            const uint32_t ah = smem_u32(A_hi), al = smem_u32(A_lo), bh = smem_u32(B_hi), bl = smem_u32(B_lo);
-            uint32_t acc = on > 0 ? 1u : 0u;
-#pragma unroll
-            for (int k = 0; k < kKB / 16; ++k) {  // 16-element K steps: +256 bytes
-                const uint32_t ko = (uint32_t)k * 256u;
-                mma_f16(d, smem_desc(ah + ko), smem_desc(bh + ko), acc);
-                acc = 1u;
-                mma_f16(d, smem_desc(ah + ko), smem_desc(bl + ko), 1u);
-                mma_f16(d, smem_desc(al + ko), smem_desc(bh + ko), 1u);
-            }
-            mma_commit(smem_u32(&mbar[s]));
-        }
-        ++on;
-        ++kb;
+        if (lane == 0) st_release(&S.ev_consumed[q], 0xFFFFFFF0u);  // never block the event ring again
     }
-    if (cur_st >= 0 && !aborted) flush();
 
-    // ---- teardown: no copies or MMAs in flight, then free the tensor memory
-    if (warp == 0) cp_async_wait<0>();
-    if (kb > 0) {
-        const int s = (kb - 1) % kStages;
-        if (!mbar_wait(smem_u32(&mbar[s]), (uint32_t)(((kb - 1) / kStages) & 1))) atomicOr(P.status, 4u);
-    }
+    // ---- teardown: all roles done, no MMA in flight; free the tensor memory
     tc_fence_before();
     __syncthreads();
-    if (warp == 0) {
+    if (warp == kMmaWarp) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
     }
@@ -591,36 +883,36 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
 
 }  // namespace
 
-int launch_grid_tc(const SampleRec* d_rec, const unsigned int* d_offsets, int n_keys, int key_lo, int key_hi,
-                   int slab_lo, const GridGeom& g, const EsPoly& poly, float2* d_planes,
-                   const unsigned int* d_vmax, unsigned int* d_status, int sm_count, cudaStream_t st) {
+int launch_grid_tc(const SampleRec* d_rec, const unsigned int* d_offsets, const unsigned int* d_kb_offsets,
+                   int n_keys, int key_lo, int key_hi, int slab_lo, const GridGeom& g, const EsPoly& poly,
+                   float2* d_planes, const unsigned int* d_vmax, unsigned int* d_status, int sm_count,
+                   cudaStream_t st) {
     if (key_lo < 0 || key_hi > n_keys || key_lo >= key_hi) {
         set_error("tensor-core gridder: bad key range");
         return SVDI_ERR_INTERNAL;
     }
     if (g.W > 8 || (g.W & 1) || g.T != kTcTileRows || g.T2 != kTcTileCols || (g.ntile2 % kTcBlocks) != 0 ||
         (key_lo % kTcBlocks) != 0) {
-        set_error("tensor-core gridder: needs even support <= 8 and 120 x 8 tiles in groups of 8");
+        set_error("tensor-core gridder: needs even support <= 8 and 56 x 8 tiles in groups of 4");
         return SVDI_ERR_UNSUPPORTED;
     }
-    static bool configured = false;
-    if (!configured) {
+    static int per_sm = -1;  // configured and checked once per process
+    if (per_sm < 0) {
         SVDI_CUDA(cudaFuncSetAttribute(k_grid_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
-        // without a carveout preference the occupancy query assumes one CTA per SM
         SVDI_CUDA(cudaFuncSetAttribute(k_grid_tc, cudaFuncAttributePreferredSharedMemoryCarveout,
                                        (int)cudaSharedmemCarveoutMaxShared));
-        configured = true;
+        int n = 0;
+        SVDI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_grid_tc, kThreads, kSmemBytes));
+        per_sm = n;
     }
-    // two CTAs per SM by design (2 x 256 of the SM's 512 TMEM columns; shared memory admits no third)
-    int per_sm = 0;
-    SVDI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grid_tc, kThreads, kSmemBytes));
     if (per_sm < 1) {
         set_error("tensor-core gridder: kernel does not fit on an SM");
         return SVDI_ERR_UNSUPPORTED;
     }
-    per_sm = 2;
-    TcParams P{d_rec, d_offsets, d_vmax, d_planes, d_status, key_lo, key_hi, slab_lo};
-    k_grid_tc<<<sm_count * per_sm, kThreads, kSmemBytes, st>>>(P, g, poly);
+    TcParams P{d_rec, d_offsets, d_kb_offsets, d_vmax, d_planes, d_status, key_lo, key_hi, slab_lo};
+    // two CTAs per SM (two MMA-issuing threads: one thread issues a skinny MMA every ~46 clk, the
+    // tensor pipe takes one every ~26), each with 256 of the SM's 512 TMEM columns
+    k_grid_tc<<<2 * sm_count, kThreads, kSmemBytes, st>>>(P, g, poly);
     SVDI_LAUNCHED();
     return SVDI_OK;
 }

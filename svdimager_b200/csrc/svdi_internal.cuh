@@ -131,20 +131,24 @@ struct SampleSource {
 int launch_histogram(const SampleSource& src, const GridGeom& g, const SlabParams& sp,
                      unsigned int* d_counts, int n_keys, unsigned long long* d_dropped,
                      cudaStream_t st);
+// d_kb_offsets (optional): exclusive scan of ceil(count / kb_size) per key, n_keys + 1 entries
 int launch_scan(const unsigned int* d_counts, int n_keys, unsigned int* d_offsets,
-                unsigned int* d_cursor, cudaStream_t st);
+                unsigned int* d_cursor, cudaStream_t st, unsigned int* d_kb_offsets = nullptr,
+                int kb_size = 32);
 // d_vmax (optional, zeroed by the caller): receives max(|vre|, |vim|) over the records as float bits
 int launch_scatter(const SampleSource& src, const GridGeom& g, const SlabParams& sp,
                    unsigned int* d_cursor, int n_keys, SampleRec* d_rec, float* d_rec_s,
                    unsigned int* d_vmax, cudaStream_t st);
 
 // gridder_tc.cu: split-precision tcgen05 gridder (one moment plane, support <= 8)
-constexpr int kTcTileRows = 120;   // tile rows: footprint origins; 128-row accumulator with halo
+constexpr int kTcTileRows = 56;    // tile rows: footprint origins; 64-row accumulator with halo
 constexpr int kTcTileCols = 8;     // tile columns: footprint origins of one column block
 constexpr int kTcBlocks = 4;       // column blocks per super-tile accumulator (4 x 32 TMEM columns)
-int launch_grid_tc(const SampleRec* d_rec, const unsigned int* d_offsets, int n_keys, int key_lo,
-                   int key_hi, int slab_lo, const GridGeom& g, const EsPoly& poly, float2* d_planes,
-                   const unsigned int* d_vmax, unsigned int* d_status, int sm_count, cudaStream_t st);
+constexpr int kTcKBlock = 32;      // records per K-block (one MMA pair of K steps)
+int launch_grid_tc(const SampleRec* d_rec, const unsigned int* d_offsets, const unsigned int* d_kb_offsets,
+                   int n_keys, int key_lo, int key_hi, int slab_lo, const GridGeom& g, const EsPoly& poly,
+                   float2* d_planes, const unsigned int* d_vmax, unsigned int* d_status, int sm_count,
+                   cudaStream_t st);
 
 // gridder.cu
 int launch_grid_fp32(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d_offsets,

@@ -2,7 +2,7 @@
 accumulation in tensor memory) with the oracle, with the FP32 gridder and with the FP64 direct DFT.
 
 The tensor-core path grids one moment plane per w-slab (K = 1), so these tests fix K = 1 on both
-sides. Tile binning (120 x 8 tiles) stays bit-exact. Grid planes: each product of the split
+sides. Tile binning (56 x 8 tiles) stays bit-exact. Grid planes: each product of the split
 operands carries <= ~2^-21 relative error (FP16 hi + lo of both factors, the lo * lo term
 dropped), plus the ES polynomial (<= 1e-7); planes are compared at TC_GRID_TOL relative L2.
 Images: 1e-5 relative RMS, as for the FP32 path."""
@@ -37,7 +37,7 @@ def tc_run(cuda_device, small_snapshot):
 def test_tc_path_is_used(tc_run):
     st = tc_run["stats"]
     assert st["used_tc"] == 1
-    assert st["tile"] == 120 and st["tile_cols"] == 8
+    assert st["tile"] == 56 and st["tile_cols"] == 8
     assert st["num_terms"] == 1
 
 
