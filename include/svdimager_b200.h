@@ -192,6 +192,34 @@ typedef struct svdi_stats {
 
 int svdi_engine_last_stats(const svdi_engine* e, svdi_stats* out);
 
+/* FP64 direct DFT of the engine's last snapshot at pixels (px[i], py[i]) of its N x N image:
+ * |sum_k Re(V_k e^{2 pi i r_k . t})| / |det V| / N_s over the samples the gridder kept (the same
+ * inclusion rule, bit for bit), i.e. the rotated-frame image before reprojection (presplat = 1).
+ * NaN where the pixel has no valid direction. An accuracy probe for any image, used by the
+ * autotuner; no counterpart in the reference (its only check is the image itself). */
+int svdi_engine_dft_pixels(svdi_engine* e, const int64_t* px, const int64_t* py, size_t npix, double* out);
+
+/* ---- batches: many snapshots imaged by one CUDA-graph launch ------------------------------
+ * No counterpart in the reference, whose driver images one snapshot per process
+ * (SVDIntegratedImager.cu:1773-1854). svdi_batch_create images every snapshot once with the
+ * engine (recording each snapshot's host decisions: rotation, w range, slab and Chebyshev
+ * configuration, and sizing the engine's buffers for the largest), then captures the device work
+ * of all snapshots into one CUDA graph. svdi_batch_launch replays it with one cudaGraphLaunch.
+ *   snapshots: device-resident descriptors as for svdi_engine_image_device; their arrays must
+ *              stay allocated at the same addresses (refill them in place to image new data of
+ *              the same layout, sizes and w range: the recorded plans are reused as they are);
+ *   d_images:  num_snapshots x N x N floats on the device, image s at d_images + s N^2.
+ * The engine holds one batch at a time and must not image anything else while a launch is in
+ * flight (the graph uses its buffers). */
+typedef struct svdi_batch svdi_batch;
+int svdi_batch_create(svdi_engine* e, const svdi_host_ms* snapshots, size_t num_snapshots, size_t image_size,
+                      float cell_size, float* d_images, svdi_batch** out);
+int svdi_batch_launch(svdi_batch* b, void* cuda_stream);  /* asynchronous; NULL: the engine's stream */
+int svdi_batch_check(svdi_batch* b);   /* waits for the last launch; SVDI_ERR_INTERNAL if a tensor-core
+                                          gridder wait gave up in any snapshot                        */
+int svdi_batch_plan(const svdi_batch* b, size_t index, int* num_slabs, int* num_terms);
+void svdi_batch_destroy(svdi_batch* b);
+
 /* Intermediate buffers of the last call, for inspection and tests (device-to-host copy). */
 #define SVDI_BUF_VIS_REAL 0      /* float [N_s] collapsed visibilities                         */
 #define SVDI_BUF_VIS_IMAG 1

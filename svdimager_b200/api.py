@@ -36,7 +36,8 @@ EXPORTED_SYMBOLS = (
     "svdi_engine_last_stats", "svdi_engine_buffer_size", "svdi_engine_copy_buffer",
     "svdi_kernel_launch_count", "svdi_bin_samples_noalloc", "svdi_server_create",
     "svdi_server_submit", "svdi_server_wait", "svdi_server_poll", "svdi_server_stats",
-    "svdi_server_destroy", "_Z6FIpipePfS_S_S_S_mmf",
+    "svdi_server_destroy", "svdi_engine_dft_pixels", "svdi_batch_create", "svdi_batch_launch",
+    "svdi_batch_check", "svdi_batch_plan", "svdi_batch_destroy", "_Z6FIpipePfS_S_S_S_mmf",
 )
 NOALLOC_MAX_KEYS = 16384
 
@@ -158,6 +159,13 @@ def lib():
                                         ctypes.POINTER(ctypes.c_uint64)]
         L.svdi_server_destroy.argtypes = [P]
         L.svdi_server_destroy.restype = None
+        L.svdi_engine_dft_pixels.argtypes = [P, P, P, sz, P]
+        L.svdi_batch_create.argtypes = [P, ctypes.POINTER(HostMS), sz, sz, f, P, ctypes.POINTER(P)]
+        L.svdi_batch_launch.argtypes = [P, P]
+        L.svdi_batch_check.argtypes = [P]
+        L.svdi_batch_plan.argtypes = [P, sz, ctypes.POINTER(i), ctypes.POINTER(i)]
+        L.svdi_batch_destroy.argtypes = [P]
+        L.svdi_batch_destroy.restype = None
         _lib = L
     return _lib
 
@@ -292,6 +300,62 @@ class Engine:
         s = Stats()
         _check(lib().svdi_engine_last_stats(self._h, ctypes.byref(s)))
         return s.as_dict()
+
+    def dft_pixels(self, px, py) -> np.ndarray:
+        """FP64 direct DFT of the last snapshot at pixels (px, py): the rotated-frame image value
+        before reprojection (compare with an image made with presplat=1); NaN outside the
+        projection."""
+        x = np.ascontiguousarray(px, np.int64)
+        y = np.ascontiguousarray(py, np.int64)
+        out = np.zeros(len(x), np.float64)
+        _check(lib().svdi_engine_dft_pixels(self._h, _ptr(x), _ptr(y), len(x), _ptr(out)))
+        return out
+
+
+class Batch:
+    """Many device-resident snapshots imaged by one CUDA-graph launch (svdi_batch_*). Creating it
+    images every snapshot once (recording each snapshot's plan) and captures the graph; launch()
+    replays it. `snapshots` are device descriptors (device_ms); `images_ptr` is a device buffer of
+    len(snapshots) x N x N floats. Keep the engine, the snapshots' arrays and the images alive
+    while the batch exists."""
+
+    def __init__(self, engine: "Engine", snapshots, image_size: int, cell_size: float, images_ptr: int):
+        arr = (HostMS * len(snapshots))(*snapshots)
+        h = ctypes.c_void_p()
+        _check(lib().svdi_batch_create(engine._h, arr, len(snapshots), int(image_size), float(cell_size),
+                                       ctypes.c_void_p(images_ptr), ctypes.byref(h)))
+        self._h = h
+        self._arr = arr
+        self.engine = engine
+        self.num = len(snapshots)
+
+    def launch(self, stream_ptr: int = 0):
+        _check(lib().svdi_batch_launch(self._h, ctypes.c_void_p(stream_ptr)))
+
+    def check(self):
+        _check(lib().svdi_batch_check(self._h))
+
+    def plan(self, index: int):
+        ns, nt = ctypes.c_int(), ctypes.c_int()
+        _check(lib().svdi_batch_plan(self._h, int(index), ctypes.byref(ns), ctypes.byref(nt)))
+        return {"num_slabs": ns.value, "num_terms": nt.value}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().svdi_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def FIpipe(Visreal, Visimag, Bin, Vin, image_size: int, cell_size: float,

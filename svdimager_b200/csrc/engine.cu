@@ -121,6 +121,15 @@ struct svdi_engine {
     double poly_beta = 0.0;
     svdi_stats last{};
     cudaEvent_t ev[8] = {};
+    // the last imaging call's sample source and geometry (for the accuracy probe)
+    svdi::SampleSource last_src{};
+    svdi::GridGeom last_g{};
+    svdi::SlabParams last_sp{};
+    long long last_N = 0;
+    double last_cell = 0.0;
+    bool have_last = false;
+    svdi::DevBuf probe;
+    bool batch_bound = false;  // a batch's captured graph refers to this engine's buffers
 
     ~svdi_engine() {
         if (device >= 0) cudaSetDevice(device);
@@ -371,32 +380,57 @@ size_t batch_slabs_for(svdi_engine* e, int nslab, int K, long long G) {
     return std::min<size_t>(nslab, std::max<size_t>(1, budget / per_slab));
 }
 
+// The host decisions of one snapshot: everything image_core reads back from the device before
+// it can launch the gridding (basis determinant, w range, slab and Chebyshev configuration,
+// slabs per batch). With a fixed plan image_core issues device work only (no synchronisation,
+// no allocation when the buffers are already large enough), so it can be captured in a graph.
+struct ExecPlan {
+    float inv_det = 0.0f;
+    SlabParams sp{};
+    double alpha_max = 0, slab_alpha = 0, r3min = 0, r3max = 0, mt3 = 0;
+    size_t bslabs = 1;
+};
+
 // Imaging core: given vin64 and sample source on the device, produce the image in d_out.
+// fixed: replay a recorded plan (device work only; *d_status_out receives the tensor-core
+// gridder's status word); record: store this call's plan.
 int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, float cell_f,
-               float* d_out) {
+               float* d_out, const ExecPlan* fixed = nullptr, ExecPlan* record = nullptr,
+               unsigned int* d_status_out = nullptr) {
     cudaStream_t st = e->stream;
     const svdi_options& o = e->opt;
     const double cell = (double)cell_f;
     const long long n = src.n;
-    // statistics: max |t3|, then one small read
-    SVDI_TRY(launch_t3_stats(e->vin64.as<double>(), N, cell, e->partial.as<double>(), kPartialCap,
-                             e->stats.as<double>(), st));
-    SVDI_CUDA(cudaMemcpyAsync(e->h_stats, e->stats.p, ST_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st));
-    SVDI_CUDA(cudaMemcpyAsync(e->last.vin, e->vin64.p, 9 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    SVDI_CUDA(cudaStreamSynchronize(st));
-    const double r3min = e->h_stats[ST_R3_MIN], r3max = e->h_stats[ST_R3_MAX];
-    const double mt3 = e->h_stats[ST_MAX_T3];
-    const double* V = e->last.vin;
-    const double det = std::fabs(V[0] * V[4] - V[1] * V[3]);
-    if (!(det > 0.0) || !std::isfinite(det)) {
-        set_error("degenerate basis: |V00 V11 - V01 V10| is zero");
-        return SVDI_ERR_INVALID_ARGUMENT;
-    }
-    src.inv_det = (float)(1.0 / det);
-
+    const bool timed = fixed == nullptr;  // events, statistics and status read-back
     SlabParams sp{};
-    double alpha_max = 0, slab_alpha = 0;
-    SVDI_TRY(choose_slabs(e, archive, r3min, r3max, mt3, sp, alpha_max, slab_alpha));
+    double alpha_max = 0, slab_alpha = 0, r3min = 0, r3max = 0, mt3 = 0;
+    if (fixed) {
+        src.inv_det = fixed->inv_det;
+        sp = fixed->sp;
+        alpha_max = fixed->alpha_max;
+        slab_alpha = fixed->slab_alpha;
+        r3min = fixed->r3min;
+        r3max = fixed->r3max;
+        mt3 = fixed->mt3;
+    } else {
+        // statistics: max |t3|, then one small read
+        SVDI_TRY(launch_t3_stats(e->vin64.as<double>(), N, cell, e->partial.as<double>(), kPartialCap,
+                                 e->stats.as<double>(), st));
+        SVDI_CUDA(cudaMemcpyAsync(e->h_stats, e->stats.p, ST_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st));
+        SVDI_CUDA(cudaMemcpyAsync(e->last.vin, e->vin64.p, 9 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        SVDI_CUDA(cudaStreamSynchronize(st));
+        r3min = e->h_stats[ST_R3_MIN];
+        r3max = e->h_stats[ST_R3_MAX];
+        mt3 = e->h_stats[ST_MAX_T3];
+        const double* V = e->last.vin;
+        const double det = std::fabs(V[0] * V[4] - V[1] * V[3]);
+        if (!(det > 0.0) || !std::isfinite(det)) {
+            set_error("degenerate basis: |V00 V11 - V01 V10| is zero");
+            return SVDI_ERR_INVALID_ARGUMENT;
+        }
+        src.inv_det = (float)(1.0 / det);
+        SVDI_TRY(choose_slabs(e, archive, r3min, r3max, mt3, sp, alpha_max, slab_alpha));
+    }
 
     GridGeom g{};
     g.G = grid_size(N, o.sigma);
@@ -436,7 +470,7 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     }
 
     // binning
-    SVDI_CUDA(cudaEventRecord(e->ev[1], st));
+    if (timed) SVDI_CUDA(cudaEventRecord(e->ev[1], st));
     SVDI_TRY(e->counts.ensure((size_t)n_keys * 4));
     SVDI_TRY(e->offsets.ensure((size_t)(n_keys + 1) * 4));
     SVDI_TRY(e->cursor.ensure((size_t)n_keys * 4));
@@ -460,10 +494,20 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     SVDI_TRY(launch_scatter(src, g, sp, e->cursor.as<unsigned int>(), n_keys, e->rec.as<SampleRec>(),
                             need_s ? e->rec_s.as<float>() : nullptr,
                             use_tc ? e->tc_status.as<unsigned int>() + 1 : nullptr, st));
-    SVDI_CUDA(cudaEventRecord(e->ev[2], st));
+    if (timed) SVDI_CUDA(cudaEventRecord(e->ev[2], st));
 
     // slab batches: grid -> FFT -> recombine
-    const size_t bslabs = batch_slabs_for(e, sp.nslab, sp.K, g.G);
+    const size_t bslabs = fixed ? fixed->bslabs : batch_slabs_for(e, sp.nslab, sp.K, g.G);
+    if (record) {
+        record->inv_det = src.inv_det;
+        record->sp = sp;
+        record->alpha_max = alpha_max;
+        record->slab_alpha = slab_alpha;
+        record->r3min = r3min;
+        record->r3max = r3max;
+        record->mt3 = mt3;
+        record->bslabs = bslabs;
+    }
     const int planes_per_batch = (int)bslabs * sp.K;
     const size_t plane_bytes = (size_t)g.G * g.G * sizeof(float2);
     SVDI_TRY(e->planes.ensure(plane_bytes * planes_per_batch));
@@ -475,7 +519,7 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     for (int s0 = 0; s0 < sp.nslab; s0 += (int)bslabs) {
         const int s1 = std::min(sp.nslab, s0 + (int)bslabs);
         SlabParams bp = sp;
-        SVDI_CUDA(cudaEventRecord(e->ev[3], st));
+        if (timed) SVDI_CUDA(cudaEventRecord(e->ev[3], st));
         SVDI_CUDA(cudaMemsetAsync(e->planes.p, 0, plane_bytes * planes_per_batch, st));
         const int tiles2 = g.ntile * g.ntile2;
         if (use_tc) {
@@ -495,15 +539,16 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
                                       cudaMemcpyDeviceToDevice, st));
             e->sz_grid = plane_bytes * (size_t)(std::min(sp.nslab, (int)bslabs) * sp.K);
         }
-        SVDI_CUDA(cudaEventRecord(e->ev[4], st));
+        if (timed) SVDI_CUDA(cudaEventRecord(e->ev[4], st));
         SVDI_CUFFT(cufftExecC2C(plan, e->planes.as<cufftComplex>(), e->planes.as<cufftComplex>(), CUFFT_INVERSE));
-        SVDI_CUDA(cudaEventRecord(e->ev[5], st));
+        if (timed) SVDI_CUDA(cudaEventRecord(e->ev[5], st));
         // recombine the slabs of this batch (moment plane index relative to the batch)
         bp.nslab = s1 - s0;
         bp.r3_min = sp.r3_min + (double)s0 * sp.slab_width;
         SVDI_TRY(launch_recombine(e->planes.as<float2>(), g, N, cell, e->vin64.as<double>(), bp,
                                   e->corr.as<float>(), 1.0 / (double)n, o.reprojection, o.presplat, d_out,
                                   st));
+        if (!timed) continue;
         SVDI_CUDA(cudaEventRecord(e->ev[6], st));
         SVDI_CUDA(cudaEventSynchronize(e->ev[6]));
         float a = 0, b = 0, c = 0;
@@ -513,6 +558,22 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
         ms_grid += a;
         ms_fft += b;
         ms_img += c;
+    }
+    e->last_src = src;
+    e->last_g = g;
+    e->last_sp = sp;
+    e->last_N = N;
+    e->last_cell = cell;
+    e->have_last = true;
+    if (!timed) {
+        if (d_status_out) {
+            if (use_tc)
+                SVDI_CUDA(cudaMemcpyAsync(d_status_out, e->tc_status.p, sizeof(unsigned int),
+                                          cudaMemcpyDeviceToDevice, st));
+            else
+                SVDI_CUDA(cudaMemsetAsync(d_status_out, 0, sizeof(unsigned int), st));
+        }
+        return SVDI_OK;
     }
     unsigned long long ndrop = 0;
     unsigned int tc_status = 0;
@@ -621,11 +682,13 @@ int check_options(const svdi_options& o) {
 }
 
 // Main path on device-resident raw snapshot arrays.
-int main_path_device(svdi_engine* e, const svdi_host_ms* d, size_t N, float cell, float* d_out) {
+int main_path_device(svdi_engine* e, const svdi_host_ms* d, size_t N, float cell, float* d_out,
+                     const ExecPlan* fixed = nullptr, ExecPlan* record = nullptr,
+                     unsigned int* d_status_out = nullptr) {
     cudaStream_t st = e->stream;
     const long long R = (long long)d->num_rows, C = (long long)d->num_channels;
     const long long n = (long long)d->num_samples;
-    SVDI_CUDA(cudaEventRecord(e->ev[0], st));
+    if (!fixed) SVDI_CUDA(cudaEventRecord(e->ev[0], st));
     SVDI_TRY(e->vr.ensure(n * 4));
     SVDI_TRY(e->vi.ensure(n * 4));
     SVDI_TRY(e->q.ensure(R * 24));
@@ -648,7 +711,8 @@ int main_path_device(svdi_engine* e, const svdi_host_ms* d, size_t N, float cell
     src.n = n;
     e->sz_q = (size_t)R * 24;
     e->sz_s = (size_t)C * 8;
-    SVDI_TRY(image_core(e, false, src, (long long)N, cell, d_out));
+    SVDI_TRY(image_core(e, false, src, (long long)N, cell, d_out, fixed, record, d_status_out));
+    if (fixed) return SVDI_OK;
     float mp = 0, mt = 0;
     cudaEventElapsedTime(&mp, e->ev[0], e->ev[1]);
     SVDI_CUDA(cudaEventRecord(e->ev[7], st));
@@ -1037,3 +1101,187 @@ int FIpipe(float* Visreal, float* Visimag, float* Bin, float* Vin, float* dirty_
            size_t image_size, float cell_size) {
     return svdi_fipipe(Visreal, Visimag, Bin, Vin, dirty_image, num_baselines, image_size, cell_size);
 }
+
+// ---------------------------------------------------------------------------------------------
+// Batches: many snapshots imaged by one CUDA-graph launch (no counterpart in the reference,
+// whose driver images one snapshot per process, SVDIntegratedImager.cu:1773-1854).
+// ---------------------------------------------------------------------------------------------
+struct svdi_batch {
+    svdi_engine* e = nullptr;
+    std::vector<svdi_host_ms> snaps;
+    std::vector<svdi::ExecPlan> plans;
+    size_t N = 0;
+    float cell = 0.0f;
+    float* d_images = nullptr;
+    svdi::DevBuf status;  // per snapshot: the tensor-core gridder's status word
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t last_stream = nullptr;
+    ~svdi_batch() {
+        if (e) cudaSetDevice(e->device);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (e) e->batch_bound = false;
+    }
+};
+
+extern "C" {
+
+int svdi_batch_create(svdi_engine* e, const svdi_host_ms* snapshots, size_t num_snapshots, size_t image_size,
+                      float cell_size, float* d_images, svdi_batch** out) {
+    using namespace svdi;
+    g_last_error.clear();
+    if (!e || !snapshots || !d_images || !out) {
+        set_error("null argument");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    if (num_snapshots == 0) {
+        set_error("a batch needs at least one snapshot");
+        return SVDI_ERR_EMPTY_INPUT;
+    }
+    SVDI_TRY(check_image_args(image_size, cell_size));
+    for (size_t s = 0; s < num_snapshots; ++s) SVDI_TRY(check_ms(&snapshots[s]));
+    if (e->opt.keep_grid) {
+        set_error("batches do not keep grids: create the engine with keep_grid = 0");
+        return SVDI_ERR_UNSUPPORTED;
+    }
+    std::lock_guard<std::mutex> lk(e->mu);
+    if (e->batch_bound) {
+        set_error("this engine already holds a batch; destroy it first");
+        return SVDI_ERR_UNSUPPORTED;
+    }
+    SVDI_CUDA(cudaSetDevice(e->device));
+    std::unique_ptr<svdi_batch> b(new svdi_batch());
+    b->snaps.assign(snapshots, snapshots + num_snapshots);
+    b->plans.resize(num_snapshots);
+    b->N = image_size;
+    b->cell = cell_size;
+    b->d_images = d_images;
+    SVDI_TRY(b->status.ensure(num_snapshots * sizeof(unsigned int)));
+    const size_t NN = image_size * image_size;
+    // plan: one ordinary pass per snapshot records its host decisions and sizes every buffer
+    for (size_t s = 0; s < num_snapshots; ++s)
+        SVDI_TRY(main_path_device(e, &b->snaps[s], image_size, cell_size, d_images + s * NN, nullptr, &b->plans[s]));
+    SVDI_CUDA(cudaStreamSynchronize(e->stream));
+    // capture the device work of every snapshot with its plan
+    SVDI_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = SVDI_OK;
+    for (size_t s = 0; s < num_snapshots && rc == SVDI_OK; ++s)
+        rc = main_path_device(e, &b->snaps[s], image_size, cell_size, d_images + s * NN, &b->plans[s], nullptr,
+                              b->status.as<unsigned int>() + s);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(e->stream, &graph);
+    if (rc != SVDI_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (ce != cudaSuccess || !graph) {
+        set_error(std::string("graph capture failed: ") + cudaGetErrorString(ce));
+        cudaGetLastError();
+        return SVDI_ERR_CUDA;
+    }
+    b->graph = graph;
+    SVDI_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    b->e = e;
+    e->batch_bound = true;
+    *out = b.release();
+    return SVDI_OK;
+}
+
+int svdi_batch_launch(svdi_batch* b, void* cuda_stream) {
+    using namespace svdi;
+    g_last_error.clear();
+    if (!b || !b->exec) {
+        set_error("null batch");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    SVDI_CUDA(cudaSetDevice(b->e->device));
+    cudaStream_t st = cuda_stream ? (cudaStream_t)cuda_stream : b->e->stream;
+    SVDI_CUDA(cudaGraphLaunch(b->exec, st));
+    b->last_stream = st;
+    return SVDI_OK;
+}
+
+int svdi_batch_check(svdi_batch* b) {
+    using namespace svdi;
+    g_last_error.clear();
+    if (!b) {
+        set_error("null batch");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    SVDI_CUDA(cudaSetDevice(b->e->device));
+    if (b->last_stream) SVDI_CUDA(cudaStreamSynchronize(b->last_stream));
+    std::vector<unsigned int> st(b->snaps.size());
+    SVDI_CUDA(cudaMemcpy(st.data(), b->status.p, st.size() * sizeof(unsigned int), cudaMemcpyDeviceToHost));
+    for (size_t s = 0; s < st.size(); ++s)
+        if (st[s]) {
+            set_error("snapshot " + std::to_string(s) + ": the tensor-core gridder gave up waiting (status " +
+                      std::to_string(st[s]) + "); its image is incomplete");
+            return SVDI_ERR_INTERNAL;
+        }
+    return SVDI_OK;
+}
+
+int svdi_batch_plan(const svdi_batch* b, size_t index, int* num_slabs, int* num_terms) {
+    using namespace svdi;
+    if (!b || index >= b->plans.size()) {
+        set_error("bad batch or snapshot index");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    if (num_slabs) *num_slabs = b->plans[index].sp.nslab;
+    if (num_terms) *num_terms = b->plans[index].sp.K;
+    return SVDI_OK;
+}
+
+void svdi_batch_destroy(svdi_batch* b) { delete b; }
+
+int svdi_engine_dft_pixels(svdi_engine* e, const int64_t* px, const int64_t* py, size_t npix, double* out) {
+    using namespace svdi;
+    g_last_error.clear();
+    if (!e || !px || !py || !out) {
+        set_error("null argument");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    if (npix == 0) return SVDI_OK;
+    if (npix > 65536) {
+        set_error("at most 65536 pixels per call");
+        return SVDI_ERR_UNSUPPORTED;
+    }
+    std::lock_guard<std::mutex> lk(e->mu);
+    if (!e->have_last) {
+        set_error("no image has been made with this engine yet");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    const long long N = e->last_N;
+    for (size_t p = 0; p < npix; ++p)
+        if (px[p] < 0 || py[p] < 0 || px[p] >= N || py[p] >= N) {
+            set_error("pixel index outside the image");
+            return SVDI_ERR_INVALID_ARGUMENT;
+        }
+    SVDI_CUDA(cudaSetDevice(e->device));
+    cudaStream_t st = e->stream;
+    SVDI_TRY(e->probe.ensure(npix * 3 * sizeof(long long)));
+    long long* d_px = e->probe.as<long long>();
+    long long* d_py = d_px + npix;
+    double* d_acc = reinterpret_cast<double*>(d_py + npix);
+    SVDI_CUDA(cudaMemcpyAsync(d_px, px, npix * 8, cudaMemcpyHostToDevice, st));
+    SVDI_CUDA(cudaMemcpyAsync(d_py, py, npix * 8, cudaMemcpyHostToDevice, st));
+    SVDI_CUDA(cudaMemsetAsync(d_acc, 0, npix * 8, st));
+    SVDI_TRY(launch_dft_probe(e->last_src, e->last_g, e->last_sp, e->vin64.as<double>(), N, e->last_cell, d_px,
+                              d_py, (int)npix, d_acc, e->sm_count, st));
+    std::vector<double> acc(npix);
+    SVDI_CUDA(cudaMemcpyAsync(acc.data(), d_acc, npix * 8, cudaMemcpyDeviceToHost, st));
+    SVDI_CUDA(cudaStreamSynchronize(st));
+    const double* V = e->last.vin;
+    const double inv_det = 1.0 / std::fabs(V[0] * V[4] - V[1] * V[3]);
+    const double cell = e->last_cell;
+    for (size_t p = 0; p < npix; ++p) {
+        const double t1 = cell * (double)(py[p] - N / 2), t2 = cell * (double)(px[p] - N / 2);
+        const double ra = 1.0 - (t1 + V[2]) * (t1 + V[2]) - (t2 + V[5]) * (t2 + V[5]);
+        out[p] = ra < 0.0 ? std::nan("") : std::fabs(acc[p] * inv_det) / (double)e->last_src.n;
+    }
+    return SVDI_OK;
+}
+
+}  // extern "C"

@@ -144,6 +144,12 @@ int launch_scatter(const SampleSource& src, const GridGeom& g, const SlabParams&
 constexpr int kTcTileRows = 56;    // tile rows: footprint origins; 64-row accumulator with halo
 constexpr int kTcTileCols = 8;     // tile columns: footprint origins of one column block
 constexpr int kTcBlocks = 4;       // column blocks per super-tile accumulator (4 x 32 TMEM columns)
+// accuracy.cu: FP64 direct DFT at pixels (px, py) of the samples the gridder keeps; d_acc (npix,
+// zeroed by the caller) receives the signed sums before |.| / |det| / N_s
+int launch_dft_probe(const SampleSource& src, const GridGeom& g, const SlabParams& sp, const double* d_vin,
+                     long long N, double cell, const long long* d_px, const long long* d_py, int npix,
+                     double* d_acc, int sm_count, cudaStream_t st);
+
 constexpr int kTcKBlock = 32;      // records per K-block (one MMA pair of K steps)
 int launch_grid_tc(const SampleRec* d_rec, const unsigned int* d_offsets, const unsigned int* d_kb_offsets,
                    int n_keys, int key_lo, int key_hi, int slab_lo, const GridGeom& g, const EsPoly& poly,

@@ -81,3 +81,13 @@ def test_bundle_reader_selects_time_groups(tmp_path):
     exe = os.path.join(ROOT, "svdimager_b200", "bin", "svd_integrated_imager_gpu")
     r = subprocess.run([exe, p, "64", "1e-3", "2", str(tmp_path / "o.fits")], capture_output=True, text=True)
     assert r.returncode == 1 and "Snapshot_Index is outside" in r.stderr
+
+
+def test_autotune_candidates_and_beta():
+    from svdimager_b200 import api, autotune
+    assert abs(autotune.es_beta(8, 1.5) - autotune.REF_BETA) < 1e-12
+    assert autotune.es_beta(12, 2.0) > autotune.es_beta(8, 2.0) > autotune.es_beta(8, 1.25)
+    c = autotune.candidates()
+    # W in {6, 8, 10, 12} x sigma in 4 values x (two FP32 tiles, plus the tensor core for W <= 8)
+    assert len(c) == 4 * 4 * 2 + 2 * 4
+    assert all(o["gridder"] == api.GRIDDER_FP32 or o["support"] <= 8 for o in c)
