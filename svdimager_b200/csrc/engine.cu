@@ -105,7 +105,7 @@ struct svdi_engine {
     svdi::DevBuf in_bin, in_vin;
     // intermediates
     svdi::DevBuf vr, vi, q, s, vin64, vin32, stats, partial, counts, offsets, cursor, dropped, rec,
-        rec_s, planes, corr, image, cheb_err, bin_out, grid_keep, tc_status, kb_offsets;
+        rec_s, planes, corr, image, cheb_err, bin_out, grid_keep, tc_status, kb_offsets, acc;
     size_t sz_vr = 0, sz_q = 0, sz_s = 0, sz_off = 0, sz_rec = 0, sz_rec_s = 0, sz_grid = 0, sz_mom = 0;
     const float* cur_vr = nullptr;
     const float* cur_vi = nullptr;
@@ -515,6 +515,13 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     SVDI_TRY(get_plan(e, g.G, planes_per_batch, plan));
     SVDI_TRY(ensure_corr(e, N, g.G, g.W, o.beta));
     SVDI_CUDA(cudaMemsetAsync(d_out, 0, (size_t)N * N * sizeof(float), st));
+    // slabs split over several batches: the signed sums of all batches before |.| (the reference
+    // takes |.| per batch, SVDIntegratedImager.cu:1445, inside its batch loop at :1681)
+    const bool multi_batch = (int)bslabs < sp.nslab;
+    if (multi_batch) {
+        SVDI_TRY(e->acc.ensure((size_t)N * N * sizeof(double)));
+        SVDI_CUDA(cudaMemsetAsync(e->acc.p, 0, (size_t)N * N * sizeof(double), st));
+    }
     float ms_grid = 0, ms_fft = 0, ms_img = 0;
     for (int s0 = 0; s0 < sp.nslab; s0 += (int)bslabs) {
         const int s1 = std::min(sp.nslab, s0 + (int)bslabs);
@@ -547,7 +554,7 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
         bp.r3_min = sp.r3_min + (double)s0 * sp.slab_width;
         SVDI_TRY(launch_recombine(e->planes.as<float2>(), g, N, cell, e->vin64.as<double>(), bp,
                                   e->corr.as<float>(), 1.0 / (double)n, o.reprojection, o.presplat, d_out,
-                                  st));
+                                  st, multi_batch ? e->acc.as<double>() : nullptr, s1 == sp.nslab));
         if (!timed) continue;
         SVDI_CUDA(cudaEventRecord(e->ev[6], st));
         SVDI_CUDA(cudaEventSynchronize(e->ev[6]));

@@ -112,7 +112,8 @@ __global__ void __launch_bounds__(256) k_recombine(const float2* __restrict__ mo
                                                   double cell, const double* __restrict__ vin,
                                                   SlabParams sp, const float* __restrict__ corr,
                                                   double inv_n, int reprojection, int presplat,
-                                                  float* __restrict__ out) {
+                                                  float* __restrict__ out, double* __restrict__ acc,
+                                                  int final_batch) {
     const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const long long y = blockIdx.y * (long long)blockDim.y + threadIdx.y;
     if (x >= N || y >= N) return;
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(256) k_recombine(const float2* __restrict__ mo
     const double t1 = cell * (double)yr, t2 = cell * (double)xr;
     const double ra = 1.0 - (t1 + V[2]) * (t1 + V[2]) - (t2 + V[5]) * (t2 + V[5]);
     if (ra < 0.0) {
-        if (presplat) out[y * N + x] = __int_as_float(0x7fc00000);  // NaN
+        if (presplat && final_batch) out[y * N + x] = __int_as_float(0x7fc00000);  // NaN
         return;
     }
     const double t3 = -V[8] + (V[8] >= 0.0 ? 1.0 : -1.0) * sqrt(ra);
@@ -155,9 +156,17 @@ __global__ void __launch_bounds__(256) k_recombine(const float2* __restrict__ mo
     }
     if ((xr + yr) & 1) sum = -sum;
     const long long ax = xr < 0 ? -xr : xr, ay = yr < 0 ? -yr : yr;
-    const double value = fabs(sum * (double)corr[ax] * (double)corr[ay]) * inv_n;
-    if (presplat) {  // slab batches add up (the reference also sums |partial| per batch)
-        out[y * N + x] += (float)value;
+    double signed_sum = sum * (double)corr[ax] * (double)corr[ay];
+    if (acc) {  // slab batches: the signed sums add up, |.| is taken once, in the last batch
+        signed_sum += acc[y * N + x];
+        if (!final_batch) {
+            acc[y * N + x] = signed_sum;
+            return;
+        }
+    }
+    const double value = fabs(signed_sum) * inv_n;
+    if (presplat) {
+        out[y * N + x] = (float)value;
         return;
     }
 
@@ -179,14 +188,14 @@ __global__ void __launch_bounds__(256) k_recombine(const float2* __restrict__ mo
 int launch_recombine(const float2* d_moments, const GridGeom& g, long long N, double cell,
                      const double* d_vin64, const SlabParams& sp, const float* d_corr,
                      double inv_n_total, int reprojection, int presplat, float* d_out,
-                     cudaStream_t st) {
+                     cudaStream_t st, double* d_acc, bool final_batch) {
     const dim3 block(32, 8);
     const dim3 grid((unsigned)((N + 31) / 32), (unsigned)((N + 7) / 8));
-    if (sp.K <= 1) k_recombine<1><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out);
-    else if (sp.K <= 8) k_recombine<8><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out);
-    else if (sp.K <= 16) k_recombine<16><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out);
-    else if (sp.K <= 32) k_recombine<32><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out);
-    else if (sp.K <= kMaxTerms) k_recombine<kMaxTerms><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out);
+    if (sp.K <= 1) k_recombine<1><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out, d_acc, final_batch ? 1 : 0);
+    else if (sp.K <= 8) k_recombine<8><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out, d_acc, final_batch ? 1 : 0);
+    else if (sp.K <= 16) k_recombine<16><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out, d_acc, final_batch ? 1 : 0);
+    else if (sp.K <= 32) k_recombine<32><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out, d_acc, final_batch ? 1 : 0);
+    else if (sp.K <= kMaxTerms) k_recombine<kMaxTerms><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out, d_acc, final_batch ? 1 : 0);
     else {
         set_error("recombine: too many Chebyshev terms");
         return SVDI_ERR_UNSUPPORTED;

@@ -164,9 +164,11 @@ int launch_grid_fp32(const SampleRec* d_rec, const float* d_rec_s, const unsigne
 void build_es_poly(int W, double beta, EsPoly* out);
 
 // image.cu
+// d_acc (N x N doubles, zeroed before the first batch) when the slabs are split over several
+// batches: every batch adds its signed sum, the final batch takes |.| and writes the image.
 int launch_recombine(const float2* d_moments, const GridGeom& g, long long N, double cell,
                      const double* d_vin64, const SlabParams& sp, const float* d_corr,
                      double inv_n_total, int reprojection, int presplat, float* d_out,
-                     cudaStream_t st);
+                     cudaStream_t st, double* d_acc = nullptr, bool final_batch = true);
 
 }  // namespace svdi

@@ -321,6 +321,26 @@ def test_wterm_multi_slab_matches_oracle_and_dft(cuda_device):
     assert O.rel_rms(R[py, px][m], d[m]) < IMG_TOL
 
 
+def test_slab_batches_add_signed_sums(cuda_device):
+    """Slabs imaged in several batches (max_batch_slabs = 1) give the image of one batch: the
+    signed sums of the batches add before |.| is taken."""
+    s = snapshot("widefield", nchan=4, n_rows_limit=6000, image_size=128, cell_size=6e-4)
+    kw = dict(k_rule=api.KRULE_FIXED, fixed_k=12, target_alpha=2.0, edge_mode=api.EDGE_STRICT)
+    with api.Engine(**kw) as e:
+        one = e.image(s)
+        assert e.stats()["num_slabs"] > 1
+    with api.Engine(max_batch_slabs=1, **kw) as e:
+        many = e.image(s)
+    assert O.rel_rms(many, one) < 1e-6
+    with api.Engine(presplat=1, **kw) as e:
+        one_p = e.image(s)
+    with api.Engine(presplat=1, max_batch_slabs=1, **kw) as e:
+        many_p = e.image(s)
+    m = np.isfinite(one_p)
+    assert np.array_equal(m, np.isfinite(many_p))
+    assert O.rel_rms(many_p[m], one_p[m]) < 5e-6  # cuFFT batch shapes differ: FP32 rounding
+
+
 def test_slab_batching_matches_single_batch_when_one_slab(cuda_device, small_snapshot):
     with api.Engine(max_batch_slabs=1) as e:
         a = e.image(small_snapshot)
