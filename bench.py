@@ -384,13 +384,14 @@ def run_ours(args):
         alg = 8 * planes * N * N + 4 * N * N
         name = "k_recombine"
     achieved = alg / (stage_ms[dom] * 1e-3) / 1e9
-    traffic = None
-    tr_path = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tr_path):
-        try:
-            traffic = json.load(open(tr_path)).get(dom)
-        except Exception:
-            traffic = None
+    traffic = None  # DRAM bytes per launch of the dominant kernel from an ncu capture, when recorded
+    tr_path = os.path.join(ROOT, "profiles", "traffic.txt")
+    if dom == "ms_grid" and os.path.exists(tr_path):
+        kern = "k_grid_tc" if st["used_tc"] else "k_grid_fp32"
+        for ln in open(tr_path):
+            f = ln.split()
+            if len(f) == 2 and f[0] == kern:
+                traffic = int(f[1])
 
     cpu = cpu_baseline(snap, eng, api, st, args) if not args.no_cpu else None
     line = {

@@ -44,8 +44,8 @@
 //               flush / exit events.
 //   warps 10-13 epilogue: TMEM lane quarter (warp % 4); merge fresh intervals into the running sum
 //               and flush super-tiles to the moment plane, in event order.
-// Every CTA takes an equal share of the binned records (a contiguous range that can start and end
-// inside a tile).
+// The scheduler warps take chunks of 32 K-blocks from a global counter (a chunk can start and end
+// inside a tile; each CTA flushes the super-tiles it touched).
 //
 // Scaling. The B values are wy * v * 2^(14 - e) with max|v| < 2^e over all records (the scatter
 // kernel's max reduction) and the A values 256 * wx, so every FP16 operand is below 65504 and the
@@ -86,6 +86,7 @@ constexpr int kFreshKB = 8;             // K-blocks (48 MMAs) per fresh interval
 constexpr int kFreshCol0 = kTcBlocks * kN;  // running blocks first, then the fresh buffers
 constexpr int kTmemCols = 256;
 constexpr int kMetaRing = 128;          // published K-block descriptors
+constexpr int kChunkKB = 32;            // K-blocks per chunk of dynamically distributed work
 constexpr int kEventRing = 64;
 
 constexpr int kABytes = kM * kKB * 2;                    // 4 KB per FP16 A operand
@@ -269,6 +270,7 @@ struct TcParams {
     const unsigned int* vmax;
     float2* planes;
     unsigned int* status;
+    unsigned int* work;              // next chunk of K-blocks to hand out (zeroed by the host)
     int key_lo, key_hi, slab_lo;
 };
 
@@ -286,8 +288,6 @@ struct __align__(8) TcShared {
     unsigned int ev_consumed[4];
     int abort;
     uint32_t tmem_base;
-    int start_key;         // key of the CTA's first K-block
-    unsigned int start_m;  // its K-block index within that key
 };
 
 __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g, EsPoly poly) {
@@ -308,11 +308,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    // equal shares of the K-blocks of keys [key_lo, key_hi) (sparse tiles cost a K-block per key)
+    // the K-blocks of keys [key_lo, key_hi), handed out in chunks by the scheduler warps
     const unsigned int kb_lo = P.kb_offsets[P.key_lo], kb_hi = P.kb_offsets[P.key_hi];
-    const unsigned long long kb_total = kb_hi - kb_lo;
-    const unsigned int kbb = kb_lo + (unsigned int)(kb_total * blockIdx.x / gridDim.x);
-    const unsigned int kbe = kb_lo + (unsigned int)(kb_total * (blockIdx.x + 1) / gridDim.x);
     if (tid == 0) {
         for (int s = 0; s < kPairs; ++s) {
             mbar_init(smem_u32(&S.full[s]), kGroups * kGroupThreads);
@@ -329,13 +326,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
         S.ev_published = 0;
         for (int q = 0; q < 4; ++q) S.ev_consumed[q] = 0;
         S.abort = 0;
-        int lo = P.key_lo, hi = P.key_hi;  // last key with kb_offsets[key] <= kbb
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (P.kb_offsets[mid] <= kbb) lo = mid; else hi = mid;
-        }
-        S.start_key = lo;
-        S.start_m = kbb - P.kb_offsets[lo];
     }
     for (int i = tid; i < kStages * kStageBytes / 16; i += kThreads)
         reinterpret_cast<uint4*>(smem)[i] = make_uint4(0, 0, 0, 0);
@@ -553,12 +543,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
         }
     } else if (warp == kSchedWarp) {
         // ============================ scheduler ============================
-        // Schedule: K-blocks [kbb, kbe) in key order; K-block m of key k covers records
-        // [offsets[k] + 32 m, min(offsets[k + 1], offsets[k] + 32 (m + 1))). Lanes hold offsets and
-        // kb_offsets of the current 32-key chunk (x = 32 from the *_e registers); the next chunk's
-        // are loaded one chunk ahead.
-        int kc = S.start_key, ci = 0;
-        unsigned int m_in_key = S.start_m, remaining = kbe - kbb;
+        // The K-blocks of keys [key_lo, key_hi) are handed out in chunks of kChunkKB from a global
+        // counter (dynamic balance: CTAs whose tiles cost more take fewer chunks). K-block m of key k
+        // covers records [offsets[k] + 32 m, min(offsets[k + 1], offsets[k] + 32 (m + 1))). Lanes hold
+        // offsets and kb_offsets of the current 32-key window (x = 32 from the *_e registers); the
+        // next window is loaded one window ahead.
+        int kc = 0, ci = 0;
+        unsigned int m_in_key = 0, remaining = 0;
         unsigned int off_l = 0, kbo_l = 0, off_e = 0, kbo_e = 0;
         unsigned int noff_l = 0, nkbo_l = 0, noff_e = 0, nkbo_e = 0;
         auto fetch = [&](int base, unsigned int& o, unsigned int& kb, unsigned int& oe, unsigned int& kbe_) {
@@ -573,12 +564,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
             const unsigned int v = __shfl_sync(0xffffffffu, vl, x & 31);
             return x == 32 ? ve : v;
         };
-        if (remaining) {
-            fetch(kc, off_l, kbo_l, off_e, kbo_e);
-            fetch(kc + 32, noff_l, nkbo_l, noff_e, nkbo_e);
-        }
         unsigned int published = 0;
-        // current key: records [ka, kb_end_rec), K-blocks m_in_key .. nkb - 1
+        // current key: records [ka, kend), K-blocks m_in_key .. nkb - 1
         unsigned int ka = 0, kend = 0, nkb = 0;
         bool have_key = false;
         auto schedule_to = [&](unsigned int target) {  // publish K-blocks up to index target - 1
@@ -624,18 +611,48 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
                 __syncwarp();
                 if (lane == 0) st_release(&S.published, published);
             }
-            if (!remaining && lane == 0 && ld_acquire(&S.sched_done) == 0) st_release(&S.sched_done, published + 1);
         };
-        for (;;) {  // keep the ring full: up to kMetaRing descriptors ahead of the MMA warp
-            int cons = 0;
-            if (lane == 0) cons = (int)ld_acquire(&S.consumed);
-            cons = __shfl_sync(0xffffffffu, cons, 0);
-            schedule_to((unsigned int)cons + kMetaRing);
-            if (!remaining) break;
-            bool ok = true;
-            if (lane == 0) ok = wait_at_least(&S.consumed, (unsigned int)cons + 1, abort_flag);
-            if (!__shfl_sync(0xffffffffu, (int)ok, 0)) break;  // the waiting role reports the failure
+        bool ok = true;
+        for (;;) {
+            // next chunk of K-blocks
+            unsigned int c = 0;
+            if (lane == 0) c = atomicAdd(P.work, 1u);
+            c = __shfl_sync(0xffffffffu, c, 0);
+            const unsigned long long kb0l = (unsigned long long)kb_lo + (unsigned long long)c * kChunkKB;
+            if (kb0l >= kb_hi) break;
+            const unsigned int kb0 = (unsigned int)kb0l, kb1 = min(kb_hi, kb0 + (unsigned int)kChunkKB);
+            // its first key: the last key with kb_offsets[key] <= kb0 (32 probes per round)
+            int lo = P.key_lo, hi = P.key_hi;
+            while (hi - lo > 1) {
+                const int step = (hi - lo + 31) / 32;
+                const int probe = lo + lane * step;
+                const bool le = probe < hi && P.kb_offsets[probe] <= kb0;
+                const unsigned int bal = __ballot_sync(0xffffffffu, le);
+                const int lmax = 31 - __clz(bal);  // lane 0 always qualifies (kb_offsets[lo] <= kb0)
+                const int nlo = lo + lmax * step;
+                hi = min(hi, nlo + step);
+                lo = nlo;
+            }
+            kc = lo;
+            ci = 0;
+            m_in_key = kb0 - P.kb_offsets[lo];
+            remaining = kb1 - kb0;
+            have_key = false;
+            fetch(kc, off_l, kbo_l, off_e, kbo_e);
+            fetch(kc + 32, noff_l, nkbo_l, noff_e, nkbo_e);
+            while (remaining) {  // keep the ring full: up to kMetaRing descriptors ahead of the MMA warp
+                int cons = 0;
+                if (lane == 0) cons = (int)ld_acquire(&S.consumed);
+                cons = __shfl_sync(0xffffffffu, cons, 0);
+                schedule_to((unsigned int)cons + kMetaRing);
+                if (!remaining) break;
+                if (lane == 0) ok = wait_at_least(&S.consumed, (unsigned int)cons + 1, abort_flag);
+                ok = __shfl_sync(0xffffffffu, (int)ok, 0);
+                if (!ok) break;  // the waiting role reports the failure
+            }
+            if (!ok) break;
         }
+        if (ok && lane == 0) st_release(&S.sched_done, published + 1);
     } else if (warp == kMmaWarp) {
         // ============================ MMA issuer ============================
         // MMA / interval / event state (lane 0)
@@ -909,7 +926,9 @@ int launch_grid_tc(const SampleRec* d_rec, const unsigned int* d_offsets, const 
         set_error("tensor-core gridder: kernel does not fit on an SM");
         return SVDI_ERR_UNSUPPORTED;
     }
-    TcParams P{d_rec, d_offsets, d_kb_offsets, d_vmax, d_planes, d_status, key_lo, key_hi, slab_lo};
+    // d_status: [0] give-up flags, [1] max |value| (read through d_vmax), [2] the work counter
+    SVDI_CUDA(cudaMemsetAsync(d_status + 2, 0, sizeof(unsigned int), st));
+    TcParams P{d_rec, d_offsets, d_kb_offsets, d_vmax, d_planes, d_status, d_status + 2, key_lo, key_hi, slab_lo};
     // two CTAs per SM (two MMA-issuing threads: one thread issues a skinny MMA every ~46 clk, the
     // tensor pipe takes one every ~26), each with 256 of the SM's 512 TMEM columns
     k_grid_tc<<<2 * sm_count, kThreads, kSmemBytes, st>>>(P, g, poly);
