@@ -9,21 +9,28 @@ frequencies, polarisations 0/3, flags, WEIGHT_SPECTRUM): FP64 SVD rotation, flag
 tile binning, gridding, cuFFT, Chebyshev recombination, grid correction, reprojection.
 
 `value` is snapshots/s with the inputs resident in HBM (device API); `e2e` is the same through the
-host API with pinned host buffers, host->device upload and device->host image read inside every
-step. The inputs (219 MB) exceed the 126 MB L2, so no flush is needed between steps.
+streaming host API (server: two resident engines, three snapshots in flight) with pinned host
+buffers, host->device upload and device->host image read inside every step; `e2e.sync` is one
+blocking host call per snapshot. The inputs (219 MB) exceed the 126 MB L2, so no flush is needed
+between steps.
 
 Multi-GPU: replicas only -- every rank images its own snapshot stream on its own GPU; no data-path
 collective. value = snapshots of all ranks / max over ranks of the timed region.
 
 --impl reference: the reference algorithm's CPU restatement (oracle: ES gridding with the
 reference's bucket Chebyshev rule, FFT, recombination, reprojection) on the host cores, rank 0.
+Its line also carries `reference_binary`: the reference's own GPU imager (archive FIpipe, compiled
+from its source for sm_100a) timed per call on the same snapshot; our arm's `fipipe` key times our
+FIpipe on the same inputs.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import math
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -273,6 +280,72 @@ def widefield_phase(api, local, npix=256):
                            "needs hundreds of slabs"}
 
 
+def archive_quartet(snap, eng, api):
+    """The archive entry's inputs for `snap` (`FIpipe`, pipe_interface.cpp:8): collapsed
+    visibilities, rotated baselines Bin [N_s][3] (float) and Vin (float), taken from the engine's
+    own preprocessing of the snapshot, in pageable host memory as the archive CLI passes them."""
+    with api.Engine(device=eng.options.device) as e:
+        e.image(snap)
+        vr, vi = e.buffer(api.BUF_VIS_REAL), e.buffer(api.BUF_VIS_IMAG)
+        q, s = e.buffer(api.BUF_Q).reshape(-1, 3), e.buffer(api.BUF_S)
+        vin = np.array(e.stats()["vin"], np.float64).reshape(3, 3)
+    b = (s[:, None, None] * q[None, :, :]).reshape(-1, 3).astype(np.float32)   # idx = row + chan * rows
+    return vr.copy(), vi.copy(), np.ascontiguousarray(b), vin.astype(np.float32)
+
+
+def fipipe_phase(api, eng, snap, steps):
+    """Our `FIpipe` (archive semantics: one slab, smallest Chebyshev order within 1e-2) on the
+    snapshot's quartet, host buffers in and out, wall clock per call: the same call and inputs as
+    the reference binary's timing in the reference arm."""
+    vr, vi, b, v = archive_quartet(snap, eng, api)
+    N, cell = snap.image_size, snap.cell_size
+    with api.Engine(api.archive_options(device=eng.options.device)) as e:
+        for _ in range(2):
+            e.fipipe(vr, vi, b, v, N, cell)
+        ts = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            e.fipipe(vr, vi, b, v, N, cell)
+            ts.append(time.perf_counter() - t0)
+        st = e.stats()
+    return {"snapshots_per_s": round(1.0 / float(np.median(ts)), 3),
+            "ms_p50": round(float(np.median(ts)) * 1e3, 3), "ms_p99": round(float(np.percentile(ts, 99)) * 1e3, 3),
+            "chebyshev_terms": st["num_terms"], "calls": steps,
+            "h2d_bytes_per_call": int(vr.nbytes + vi.nbytes + b.nbytes + v.nbytes), "d2h_bytes_per_call": N * N * 4,
+            "what": "FIpipe(Visreal, Visimag, Bin, Vin, dirty, N_s, N, cell) from pageable host buffers, wall clock"}
+
+
+def e2e_stream(api, opts, psnap, N, cell, steps, warmup, dist, dev, slots=2, window=3):
+    """End to end through the streaming API: `steps` snapshots submitted to a server with `slots`
+    resident engines, at most `window` in flight (a correlator client that hands over the next
+    snapshot when a receive buffer frees up). Every request uploads its inputs from pinned host
+    memory and reads its image back into a pinned host image; the upload of one request overlaps
+    the imaging of another. Timed from the first submit to the last completion."""
+    import torch
+    outs = [torch.zeros((N, N), dtype=torch.float32).pin_memory().numpy() for _ in range(window)]
+    lat = []
+    with api.Server(num_slots=slots, **opts) as srv:
+        for i in range(max(warmup, slots)):
+            srv.wait(srv.submit(psnap, N, cell, out=outs[i % window]), 120)
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        inflight = []
+        for i in range(steps):
+            if len(inflight) == window:
+                _, info = srv.wait(inflight.pop(0), 120)
+                lat.append(info["latency_ms"])
+            inflight.append(srv.submit(psnap, N, cell, out=outs[i % window]))
+        for t in inflight:
+            _, info = srv.wait(t, 120)
+            lat.append(info["latency_ms"])
+        sec = time.perf_counter() - t0
+    from svdimager_b200 import replicas
+    return {"seconds": replicas.max_over_ranks(sec, dist, dev), "slots": slots, "window": window,
+            "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3),
+                           "p99": round(float(np.percentile(lat, 99)), 3)}}
+
+
 def make_workload(config, rank):
     from svdimager_b200 import synth
     return synth.make_snapshot(config, snapshot_index=rank)
@@ -313,19 +386,24 @@ def run_ours(args):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     stage = {"ms_preprocess": [], "ms_bin": [], "ms_grid": [], "ms_fft": [], "ms_image": []}
+    # throughput: snapshots submitted back to back (the host enqueues the next snapshot while the
+    # device finishes the previous one)
     with ClockSampler(local) as clk:
         ev0.record(stream)
         for _ in range(args.steps):
-            t0 = time.perf_counter()
             step()
-            torch.cuda.synchronize(dev)
-            lat.append((time.perf_counter() - t0) * 1e3)
-            s2 = eng.stats()
-            for k in stage:
-                stage[k].append(s2[k])
         ev1.record(stream)
         torch.cuda.synchronize(dev)
     launches = api.kernel_launch_count() - n_launch0
+    # latency and per-stage device times: one snapshot at a time
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        step()
+        torch.cuda.synchronize(dev)
+        lat.append((time.perf_counter() - t0) * 1e3)
+        s2 = eng.stats()
+        for k in stage:
+            stage[k].append(s2[k])
     from svdimager_b200 import replicas
     ms_total = replicas.max_over_ranks(ev0.elapsed_time(ev1), dist, dev)
     ms_step = ms_total / args.steps
@@ -349,13 +427,17 @@ def run_ours(args):
         eng.image(psnap, out=himg)
         e2e_lat.append((time.perf_counter() - t1) * 1e3)
     e2e_s = replicas.max_over_ranks(time.perf_counter() - t0, dist, dev)
-    e2e_value = replicas.aggregate_rate(args.steps, ws, e2e_s)
+    e2e_sync_value = replicas.aggregate_rate(args.steps, ws, e2e_s)
+    # streaming through the server: the next snapshot uploads while the previous one images
+    stream_out = e2e_stream(api, opts, psnap, N, cell, args.steps, args.warmup, dist, dev)
+    e2e_value = replicas.aggregate_rate(args.steps, ws, stream_out["seconds"])
     serving = None if args.no_serving else serving_phase(api, snap, args.serving_requests, 50.0, local,
                                                          gridder=gridder)
     batching = None if args.no_batching else batching_phase(api, local, args.batch_snapshots,
                                                              seed_offset=rank)
     widefield = None if args.no_widefield else widefield_phase(api, local)
-    h2d = int(sum(v.nbytes for v in host.values()))
+    fipipe = None if args.no_fipipe else fipipe_phase(api, eng, snap, max(3, min(args.steps, 10)))
+    h2d =int(sum(v.nbytes for v in host.values()))
     d2h = int(N * N * 4)
 
     if rank != 0:
@@ -422,8 +504,12 @@ def run_ours(args):
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "e2e": {"value": round(e2e_value, 3), "unit": "snapshots/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
-                "latency_ms": {"p50": round(float(np.percentile(e2e_lat, 50)), 3),
-                               "p99": round(float(np.percentile(e2e_lat, 99)), 3)}},
+                "api": f"svdi_server submit/wait, {stream_out['slots']} slots, {stream_out['window']} requests "
+                       "in flight, pinned host inputs and output images",
+                "latency_ms": stream_out["latency_ms"],
+                "sync": {"value": round(e2e_sync_value, 3), "api": "svdi_engine_image_host, one blocking call per step",
+                         "latency_ms": {"p50": round(float(np.percentile(e2e_lat, 50)), 3),
+                                        "p99": round(float(np.percentile(e2e_lat, 99)), 3)}}},
         "roofline": {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
                      "peak_kind": peak_kind,
@@ -441,6 +527,8 @@ def run_ours(args):
         line["batching"] = batching
     if widefield:
         line["widefield"] = widefield
+    if fipipe:
+        line["fipipe"] = fipipe
     if cpu:
         line["cpu_baseline"] = cpu["baseline"]
         line["accuracy"] = cpu["accuracy"]
@@ -485,6 +573,56 @@ def cpu_baseline(snap, eng, api, st, args):
         "accuracy": {"rel_rms_vs_fp64_dft": err, "peak_rel_vs_fp64_dft": peak_err, "pixels": int(valid.sum()),
                      "image": "rotated-frame image before reprojection (strict edges)"},
     }
+
+
+def reference_binary_phase(O, snap, calls):
+    """The reference's own GPU imager, its archive `FIpipe` (archive/FIPkernels.cu:679-911,
+    compiled unmodified for sm_100a into oracle/_ref), on the snapshot's full quartet from
+    pageable host buffers: wall clock per call (its allocations, uploads, host Chebyshev selection,
+    cuFFT plan, kernels, download, frees) and its own "Time elapsed" line (FIPkernels.cu:888,
+    plan + kernels). Its stdout is captured so that the JSON line stays the only output."""
+    fn = O.load_reference_fipipe()
+    if fn is None:
+        return {"unavailable": "reference library not built (make -C oracle ref)"}
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no CUDA device"}
+    except ImportError:
+        return {"unavailable": "torch missing"}
+    vr, vi = O.collapse(snap)
+    vin, q, sv, _ = O.preprocess64(snap)
+    b = np.ascontiguousarray(O.expand_coords(q, sv).astype(np.float32))
+    v = np.ascontiguousarray(vin.astype(np.float32).reshape(-1))
+    N, cell = snap.image_size, snap.cell_size
+    out = np.zeros(N * N, np.float32)
+    ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    walls = []
+    with tempfile.TemporaryFile(mode="w+b") as cap:
+        sys.stdout.flush()
+        saved = os.dup(1)
+        os.dup2(cap.fileno(), 1)
+        try:
+            for i in range(calls + 1):   # the first call warms the CUDA context and cuFFT
+                t0 = time.perf_counter()
+                fn(ptr(vr), ptr(vi), ptr(b), ptr(v), ptr(out), vr.shape[0], N, float(cell))
+                if i:
+                    walls.append(time.perf_counter() - t0)
+        finally:
+            os.dup2(saved, 1)
+            os.close(saved)
+        cap.seek(0)
+        text = cap.read().decode(errors="replace")
+    elapsed = [float(m) for m in re.findall(r"Time elapsed: ([0-9.eE+-]+) ms", text)][1:]
+    terms = re.findall(r"selected kept terms\s*=\s*(\d+)", text)
+    return {"snapshots_per_s": round(1.0 / float(np.median(walls)), 3),
+            "ms_p50": round(float(np.median(walls)) * 1e3, 3),
+            "ms_self_timed_p50": round(float(np.median(elapsed)), 3) if elapsed else None,
+            "chebyshev_terms": int(terms[-1]) if terms else None, "calls": calls,
+            "image_nonzero": bool(np.any(out != 0)),
+            "what": "reference archive FIpipe (archive/FIPkernels.cu, nvcc -O3 --use_fast_math -maxrregcount=64, "
+                    "sm_100a) from pageable host buffers, wall clock; ms_self_timed = its own "
+                    "'Time elapsed' (cuFFT plan + kernels)"}
 
 
 def run_reference(args):
@@ -543,6 +681,8 @@ def run_reference(args):
                                    f"fraction; FFT of one {G}^2 plane scaled by the {P} planes; recombination and reprojection full"},
         "e2e": {"value": value, "unit": "snapshots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_ref_binary:
+        line["reference_binary"] = reference_binary_phase(O, snap, max(1, min(args.steps, 3)))
     print(json.dumps(line), flush=True)
 
 
@@ -561,6 +701,9 @@ def main():
     ap.add_argument("--no-batching", action="store_true")
     ap.add_argument("--no-widefield", action="store_true")
     ap.add_argument("--batch-snapshots", type=int, default=256)
+    ap.add_argument("--no-fipipe", action="store_true", help="skip the archive-entry (FIpipe) timing")
+    ap.add_argument("--no-ref-binary", action="store_true",
+                    help="reference arm: skip timing the reference's own GPU imager")
     ap.add_argument("--gridder", default="fp32", choices=["tc", "fp32"],
                     help="tc: split-precision tcgen05 gridder; fp32: CUDA-core fixed-point gridder")
     args = ap.parse_args()

@@ -158,7 +158,11 @@ void svdi_engine_destroy(svdi_engine* e);
 int svdi_engine_image_host(svdi_engine* e, const svdi_host_ms* host, size_t image_size,
                            float cell_size, float* dirty_image);
 
-/* Device-resident snapshot: the same fields as svdi_host_ms but DEVICE pointers (no upload). */
+/* Device-resident snapshot: the same fields as svdi_host_ms but DEVICE pointers (no upload).
+ * The work is ordered on cuda_stream (0: the legacy default stream): it starts after the caller's
+ * earlier work on that stream, and later work there sees the image. The call waits once, for the
+ * w statistics that size the plan, and returns while the gridding, FFT and recombination still
+ * run; svdi_engine_last_stats and the buffer accessors wait for them. */
 int svdi_engine_image_device(svdi_engine* e, const svdi_host_ms* dev_ms, size_t image_size,
                              float cell_size, float* d_dirty_image, void* cuda_stream);
 

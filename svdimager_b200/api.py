@@ -424,11 +424,17 @@ class Server:
         self._h = h
         self._pending = {}
 
-    def submit(self, snap, image_size: Optional[int] = None, cell_size: Optional[float] = None) -> int:
+    def submit(self, snap, image_size: Optional[int] = None, cell_size: Optional[float] = None,
+               out: Optional[np.ndarray] = None) -> int:
+        """Queue one snapshot; `out` (float32 [N][N], e.g. in pinned memory) receives the image,
+        a new array when omitted."""
         N = int(snap.image_size if image_size is None else image_size)
         cell = float(snap.cell_size if cell_size is None else cell_size)
         h, keep = host_ms(snap)
-        out = np.zeros((N, N), np.float32)
+        if out is None:
+            out = np.zeros((N, N), np.float32)
+        elif out.dtype != np.float32 or out.shape != (N, N) or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float32 array of N x N")
         t = ctypes.c_uint64()
         _check(lib().svdi_server_submit(self._h, ctypes.byref(h), N, cell, _ptr(out), ctypes.byref(t)))
         self._pending[t.value] = (h, keep, out)

@@ -177,6 +177,158 @@ __global__ void __launch_bounds__(kThreads) k_scatter(SampleSource src, GridGeom
     }
 }
 
+// Separable sources (r = s[chan] q[row], idx = row + chan R). A warp takes units of kUnitRows
+// rows x one chunk of `lpr` channels (lpr a power of two <= 32): lane -> (row kUnitRows-subset
+// lane / lpr, channel lane % lpr), so consecutive lanes hold consecutive channels of one row. The
+// channels of a baseline mostly share a tile, so match groups are large: one shared-memory or
+// global atomic per group, and a group's records land in consecutive slots. No 64-bit division.
+constexpr int kUnitRows = 16;
+static_assert(32 / 2 <= kUnitRows, "every lane must take part in each row step");
+
+struct SepMap {
+    int lpr;       // lanes per row (channels per chunk)
+    int nch;       // channel chunks
+    int nrt;       // row tiles of kUnitRows
+    int C;
+};
+
+__device__ inline void unit_of(long long u, const SepMap& m, int& rt, int& ch) {
+    rt = (int)(u / m.nch);
+    ch = (int)(u - (long long)rt * m.nch);
+}
+
+__global__ void __launch_bounds__(kThreads) k_histogram_sep(SampleSource src, SepMap m, GridGeom g, SlabParams sp,
+                                                           unsigned int* __restrict__ counts, int n_keys,
+                                                           unsigned long long* __restrict__ dropped) {
+    extern __shared__ unsigned int sh[];
+    const bool use_smem = n_keys <= kSmemKeyLimit;
+    if (use_smem) {
+        for (int k = threadIdx.x; k < n_keys; k += kThreads) sh[k] = 0;
+        __syncthreads();
+    }
+    const int lane = threadIdx.x & 31;
+    const int rps = 32 / m.lpr, sub = lane / m.lpr, coff = lane % m.lpr;
+    const long long nunits = (long long)m.nrt * m.nch;
+    const long long nwarps = (long long)gridDim.x * (kThreads / 32);
+    unsigned int ndrop = 0;
+    for (long long u = (long long)blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5); u < nunits; u += nwarps) {
+        int rt, ch;
+        unit_of(u, m, rt, ch);
+        const int c = ch * m.lpr + coff;
+        const bool cvalid = c < m.C;
+        const double sc = cvalid ? src.s[c] : 0.0;
+        for (int i = sub; i < kUnitRows; i += rps) {
+            const long long row = (long long)rt * kUnitRows + i;
+            int key = -2;
+            if (cvalid && row < src.R) {
+                const double* q = src.q + row * 3;
+                key = row_chan_key(sc, q[0], q[1], q[2], g, sp).key;
+                if (key < 0) ++ndrop;
+            }
+            const unsigned int peers = __match_any_sync(0xffffffffu, key);
+            if (key >= 0 && lane == __ffs(peers) - 1) {
+                if (use_smem) atomicAdd(&sh[key], __popc(peers));
+                else atomicAdd(&counts[key], __popc(peers));
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) ndrop += __shfl_xor_sync(0xffffffffu, ndrop, o);
+    if (lane == 0 && ndrop) atomicAdd(dropped, (unsigned long long)ndrop);
+    if (use_smem) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < n_keys; k += kThreads)
+            if (sh[k]) atomicAdd(&counts[k], sh[k]);
+    }
+}
+
+// Scatter for separable sources: per unit, the warp stages the unit's collapsed visibilities in
+// shared memory with row-contiguous loads, then writes each group's records to the slots one
+// global atomic on the key's cursor reserved.
+constexpr int kVisPitch = kUnitRows + 1;   // float2 pitch of a staged channel (bank-conflict free)
+
+__global__ void __launch_bounds__(kThreads) k_scatter_sep(SampleSource src, SepMap m, GridGeom g, SlabParams sp,
+                                                         unsigned int* __restrict__ cursor,
+                                                         SampleRec* __restrict__ rec, float* __restrict__ rec_s,
+                                                         unsigned int* __restrict__ vmax) {
+    __shared__ float2 stage[kThreads / 32][32 * kVisPitch];
+    float2* my = stage[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int rps = 32 / m.lpr, sub = lane / m.lpr, coff = lane % m.lpr;
+    const long long nunits = (long long)m.nrt * m.nch;
+    const long long nwarps = (long long)gridDim.x * (kThreads / 32);
+    const long long R = src.R;
+    float vm = 0.0f;
+    for (long long u = (long long)blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5); u < nunits; u += nwarps) {
+        int rt, ch;
+        unit_of(u, m, rt, ch);
+        const long long row0 = (long long)rt * kUnitRows;
+        const int c0 = ch * m.lpr;
+        // stage: lanes 0-15 and 16-31 read kUnitRows consecutive rows of two channels
+        __syncwarp();
+        for (int k = 0; k < m.lpr; k += 2) {
+            const int cc = k + (lane >> 4);
+            const long long row = row0 + (lane & 15);
+            float2 v = make_float2(0.0f, 0.0f);
+            if (c0 + cc < m.C && row < R) {
+                const long long idx = row + (long long)(c0 + cc) * R;
+                v = make_float2(src.vr[idx], src.vi[idx]);
+            }
+            my[cc * kVisPitch + (lane & 15)] = v;
+        }
+        __syncwarp();
+        const int c = c0 + coff;
+        const bool cvalid = c < m.C;
+        const double sc = cvalid ? src.s[c] : 0.0;
+        for (int i = sub; i < kUnitRows; i += rps) {
+            const long long row = row0 + i;
+            KeyRec kr;
+            kr.key = -2;
+            if (cvalid && row < R) {
+                const double* q = src.q + row * 3;
+                kr = row_chan_key(sc, q[0], q[1], q[2], g, sp);
+            }
+            const int key = kr.key;
+            const unsigned int peers = __match_any_sync(0xffffffffu, key);
+            const int leader = __ffs(peers) - 1;
+            unsigned int b0 = 0;
+            if (key >= 0 && lane == leader) b0 = atomicAdd(&cursor[key], __popc(peers));
+            b0 = __shfl_sync(0xffffffffu, b0, leader);
+            if (key >= 0) {
+                const unsigned int pos = b0 + __popc(peers & ((1u << lane) - 1u));
+                const float2 v = my[coff * kVisPitch + i];
+                SampleRec r;
+                r.xq = kr.xq;
+                r.yq = kr.yq;
+                r.vre = __fmul_rn(v.x, src.inv_det);
+                r.vim = __fmul_rn(v.y, src.inv_det);
+                rec[pos] = r;
+                if (rec_s) rec_s[pos] = kr.s;
+                vm = fmaxf(vm, fmaxf(fabsf(r.vre), fabsf(r.vim)));
+            }
+        }
+    }
+    if (vmax) {  // non-negative floats order like their bit patterns
+        const unsigned int mb = __reduce_max_sync(0xffffffffu, __float_as_uint(vm));
+        if (lane == 0 && mb) atomicMax(vmax, mb);
+    }
+}
+
+SepMap sep_map(const SampleSource& src) {
+    SepMap m{};
+    m.C = (int)(src.n / src.R);
+    m.lpr = 2;   // >= 2: then 32 / lpr <= kUnitRows and every lane runs the same row loop
+    while (m.lpr < 32 && m.lpr < m.C) m.lpr <<= 1;
+    m.nch = (m.C + m.lpr - 1) / m.lpr;
+    m.nrt = (int)((src.R + kUnitRows - 1) / kUnitRows);
+    return m;
+}
+
+// Separable kernels need whole rows x channels and 32-bit unit and row counts.
+bool use_sep(const SampleSource& src) {
+    return !src.bin && src.R > 0 && src.n % src.R == 0 && src.n / src.R <= (1LL << 20) &&
+           (src.R + kUnitRows - 1) / kUnitRows * ((src.n / src.R + 31) / 32) < (1LL << 31);
+}
+
 }  // namespace
 
 int launch_histogram(const SampleSource& src, const GridGeom& g, const SlabParams& sp,
@@ -187,6 +339,21 @@ int launch_histogram(const SampleSource& src, const GridGeom& g, const SlabParam
     if (smem > configured) {
         SVDI_CUDA(cudaFuncSetAttribute(k_histogram, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         configured = smem;
+    }
+    if (use_sep(src)) {
+        static size_t configured_sep = 48 * 1024;
+        if (smem > configured_sep) {
+            SVDI_CUDA(cudaFuncSetAttribute(k_histogram_sep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            configured_sep = smem;
+        }
+        const SepMap m = sep_map(src);
+        const long long units = (long long)m.nrt * m.nch;
+        long long blocks = (units + kThreads / 32 - 1) / (kThreads / 32);
+        if (blocks > 148 * 4) blocks = 148 * 4;   // a few units per warp: the shared histogram is flushed once
+        if (blocks < 1) blocks = 1;
+        k_histogram_sep<<<(int)blocks, kThreads, smem, st>>>(src, m, g, sp, d_counts, n_keys, d_dropped);
+        SVDI_LAUNCHED();
+        return SVDI_OK;
     }
     long long blocks = (src.n + kThreads - 1) / kThreads;
     if (blocks > 148 * 8) blocks = 148 * 8;
@@ -206,6 +373,16 @@ int launch_scan(const unsigned int* d_counts, int n_keys, unsigned int* d_offset
 int launch_scatter(const SampleSource& src, const GridGeom& g, const SlabParams& sp,
                    unsigned int* d_cursor, int n_keys, SampleRec* d_rec, float* d_rec_s,
                    unsigned int* d_vmax, cudaStream_t st) {
+    if (use_sep(src)) {
+        const SepMap m = sep_map(src);
+        const long long units = (long long)m.nrt * m.nch;
+        long long blocks = (units + kThreads / 32 - 1) / (kThreads / 32);
+        if (blocks > 148 * 8) blocks = 148 * 8;
+        if (blocks < 1) blocks = 1;
+        k_scatter_sep<<<(int)blocks, kThreads, 0, st>>>(src, m, g, sp, d_cursor, d_rec, d_rec_s, d_vmax);
+        SVDI_LAUNCHED();
+        return SVDI_OK;
+    }
     const size_t smem = n_keys <= kSmemKeyLimit / 2 ? (size_t)n_keys * 8 : 0;
     static size_t configured = 48 * 1024;  // the attribute is raised once, to the largest size used
     if (smem > configured) {

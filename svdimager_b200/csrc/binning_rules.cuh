@@ -14,24 +14,39 @@ struct KeyRec {
     float s;
 };
 
+// floor(x / T) for 0 <= x < 2^24 and 1 <= T < 2^24, exact: a float estimate (off by at most one
+// for these ranges) and one integer correction.
+__device__ inline int tile_div(int x, int T) {
+    int t = __float2int_rz(__fmul_rn(__int2float_rn(x), __frcp_rn(__int2float_rn(T))));
+    if (t * T > x) --t;
+    else if ((t + 1) * T <= x) ++t;
+    return t;
+}
+
+// Q = floor(p 2^24) split exactly in FP64 into cell = floor(p) = Q >> 24 and frac = Q & (2^24 - 1):
+// p 2^24 and cell 2^24 are exact (power-of-two scaling), Q - cell 2^24 is an exact difference of
+// integers below 2^53. |p| >= 1e9 lies beyond every grid (G < 2^24) and is dropped under both edge
+// rules, like the contract's 1e15 bound; within it every integer fits 32 bits (tiles T <= 64).
 __device__ inline bool quantise_axis(double p, const GridGeom& g, int T, int& tile, int& qrel) {
-    if (!(fabs(p) < 1e15)) return false;
-    const long long Q = (long long)floor(p * 16777216.0);
-    const long long cell = Q >> 24;
-    const long long frac = Q & 0xFFFFFFLL;
-    const long long hw = g.W / 2;
-    long long lo = frac ? cell - (hw - 1) : cell - hw;
-    long long hi = cell + hw;
+    if (!(fabs(p) < 1e9)) return false;
+    const double Qd = floor(p * 16777216.0);
+    const double celld = floor(Qd * (1.0 / 16777216.0));
+    const int cell = (int)celld;
+    const int frac = (int)fma(celld, -16777216.0, Qd);
+    const int hw = g.W / 2;
+    const int gmin = (int)g.gmin, gmax = (int)g.gmax;
+    int lo = frac ? cell - (hw - 1) : cell - hw;
+    int hi = cell + hw;
     if (g.edge_mode == SVDI_EDGE_STRICT) {
-        if (lo < g.gmin || hi > g.gmax) return false;
+        if (lo < gmin || hi > gmax) return false;
     } else {
-        if (lo < g.gmin) lo = g.gmin;
-        if (hi > g.gmax) hi = g.gmax;
+        if (lo < gmin) lo = gmin;
+        if (hi > gmax) hi = gmax;
         if (lo > hi) return false;
     }
-    tile = (int)((lo - g.gmin) / T);
-    const long long origin = g.gmin + (long long)tile * T;
-    qrel = (int)(Q - origin * 16777216LL);
+    tile = tile_div(lo - gmin, T);  // 0 <= lo - gmin < G < 2^24
+    const int origin = gmin + tile * T;
+    qrel = (int)((unsigned)(cell - origin) * 16777216u + (unsigned)frac);  // Q - origin 2^24
     return true;
 }
 
@@ -55,12 +70,10 @@ __device__ inline void sample_coords(const SampleSource& src, long long idx, dou
     }
 }
 
-__device__ inline KeyRec sample_key(const SampleSource& src, long long idx, const GridGeom& g,
-                                    const SlabParams& sp) {
+// Key of a sample at rotated coordinate (r1, r2, r3).
+__device__ inline KeyRec coord_key(double r1, double r2, double r3, const GridGeom& g, const SlabParams& sp) {
     KeyRec k;
     k.key = -1;
-    double r1, r2, r3;
-    sample_coords(src, idx, r1, r2, r3);
     int t1, t2;
     if (!quantise_axis(grid_pos(r1, g), g, g.T, t1, k.xq) || !quantise_axis(grid_pos(r2, g), g, g.T2, t2, k.yq))
         return k;
@@ -78,6 +91,20 @@ __device__ inline KeyRec sample_key(const SampleSource& src, long long idx, cons
     k.s = (float)sv;
     k.key = (j * g.ntile + t1) * g.ntile2 + t2;
     return k;
+}
+
+__device__ inline KeyRec sample_key(const SampleSource& src, long long idx, const GridGeom& g,
+                                    const SlabParams& sp) {
+    double r1, r2, r3;
+    sample_coords(src, idx, r1, r2, r3);
+    return coord_key(r1, r2, r3, g, sp);
+}
+
+// Key of channel scale `sc` on the row with rotated coordinates q: the separable form of
+// sample_coords (the same three FP64 products) followed by coord_key.
+__device__ inline KeyRec row_chan_key(double sc, double q1, double q2, double q3, const GridGeom& g,
+                                      const SlabParams& sp) {
+    return coord_key(__dmul_rn(sc, q1), __dmul_rn(sc, q2), __dmul_rn(sc, q3), g, sp);
 }
 
 }  // namespace binrules

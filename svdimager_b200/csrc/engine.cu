@@ -99,6 +99,9 @@ struct svdi_engine {
     int sm_count = 148;
     cudaStream_t stream = nullptr;
     bool own_stream = true;
+    // the flag/weight collapse runs on `side`, beside the rotation, statistics and histogram
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_vis = nullptr;
     std::mutex mu;
     // staging for host inputs
     svdi::DevBuf in_uvw, in_freq, in_v0r, in_v0i, in_v3r, in_v3i, in_f0, in_f3, in_w0, in_w3;
@@ -112,6 +115,14 @@ struct svdi_engine {
     const double* cur_q = nullptr;
     const double* cur_s = nullptr;
     double* h_stats = nullptr;  // pinned
+    // Completion of the last call, read lazily (finish_pending): the device-API call returns once
+    // its work is enqueued, so that the host can enqueue the next snapshot meanwhile.
+    unsigned long long* h_ndrop = nullptr;  // pinned: dropped-sample count of the last call
+    bool pending = false;                   // last call's device-side statistics not yet read
+    bool pending_times = false;             // its stage events are valid (single slab batch)
+    bool pending_total = false;             // ev[0] -> ev[7] spans the whole call
+    bool pending_need_s = false;
+    long long pending_n = 0;
     std::map<std::pair<long long, int>, cufftHandle> plans;
     std::map<std::tuple<long long, long long, int, double>, std::vector<float>> corr_cache;
     std::tuple<long long, long long, int, double> corr_key{-1, -1, -1, 0.0};
@@ -137,6 +148,10 @@ struct svdi_engine {
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         if (h_stats) cudaFreeHost(h_stats);
+        if (h_ndrop) cudaFreeHost(h_ndrop);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_vis) cudaEventDestroy(ev_vis);
+        if (side) cudaStreamDestroy(side);
         if (stream && own_stream) cudaStreamDestroy(stream);
     }
 };
@@ -149,8 +164,16 @@ int engine_init(svdi_engine* e, const svdi_options* opt) {
     e->device = opt->device;
     SVDI_CUDA(cudaSetDevice(e->device));
     SVDI_CUDA(cudaDeviceGetAttribute(&e->sm_count, cudaDevAttrMultiProcessorCount, e->device));
-    SVDI_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    // the main stream at the highest priority: when blocks of the side stream's collapse retire,
+    // the block scheduler starts the main stream's kernels first
+    int prio_low = 0, prio_high = 0;
+    SVDI_CUDA(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+    SVDI_CUDA(cudaStreamCreateWithPriority(&e->stream, cudaStreamNonBlocking, prio_high));
+    SVDI_CUDA(cudaStreamCreateWithPriority(&e->side, cudaStreamNonBlocking, prio_low));
+    SVDI_CUDA(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
+    SVDI_CUDA(cudaEventCreateWithFlags(&e->ev_vis, cudaEventDisableTiming));
     SVDI_CUDA(cudaMallocHost(&e->h_stats, ST_COUNT * sizeof(double)));
+    SVDI_CUDA(cudaMallocHost(&e->h_ndrop, 2 * sizeof(unsigned long long)));
     for (auto& ev : e->ev) SVDI_CUDA(cudaEventCreate(&ev));
     return SVDI_OK;
 }
@@ -394,14 +417,49 @@ struct ExecPlan {
 // Imaging core: given vin64 and sample source on the device, produce the image in d_out.
 // fixed: replay a recorded plan (device work only; *d_status_out receives the tensor-core
 // gridder's status word); record: store this call's plan.
+// Reads the last call's device-side results once its work has completed: the dropped-sample
+// count and, when its stage events are valid, the stage and total device times.
+int finish_pending(svdi_engine* e) {
+    if (!e->pending) return SVDI_OK;
+    SVDI_CUDA(cudaEventSynchronize(e->pending_total ? e->ev[7] : e->ev[6]));
+    svdi_stats& L = e->last;
+    const unsigned long long ndrop = *e->h_ndrop;
+    L.num_gridded = (size_t)(e->pending_n - (long long)ndrop);
+    e->sz_rec = (size_t)(e->pending_n - (long long)ndrop) * sizeof(SampleRec);
+    e->sz_rec_s = e->pending_need_s ? (size_t)(e->pending_n - (long long)ndrop) * 4 : 0;
+    if (e->pending_times) {
+        float a = 0, b = 0, c = 0, d = 0;
+        cudaEventElapsedTime(&d, e->ev[1], e->ev[2]);
+        cudaEventElapsedTime(&a, e->ev[3], e->ev[4]);
+        cudaEventElapsedTime(&b, e->ev[4], e->ev[5]);
+        cudaEventElapsedTime(&c, e->ev[5], e->ev[6]);
+        L.ms_bin = d;
+        L.ms_grid = a;
+        L.ms_fft = b;
+        L.ms_image = c;
+    }
+    if (e->pending_total) {
+        float mp = 0, mt = 0;
+        cudaEventElapsedTime(&mp, e->ev[0], e->ev[1]);
+        cudaEventElapsedTime(&mt, e->ev[0], e->ev[7]);
+        L.ms_preprocess = mp;
+        L.ms_total = mt;
+    }
+    e->pending = false;
+    return SVDI_OK;
+}
+
+// vis_ready (optional): event after which src.vr / src.vi hold the collapsed visibilities; only
+// the scatter reads them.
 int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, float cell_f,
                float* d_out, const ExecPlan* fixed = nullptr, ExecPlan* record = nullptr,
-               unsigned int* d_status_out = nullptr) {
+               unsigned int* d_status_out = nullptr, cudaEvent_t vis_ready = nullptr) {
     cudaStream_t st = e->stream;
     const svdi_options& o = e->opt;
     const double cell = (double)cell_f;
     const long long n = src.n;
     const bool timed = fixed == nullptr;  // events, statistics and status read-back
+    if (timed) e->pending = false;         // the previous call's statistics are superseded
     SlabParams sp{};
     double alpha_max = 0, slab_alpha = 0, r3min = 0, r3max = 0, mt3 = 0;
     if (fixed) {
@@ -491,6 +549,7 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
         SVDI_TRY(e->tc_status.ensure(4 * sizeof(unsigned int)));
         SVDI_CUDA(cudaMemsetAsync(e->tc_status.p, 0, 4 * sizeof(unsigned int), st));
     }
+    if (vis_ready) SVDI_CUDA(cudaStreamWaitEvent(st, vis_ready, 0));
     SVDI_TRY(launch_scatter(src, g, sp, e->cursor.as<unsigned int>(), n_keys, e->rec.as<SampleRec>(),
                             need_s ? e->rec_s.as<float>() : nullptr,
                             use_tc ? e->tc_status.as<unsigned int>() + 1 : nullptr, st));
@@ -557,6 +616,7 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
                                   st, multi_batch ? e->acc.as<double>() : nullptr, s1 == sp.nslab));
         if (!timed) continue;
         SVDI_CUDA(cudaEventRecord(e->ev[6], st));
+        if (!multi_batch) continue;  // one batch: its stage times are read when the call completes
         SVDI_CUDA(cudaEventSynchronize(e->ev[6]));
         float a = 0, b = 0, c = 0;
         cudaEventElapsedTime(&a, e->ev[3], e->ev[4]);
@@ -582,20 +642,32 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
         }
         return SVDI_OK;
     }
-    unsigned long long ndrop = 0;
-    unsigned int tc_status = 0;
-    SVDI_CUDA(cudaMemcpyAsync(&ndrop, e->dropped.p, 8, cudaMemcpyDeviceToHost, st));
-    if (use_tc) SVDI_CUDA(cudaMemcpyAsync(&tc_status, e->tc_status.p, 4, cudaMemcpyDeviceToHost, st));
-    SVDI_CUDA(cudaStreamSynchronize(st));
-    if (tc_status != 0) {
-        set_error("tensor-core gridder gave up waiting for an MMA completion (status " +
-                  std::to_string(tc_status) + "); the grid is incomplete");
-        return SVDI_ERR_INTERNAL;
+    SVDI_CUDA(cudaMemcpyAsync(e->h_ndrop, e->dropped.p, 8, cudaMemcpyDeviceToHost, st));
+    if (use_tc) {  // the tensor-core gridder's give-up status is checked before the call returns
+        unsigned int tc_status = 0;
+        SVDI_CUDA(cudaMemcpyAsync(&tc_status, e->tc_status.p, 4, cudaMemcpyDeviceToHost, st));
+        SVDI_CUDA(cudaStreamSynchronize(st));
+        if (tc_status != 0) {
+            set_error("tensor-core gridder gave up waiting for an MMA completion (status " +
+                      std::to_string(tc_status) + "); the grid is incomplete");
+            return SVDI_ERR_INTERNAL;
+        }
+    }
+    e->pending = true;
+    e->pending_times = !multi_batch;
+    e->pending_total = false;
+    e->pending_need_s = need_s;
+    e->pending_n = n;
+    if (multi_batch) {
+        float mb = 0;
+        cudaEventElapsedTime(&mb, e->ev[1], e->ev[2]);
+        e->last.ms_bin = mb;
+        e->last.ms_grid = ms_grid;
+        e->last.ms_fft = ms_fft;
+        e->last.ms_image = ms_img;
     }
 
     e->sz_off = (size_t)(n_keys + 1) * 4;
-    e->sz_rec = (size_t)(n - (long long)ndrop) * sizeof(SampleRec);
-    e->sz_rec_s = need_s ? (size_t)(n - (long long)ndrop) * 4 : 0;
     e->sz_mom = plane_bytes * (size_t)planes_per_batch;
     e->cur_vr = src.vr;
     e->cur_vi = src.vi;
@@ -611,7 +683,6 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     L.slab_width = sp.slab_width;
     L.slab_half = sp.slab_half;
     L.num_samples = (size_t)n;
-    L.num_gridded = (size_t)(n - (long long)ndrop);
     L.grid_size = (size_t)g.G;
     L.num_slabs = sp.nslab;
     L.num_terms = sp.K;
@@ -622,12 +693,6 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     L.valid_pixels = (size_t)e->h_stats[ST_VALID_PIX];
     L.alpha_max = alpha_max;
     L.slab_alpha_max = slab_alpha;
-    float mb = 0;
-    cudaEventElapsedTime(&mb, e->ev[1], e->ev[2]);
-    L.ms_bin = mb;
-    L.ms_grid = ms_grid;
-    L.ms_fft = ms_fft;
-    L.ms_image = ms_img;
     return SVDI_OK;
 }
 
@@ -704,8 +769,13 @@ int main_path_device(svdi_engine* e, const svdi_host_ms* d, size_t N, float cell
     SVDI_TRY(e->vin32.ensure(9 * 4));
     SVDI_TRY(e->stats.ensure(ST_COUNT * 8));
     SVDI_TRY(e->partial.ensure((size_t)kPartialCap * 9 * 8));
+    // the collapse (HBM-bound) overlaps the rotation, the statistics read-back and the histogram
+    // (compute-bound), which need only uvw and frequencies; the scatter waits for it
+    SVDI_CUDA(cudaEventRecord(e->ev_fork, st));
+    SVDI_CUDA(cudaStreamWaitEvent(e->side, e->ev_fork, 0));
     SVDI_TRY(launch_collapse(d->vis0_real, d->vis0_imag, d->vis3_real, d->vis3_imag, d->flag0, d->flag3,
-                             d->weight0, d->weight3, e->vr.as<float>(), e->vi.as<float>(), n, st));
+                             d->weight0, d->weight3, e->vr.as<float>(), e->vi.as<float>(), n, e->side));
+    SVDI_CUDA(cudaEventRecord(e->ev_vis, e->side));
     SVDI_TRY(launch_preprocess(d->uvw, d->frequencies_hz, R, C, d->array_center_x, e->partial.as<double>(),
                                kPartialCap, e->vin64.as<double>(), e->vin32.as<float>(), e->q.as<double>(),
                                e->s.as<double>(), e->stats.as<double>(), st));
@@ -718,15 +788,10 @@ int main_path_device(svdi_engine* e, const svdi_host_ms* d, size_t N, float cell
     src.n = n;
     e->sz_q = (size_t)R * 24;
     e->sz_s = (size_t)C * 8;
-    SVDI_TRY(image_core(e, false, src, (long long)N, cell, d_out, fixed, record, d_status_out));
+    SVDI_TRY(image_core(e, false, src, (long long)N, cell, d_out, fixed, record, d_status_out, e->ev_vis));
     if (fixed) return SVDI_OK;
-    float mp = 0, mt = 0;
-    cudaEventElapsedTime(&mp, e->ev[0], e->ev[1]);
     SVDI_CUDA(cudaEventRecord(e->ev[7], st));
-    SVDI_CUDA(cudaEventSynchronize(e->ev[7]));
-    cudaEventElapsedTime(&mt, e->ev[0], e->ev[7]);
-    e->last.ms_preprocess = mp;
-    e->last.ms_total = mt;
+    e->pending_total = true;  // preprocessing and total times are read with the other statistics
     return SVDI_OK;
 }
 
@@ -775,6 +840,7 @@ int archive_path(svdi_engine* e, const float* Visreal, const float* Visimag, con
     SVDI_CUDA(cudaMemcpyAsync(dirty_image, e->image.p, N * N * 4, cudaMemcpyDeviceToHost, st));
     SVDI_CUDA(cudaEventRecord(e->ev[7], st));
     SVDI_CUDA(cudaStreamSynchronize(st));
+    SVDI_TRY(finish_pending(e));
     float mt = 0;
     cudaEventElapsedTime(&mt, e->ev[0], e->ev[7]);
     e->last.ms_total = mt;
@@ -868,16 +934,22 @@ int svdi_engine_image_host(svdi_engine* e, const svdi_host_ms* h, size_t N, floa
     SVDI_CUDA(cudaSetDevice(e->device));
     cudaStream_t st = e->stream;
     const size_t n = h->num_samples, R = h->num_rows, C = h->num_channels;
+    // uvw and frequencies first on the main stream: the rotation, statistics, histogram and scan
+    // need only these and run while the visibilities, flags and weights upload on the side
+    // stream, which then collapses them (main_path_device)
     SVDI_TRY(upload(e->in_uvw, h->uvw, R * 3, st));
     SVDI_TRY(upload(e->in_freq, h->frequencies_hz, C, st));
-    SVDI_TRY(upload(e->in_v0r, h->vis0_real, n, st));
-    SVDI_TRY(upload(e->in_v0i, h->vis0_imag, n, st));
-    SVDI_TRY(upload(e->in_v3r, h->vis3_real, n, st));
-    SVDI_TRY(upload(e->in_v3i, h->vis3_imag, n, st));
-    SVDI_TRY(upload(e->in_f0, h->flag0, n, st));
-    SVDI_TRY(upload(e->in_f3, h->flag3, n, st));
-    SVDI_TRY(upload(e->in_w0, h->weight0, n, st));
-    SVDI_TRY(upload(e->in_w3, h->weight3, n, st));
+    SVDI_CUDA(cudaEventRecord(e->ev_fork, st));
+    SVDI_CUDA(cudaStreamWaitEvent(e->side, e->ev_fork, 0));
+    cudaStream_t sd = e->side;
+    SVDI_TRY(upload(e->in_v0r, h->vis0_real, n, sd));
+    SVDI_TRY(upload(e->in_v0i, h->vis0_imag, n, sd));
+    SVDI_TRY(upload(e->in_v3r, h->vis3_real, n, sd));
+    SVDI_TRY(upload(e->in_v3i, h->vis3_imag, n, sd));
+    SVDI_TRY(upload(e->in_f0, h->flag0, n, sd));
+    SVDI_TRY(upload(e->in_f3, h->flag3, n, sd));
+    SVDI_TRY(upload(e->in_w0, h->weight0, n, sd));
+    SVDI_TRY(upload(e->in_w3, h->weight3, n, sd));
     svdi_host_ms d = *h;
     d.uvw = e->in_uvw.as<float>();
     d.frequencies_hz = e->in_freq.as<float>();
@@ -893,6 +965,7 @@ int svdi_engine_image_host(svdi_engine* e, const svdi_host_ms* h, size_t N, floa
     SVDI_TRY(main_path_device(e, &d, N, cell, e->image.as<float>()));
     SVDI_CUDA(cudaMemcpyAsync(dirty_image, e->image.p, N * N * 4, cudaMemcpyDeviceToHost, st));
     SVDI_CUDA(cudaStreamSynchronize(st));
+    SVDI_TRY(finish_pending(e));
     return SVDI_OK;
 }
 
@@ -907,16 +980,14 @@ int svdi_engine_image_device(svdi_engine* e, const svdi_host_ms* d, size_t N, fl
     SVDI_TRY(check_image_args(N, cell));
     std::lock_guard<std::mutex> lk(e->mu);
     SVDI_CUDA(cudaSetDevice(e->device));
+    // the call is ordered on the caller's stream (0: the legacy default stream): it starts after
+    // the caller's earlier work there and the caller's later work there sees the image
     cudaStream_t user = (cudaStream_t)cuda_stream;
-    if (user) {  // order the engine stream after the caller's work
-        SVDI_CUDA(cudaEventRecord(e->ev[0], user));
-        SVDI_CUDA(cudaStreamWaitEvent(e->stream, e->ev[0], 0));
-    }
+    SVDI_CUDA(cudaEventRecord(e->ev[0], user));
+    SVDI_CUDA(cudaStreamWaitEvent(e->stream, e->ev[0], 0));
     SVDI_TRY(main_path_device(e, d, N, cell, d_out));
-    if (user) {
-        SVDI_CUDA(cudaEventRecord(e->ev[7], e->stream));
-        SVDI_CUDA(cudaStreamWaitEvent(user, e->ev[7], 0));
-    }
+    SVDI_CUDA(cudaEventRecord(e->ev[7], e->stream));
+    SVDI_CUDA(cudaStreamWaitEvent(user, e->ev[7], 0));
     return SVDI_OK;
 }
 
@@ -936,6 +1007,10 @@ int svdi_engine_last_stats(const svdi_engine* e, svdi_stats* out) {
         set_error("null argument");
         return SVDI_ERR_INVALID_ARGUMENT;
     }
+    svdi_engine* m = const_cast<svdi_engine*>(e);
+    std::lock_guard<std::mutex> lk(m->mu);
+    SVDI_CUDA(cudaSetDevice(m->device));
+    SVDI_TRY(finish_pending(m));
     *out = e->last;
     return SVDI_OK;
 }
@@ -963,6 +1038,10 @@ int svdi_engine_buffer_size(const svdi_engine* e, int which, size_t* bytes) {
         set_error("null argument");
         return SVDI_ERR_INVALID_ARGUMENT;
     }
+    svdi_engine* m = const_cast<svdi_engine*>(e);
+    std::lock_guard<std::mutex> lk(m->mu);
+    SVDI_CUDA(cudaSetDevice(m->device));
+    SVDI_TRY(finish_pending(m));
     const void* p = nullptr;
     return buffer_of(e, which, &p, bytes);
 }
@@ -973,6 +1052,8 @@ int svdi_engine_copy_buffer(svdi_engine* e, int which, void* host_dst, size_t by
         return SVDI_ERR_INVALID_ARGUMENT;
     }
     std::lock_guard<std::mutex> lk(e->mu);
+    SVDI_CUDA(cudaSetDevice(e->device));
+    SVDI_TRY(finish_pending(e));
     const void* p = nullptr;
     size_t have = 0;
     SVDI_TRY(buffer_of(e, which, &p, &have));
@@ -1088,6 +1169,7 @@ int svdi_fipipe_device(const svdi_device_buffers* dev, float* dirty_image, size_
     SVDI_TRY(image_core(e, false, src, (long long)N, cell, e->image.as<float>()));
     SVDI_CUDA(cudaMemcpyAsync(dirty_image, e->image.p, N * N * 4, cudaMemcpyDeviceToHost, e->stream));
     SVDI_CUDA(cudaStreamSynchronize(e->stream));
+    SVDI_TRY(finish_pending(e));
     return SVDI_OK;
 }
 
@@ -1171,6 +1253,7 @@ int svdi_batch_create(svdi_engine* e, const svdi_host_ms* snapshots, size_t num_
     for (size_t s = 0; s < num_snapshots; ++s)
         SVDI_TRY(main_path_device(e, &b->snaps[s], image_size, cell_size, d_images + s * NN, nullptr, &b->plans[s]));
     SVDI_CUDA(cudaStreamSynchronize(e->stream));
+    SVDI_TRY(finish_pending(e));
     // capture the device work of every snapshot with its plan
     SVDI_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
     int rc = SVDI_OK;

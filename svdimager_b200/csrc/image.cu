@@ -20,23 +20,40 @@ struct SplatTarget {
     bool ok;
 };
 
-// SVDIntegratedImager.cu:1325-1379 (simplified SIN deprojection; keeps p1, p2 when h > r0)
-__device__ inline SplatTarget reproject_sii(long long idx, long long idy, long long N, double dc_rad,
+// Per-launch constants of the deprojection, computed once per block from Vin.
+struct ReprojConst {
+    double xi, eta;     // V[6] / V[8], V[7] / V[8]
+    double inv_v8;      // 1 / |V[8]|
+    double dc, inv_dc;  // cell in degrees and its reciprocal
+};
+
+__device__ inline ReprojConst reproj_const(const double* V, double dc_rad) {
+    ReprojConst c;
+    c.xi = V[6] / V[8];
+    c.eta = V[7] / V[8];
+    c.inv_v8 = 1.0 / fabs(V[8]);
+    c.dc = dc_rad / kPi * 180.0;
+    c.inv_dc = 1.0 / c.dc;
+    return c;
+}
+
+// SVDIntegratedImager.cu:1325-1379 (simplified SIN deprojection; keeps p1, p2 when h > r0), with
+// the divisions by per-launch constants as products by their reciprocals and one 1 / h.
+__device__ inline SplatTarget reproject_sii(long long idx, long long idy, long long N, const ReprojConst& k,
                                             const double* V) {
-    const double r0 = 180.0 / kPi;
-    const double dc = dc_rad / kPi * 180.0;
+    const double r0 = 180.0 / kPi, inv_r0 = kPi / 180.0;
     const double di2 = (double)N * 0.5;
     const long long half = N / 2;
-    const double xi = V[6] / V[8], eta = V[7] / V[8];
     const double idxf = (double)idx - di2, idyf = (double)idy - di2;
-    const double p1 = (-V[0] * idxf + V[3] * idyf) / fabs(V[8]) + di2;
-    const double p2 = (-V[1] * idxf + V[4] * idyf) / fabs(V[8]) + di2;
-    double x = -dc * (p1 - (di2 + 1.0));
-    double y = dc * (p2 - (di2 + 1.0));
-    const double h = hypot(x, y), hr0 = h / r0;
+    const double p1 = (-V[0] * idxf + V[3] * idyf) * k.inv_v8 + di2;
+    const double p2 = (-V[1] * idxf + V[4] * idyf) * k.inv_v8 + di2;
+    double x = -k.dc * (p1 - (di2 + 1.0));
+    double y = k.dc * (p2 - (di2 + 1.0));
+    const double h = sqrt(fma(x, x, y * y)), hr0 = h * inv_r0;
     if (h != 0.0) {
-        x /= h;
-        y /= -h;
+        const double ih = 1.0 / h;
+        x *= ih;
+        y *= -ih;
     } else {
         x = 0.0;
         y = 1.0;
@@ -44,18 +61,18 @@ __device__ inline SplatTarget reproject_sii(long long idx, long long idy, long l
     double oi0, oi1;
     if (h <= r0) {
         const double r = h;
-        const double z = (h < r0 * sqrt(0.5)) ? 1.0 - sqrt(1.0 - hr0 * hr0)
-                                              : hr0 * hr0 / (1.0 + sqrt(1.0 - hr0 * hr0));
-        const double w = xi * xi + eta * eta;
+        const double sq = sqrt(1.0 - hr0 * hr0);
+        const double z = (h < r0 * sqrt(0.5)) ? 1.0 - sq : hr0 * hr0 / (1.0 + sq);
+        const double w = k.xi * k.xi + k.eta * k.eta;
         if (w == 0.0) {
             x = r * x;
             y = -r * y;
         } else {
-            x = r * x + z * r0 * xi;
-            y = -r * y + z * r0 * eta;
+            x = r * x + z * r0 * k.xi;
+            y = -r * y + z * r0 * k.eta;
         }
-        oi0 = -x / dc + di2 + 1.0;
-        oi1 = y / dc + di2 + 1.0;
+        oi0 = -x * k.inv_dc + di2 + 1.0;
+        oi1 = y * k.inv_dc + di2 + 1.0;
     } else {
         oi0 = p1;
         oi1 = p2;
@@ -114,6 +131,9 @@ __global__ void __launch_bounds__(256) k_recombine(const float2* __restrict__ mo
                                                   double inv_n, int reprojection, int presplat,
                                                   float* __restrict__ out, double* __restrict__ acc,
                                                   int final_batch) {
+    __shared__ ReprojConst kc;
+    if (threadIdx.x == 0 && threadIdx.y == 0) kc = reproj_const(vin, cell);
+    __syncthreads();
     const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const long long y = blockIdx.y * (long long)blockDim.y + threadIdx.y;
     if (x >= N || y >= N) return;
@@ -139,7 +159,7 @@ __global__ void __launch_bounds__(256) k_recombine(const float2* __restrict__ mo
     for (int j = 0; j < sp.nslab; ++j) {
         const double centre = sp.r3_min + ((double)j + 0.5) * sp.slab_width;
         double sb, cb;
-        sincos(2.0 * kPi * t3 * centre, &sb, &cb);
+        sincospi(2.0 * t3 * centre, &sb, &cb);   // e^{i 2 pi t3 centre}
         const float2* mp = moments + (long long)j * K * GG + gidx;
         for (int n = 0; n < K; ++n) {
             const float2 m = mp[(long long)n * GG];
@@ -171,7 +191,7 @@ __global__ void __launch_bounds__(256) k_recombine(const float2* __restrict__ mo
     }
 
     const SplatTarget tg = reprojection == SVDI_REPROJ_FIPK ? reproject_fipk(x, y, N, cell, V)
-                                                            : reproject_sii(x, y, N, cell, V);
+                                                            : reproject_sii(x, y, N, kc, V);
     if (!tg.ok) return;
     const double LL = tg.LL, MM = tg.MM;
     if (!(fabs(LL) < (double)(half - 1) && fabs(MM) < (double)(half - 1))) return;

@@ -191,6 +191,60 @@ __global__ void __launch_bounds__(kThreads) k_collapse(const float* __restrict__
     }
 }
 
+__device__ __forceinline__ void collapse_one(float a0r, float a0i, float a3r, float a3i, uint8_t g0, uint8_t g3,
+                                             float w0in, float w3in, float& re, float& im) {
+    const float w0 = g0 ? 0.0f : w0in;
+    const float w3 = g3 ? 0.0f : w3in;
+    const float ws = __fadd_rn(w0, w3);
+    re = 0.0f;
+    im = 0.0f;
+    if (ws > 0.0f) {
+        re = __fdiv_rn(__fadd_rn(__fmul_rn(a0r, w0), __fmul_rn(a3r, w3)), ws);
+        im = __fdiv_rn(__fadd_rn(__fmul_rn(a0i, w0), __fmul_rn(a3i, w3)), ws);
+    }
+}
+
+// The same collapse on four consecutive samples per thread with 16-byte loads and stores (all
+// float arrays 16-byte and both flag arrays 4-byte aligned; n4 = n / 4 groups, the tail of
+// n % 4 samples by the first threads). Its grid fills half of each SM, so that kernels of the
+// main stream (rotation, statistics, histogram) run beside it.
+__global__ void __launch_bounds__(kThreads) k_collapse4(const float4* __restrict__ v0r, const float4* __restrict__ v0i,
+                                                       const float4* __restrict__ v3r, const float4* __restrict__ v3i,
+                                                       const uchar4* __restrict__ f0, const uchar4* __restrict__ f3,
+                                                       const float4* __restrict__ w0in, const float4* __restrict__ w3in,
+                                                       float4* __restrict__ outr, float4* __restrict__ outi,
+                                                       long long n) {
+    const long long n4 = n >> 2;
+    for (long long k = blockIdx.x * (long long)kThreads + threadIdx.x; k < n4;
+         k += (long long)gridDim.x * kThreads) {
+        const float4 a0r = v0r[k], a0i = v0i[k], a3r = v3r[k], a3i = v3i[k], b0 = w0in[k], b3 = w3in[k];
+        const uchar4 g0 = f0[k], g3 = f3[k];
+        float4 re, im;
+        collapse_one(a0r.x, a0i.x, a3r.x, a3i.x, g0.x, g3.x, b0.x, b3.x, re.x, im.x);
+        collapse_one(a0r.y, a0i.y, a3r.y, a3i.y, g0.y, g3.y, b0.y, b3.y, re.y, im.y);
+        collapse_one(a0r.z, a0i.z, a3r.z, a3i.z, g0.z, g3.z, b0.z, b3.z, re.z, im.z);
+        collapse_one(a0r.w, a0i.w, a3r.w, a3i.w, g0.w, g3.w, b0.w, b3.w, re.w, im.w);
+        outr[k] = re;
+        outi[k] = im;
+    }
+    const long long t = blockIdx.x * (long long)kThreads + threadIdx.x;
+    const long long k = (n4 << 2) + t;
+    if (t < (n & 3)) {
+        const float* s0r = reinterpret_cast<const float*>(v0r);
+        const float* s0i = reinterpret_cast<const float*>(v0i);
+        const float* s3r = reinterpret_cast<const float*>(v3r);
+        const float* s3i = reinterpret_cast<const float*>(v3i);
+        const uint8_t* h0 = reinterpret_cast<const uint8_t*>(f0);
+        const uint8_t* h3 = reinterpret_cast<const uint8_t*>(f3);
+        const float* c0 = reinterpret_cast<const float*>(w0in);
+        const float* c3 = reinterpret_cast<const float*>(w3in);
+        float re, im;
+        collapse_one(s0r[k], s0i[k], s3r[k], s3i[k], h0[k], h3[k], c0[k], c3[k], re, im);
+        reinterpret_cast<float*>(outr)[k] = re;
+        reinterpret_cast<float*>(outi)[k] = im;
+    }
+}
+
 // Optional float Bin [N_s][3] of the reference layout: bin[k] = float(s[chan] * q[row]).
 __global__ void __launch_bounds__(kThreads) k_expand_bin(const double* __restrict__ q, const double* __restrict__ s,
                                                         long long R, long long C, float* __restrict__ bin) {
@@ -378,7 +432,24 @@ int launch_preprocess(const float* d_uvw, const float* d_freq, long long R, long
 int launch_collapse(const float* v0r, const float* v0i, const float* v3r, const float* v3i,
                     const uint8_t* f0, const uint8_t* f3, const float* w0, const float* w3,
                     float* outr, float* outi, long long n, cudaStream_t st) {
-    k_collapse<<<grid_for(n, 148 * 16), kThreads, 0, st>>>(v0r, v0i, v3r, v3i, f0, f3, w0, w3, outr, outi, n);
+    auto al = [](const void* p, uintptr_t a) { return ((uintptr_t)p & (a - 1)) == 0; };
+    if (al(v0r, 16) && al(v0i, 16) && al(v3r, 16) && al(v3i, 16) && al(w0, 16) && al(w3, 16) && al(outr, 16) &&
+        al(outi, 16) && al(f0, 4) && al(f3, 4)) {
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess)
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        long long b = ((n >> 2) + kThreads - 1) / kThreads;
+        if (b > (long long)sms * 4) b = (long long)sms * 4;   // 4 of the 8 resident 256-thread blocks per SM
+        if (b < 1) b = 1;
+        k_collapse4<<<(int)b, kThreads, 0, st>>>(
+            reinterpret_cast<const float4*>(v0r), reinterpret_cast<const float4*>(v0i),
+            reinterpret_cast<const float4*>(v3r), reinterpret_cast<const float4*>(v3i),
+            reinterpret_cast<const uchar4*>(f0), reinterpret_cast<const uchar4*>(f3),
+            reinterpret_cast<const float4*>(w0), reinterpret_cast<const float4*>(w3),
+            reinterpret_cast<float4*>(outr), reinterpret_cast<float4*>(outi), n);
+    } else {
+        k_collapse<<<grid_for(n, 148 * 16), kThreads, 0, st>>>(v0r, v0i, v3r, v3i, f0, f3, w0, w3, outr, outi, n);
+    }
     SVDI_LAUNCHED();
     return SVDI_OK;
 }
