@@ -29,8 +29,6 @@ namespace svdi {
 
 namespace {
 
-constexpr int kThreads = 256;
-constexpr int kWarps = kThreads / 32;
 
 // Exact ES kernel psi(x) = exp(beta (sqrt(1 - x^2) - 1)) written without cancellation (rare path).
 __device__ __forceinline__ float es_exact(float beta, float x) {
@@ -46,8 +44,35 @@ __device__ __forceinline__ int fx_round(float x_plus_magic) {
     return __float_as_int(x_plus_magic) - kMagicBits;
 }
 
+// red.shared.add.u32 at shared-window address addr + OFF (OFF an immediate)
+template <int OFF>
+__device__ __forceinline__ void red_shared(unsigned int addr, int v) {
+    asm volatile("red.shared.add.u32 [%0+%2], %1;" ::"r"(addr), "r"(v), "n"(OFF) : "memory");
+}
+
+__device__ __forceinline__ void red_add_v4(float2* addr, float a, float b, float c, float d) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(addr), "f"(a), "f"(b), "f"(c), "f"(d)
+                 : "memory");
+}
+
 __device__ __forceinline__ void red_add_v2(float2* addr, float a, float b) {
     asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(addr), "f"(a), "f"(b) : "memory");
+}
+
+// Passes P..PASSES-1 of one sample's footprint for this lane (one cell per pass): x-weight from the
+// lane that evaluated it, then one fixed-point reduction per component at an immediate offset.
+template <int P, int PASSES, int RPP, int RS, int PLANE, bool ALL>
+__device__ __forceinline__ void grid_passes(unsigned int a, float w, float wy, float vr, float vi, int src0,
+                                            const int* wx_src, const bool* pass_on) {
+    if constexpr (P < PASSES) {
+        const float wx = __shfl_sync(0xffffffffu, w, src0 + wx_src[P]);
+        if (ALL || pass_on[P]) {
+            const float kv = wx * wy;
+            red_shared<4 * P * RPP * RS>(a, fx_round(fmaf(kv, vr, kMagic)));
+            red_shared<4 * (P * RPP * RS + PLANE)>(a, fx_round(fmaf(kv, vi, kMagic)));
+        }
+        grid_passes<P + 1, PASSES, RPP, RS, PLANE, ALL>(a, w, wy, vr, vi, src0, wx_src, pass_on);
+    }
 }
 
 template <int W, int T, int KC>
@@ -56,11 +81,13 @@ struct TileCfg {
     static constexpr int RS = R;          // row stride; R == W (mod 32) for T in {32, 64}
     static constexpr int PLANE = R * RS;  // floats per re or im plane
     static constexpr size_t SMEM = (size_t)KC * 2 * PLANE * sizeof(float);
+    static constexpr int NT = 256;  // threads per CTA
+    static constexpr int NW = NT / 32;
     static_assert((RS % 32) == (W % 32), "row stride must be == W (mod 32)");
 };
 
 template <int W, int T, int KC>
-__global__ void __launch_bounds__(kThreads) k_grid_fp32(
+__global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
     const SampleRec* __restrict__ rec, const float* __restrict__ rec_s,
     const unsigned int* __restrict__ offsets, int key_lo, int key_hi, int slab_lo, GridGeom g,
     SlabParams sp, EsPoly poly, float2* __restrict__ planes, int term0, unsigned int chunk) {
@@ -70,14 +97,16 @@ __global__ void __launch_bounds__(kThreads) k_grid_fp32(
     __shared__ int bbox[4];          // row min, row max, col min, col max
     __shared__ int seg_key;
     // per-warp staging of the decoded batch: {u_x, u_y, vre, vim} and {fast-path base, s}
-    __shared__ float4 st_f[kWarps][32];
-    __shared__ int2 st_i[kWarps][32];
+    constexpr int kThreads = C::NT, kWarps = C::NW;
+    __shared__ float4 st_f[kWarps][33];  // 32 samples + the zero pad
+    __shared__ int2 st_i[kWarps][33];
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int HW = W / 2;
     constexpr int RPP = 32 / W;                  // footprint rows per pass
     constexpr int PASSES = (W + RPP - 1) / RPP;
     constexpr bool PAIR = 2 * W <= 16;           // two samples per polynomial pass
+    constexpr bool kAllLanes = (32 % W) == 0;    // every lane owns a cell in every pass
     const int la = lane / W, lb = lane % W;
     const bool lane_cell = lane < RPP * W;
     const int lane_off = la * C::RS + lb;
@@ -88,6 +117,15 @@ __global__ void __launch_bounds__(kThreads) k_grid_fp32(
     float coef[kPolyDeg + 1];
 #pragma unroll
     for (int d = 0; d <= kPolyDeg; ++d) coef[d] = poly.c[piece][d];
+    int wx_src[PASSES];     // lane holding the x-weight of this lane's row in pass p
+    bool pass_on[PASSES];   // this lane owns a footprint cell in pass p
+#pragma unroll
+    for (int p = 0; p < PASSES; ++p) {
+        const int i = la + p * RPP;
+        wx_src[p] = i < W ? i : 0;
+        pass_on[p] = lane_cell && i < W;
+    }
+    const unsigned int tile_s = (unsigned int)__cvta_generic_to_shared(tile);
 
     for (int i = threadIdx.x; i < KC * 2 * C::PLANE; i += kThreads) tile[i] = 0;
     if (threadIdx.x == 0) {
@@ -160,10 +198,21 @@ __global__ void __launch_bounds__(kThreads) k_grid_fp32(
                     const int fxq = r.xq & 0xFFFFFF, fyq = r.yq & 0xFFFFFF;
                     const int r0 = cx - (HW - 1), c0 = cy - (HW - 1);
                     const bool rare = valid && (fxq == 0 || fyq == 0 || r0 < 0 || c0 < 0);
-                    st_f[warp][lane] = make_float4(fmaf(2.0f, (float)fxq * (1.0f / 16777216.0f), -1.0f),
-                                                   fmaf(2.0f, (float)fyq * (1.0f / 16777216.0f), -1.0f),
-                                                   r.vre * scale, r.vim * scale);
-                    st_i[warp][lane] = make_int2(r0 * C::RS + c0, __float_as_int(sv));
+                    // fast samples compacted into slots [0, nfast); slot nfast is a zero pad, so
+                    // the pair loop below needs no per-sample test
+                    const unsigned int fast_mask = __ballot_sync(0xffffffffu, valid && !rare);
+                    const int nfast = __popc(fast_mask);
+                    if (valid && !rare) {
+                        const int pos = __popc(fast_mask & ((1u << lane) - 1u));
+                        st_f[warp][pos] = make_float4(fmaf(2.0f, (float)fxq * (1.0f / 16777216.0f), -1.0f),
+                                                      fmaf(2.0f, (float)fyq * (1.0f / 16777216.0f), -1.0f),
+                                                      r.vre * scale, r.vim * scale);
+                        st_i[warp][pos] = make_int2(r0 * C::RS + c0, __float_as_int(sv));
+                    }
+                    if (lane == 0) {
+                        st_f[warp][nfast] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                        st_i[warp][nfast] = make_int2(0, 0);
+                    }
                     // bounding box of the batch (one warp reduction per 32 samples)
                     const int rlo = valid ? max(0, fxq ? r0 : r0 - 1) : C::R;
                     const int rhi = valid ? cx + HW : -1;
@@ -179,48 +228,55 @@ __global__ void __launch_bounds__(kThreads) k_grid_fp32(
                     }
                     unsigned int rare_mask = __ballot_sync(0xffffffffu, rare);
                     __syncwarp();
-                    const int nb = min(32u, s_end - b0);
                     // ---- fast path: W x W footprint, polynomial weights, no bounds checks
                     constexpr int STEP = PAIR ? 2 : 1;
-                    for (int j = 0; j < nb; j += STEP) {
-                        const int jw = PAIR ? min(j + (lane >> 4), 31) : j;
-                        const float4 su = st_f[warp][jw];
-                        const float u = is_x ? su.x : su.y;
-                        float w = coef[kPolyDeg];
+                    if (!need_s) {
+                        for (int j = 0; j < nfast; j += STEP) {
+                            const float4 su = st_f[warp][PAIR ? j + (lane >> 4) : j];
+                            const float u = is_x ? su.x : su.y;
+                            float w = coef[kPolyDeg];
 #pragma unroll
-                        for (int d = kPolyDeg - 1; d >= 0; --d) w = fmaf(w, u, coef[d]);
+                            for (int d = kPolyDeg - 1; d >= 0; --d) w = fmaf(w, u, coef[d]);
 #pragma unroll
-                        for (int h = 0; h < STEP; ++h) {
-                            const int js = j + h;
-                            if (js >= nb || ((rare_mask >> js) & 1u)) continue;  // warp-uniform
-                            const float4 sf = st_f[warp][js];
-                            const int2 si = st_i[warp][js];
-                            const int src = PAIR ? 16 * h : 0;
-                            const float wy = __shfl_sync(0xffffffffu, w, src + W + lb);
-                            float tv[KC];
-                            if (!need_s) {
-                                tv[0] = 1.0f;
-                            } else {
-                                const float s = __int_as_float(si.y);
-                                float tm2 = 1.0f, tm1 = s;
-                                for (int t = 0; t < term0 + KC; ++t) {
-                                    const float tn = t == 0 ? 1.0f : (t == 1 ? s : 2.0f * s * tm1 - tm2);
-                                    if (t >= 2) { tm2 = tm1; tm1 = tn; }
-                                    if (t >= term0) tv[t - term0] = tn;
-                                }
+                            for (int h = 0; h < STEP; ++h) {
+                                const float4 sf = st_f[warp][j + h];
+                                const int base = st_i[warp][j + h].x;
+                                const float wy = __shfl_sync(0xffffffffu, w, 16 * h + W + lb);
+                                const unsigned int a = tile_s + 4u * (unsigned int)(base + lane_off);
+#pragma unroll
+                                grid_passes<0, PASSES, RPP, C::RS, C::PLANE, kAllLanes>(
+                                    a, w, wy, sf.z, sf.w, 16 * h, wx_src, pass_on);
                             }
-                            const int base = si.x + lane_off;
+                        }
+                    } else {
+                        for (int j = 0; j < nfast; j += STEP) {
+                            const float4 su = st_f[warp][PAIR ? j + (lane >> 4) : j];
+                            const float u = is_x ? su.x : su.y;
+                            float w = coef[kPolyDeg];
 #pragma unroll
-                            for (int p = 0; p < PASSES; ++p) {
-                                const int i = la + p * RPP;
-                                const float wx = __shfl_sync(0xffffffffu, w, src + (i < W ? i : 0));
-                                if (lane_cell && i < W) {
-                                    const float kv = wx * wy;
-                                    int* pl = tile + base + p * RPP * C::RS;
-                                    if (!need_s) {
-                                        atomicAdd(pl, fx_round(fmaf(kv, sf.z, kMagic)));
-                                        atomicAdd(pl + C::PLANE, fx_round(fmaf(kv, sf.w, kMagic)));
-                                    } else {
+                            for (int d = kPolyDeg - 1; d >= 0; --d) w = fmaf(w, u, coef[d]);
+#pragma unroll
+                            for (int h = 0; h < STEP; ++h) {
+                                const float4 sf = st_f[warp][j + h];
+                                const int2 si = st_i[warp][j + h];
+                                const float wy = __shfl_sync(0xffffffffu, w, 16 * h + W + lb);
+                                float tv[KC];
+                                {
+                                    const float s = __int_as_float(si.y);
+                                    float tm2 = 1.0f, tm1 = s;
+                                    for (int t = 0; t < term0 + KC; ++t) {
+                                        const float tn = t == 0 ? 1.0f : (t == 1 ? s : 2.0f * s * tm1 - tm2);
+                                        if (t >= 2) { tm2 = tm1; tm1 = tn; }
+                                        if (t >= term0) tv[t - term0] = tn;
+                                    }
+                                }
+                                const int base = si.x + lane_off;
+#pragma unroll
+                                for (int p = 0; p < PASSES; ++p) {
+                                    const float wx = __shfl_sync(0xffffffffu, w, 16 * h + wx_src[p]);
+                                    if (pass_on[p]) {
+                                        const float kv = wx * wy;
+                                        int* pl = tile + base + p * RPP * C::RS;
                                         const float ar = kv * sf.z, ai = kv * sf.w;
 #pragma unroll
                                         for (int t = 0; t < KC; ++t) {
@@ -272,31 +328,76 @@ __global__ void __launch_bounds__(kThreads) k_grid_fp32(
                     __syncwarp();
                 }
                 __syncthreads();
-                // flush the bounding box: checkerboard sign, clip to the grid, zero behind
+                // flush the bounding box: checkerboard sign, clip to the grid, zero behind. Warps
+                // take rows, lanes consecutive columns (coalesced reductions along a plane row);
+                // the row's plane pointer, parity and on-grid test are computed once per row.
                 const int br0 = bbox[0], br1 = min(bbox[1], C::R - 1);
                 const int bc0 = bbox[2], bc1 = min(bbox[3], C::R - 1);
                 if (br1 >= br0 && bc1 >= bc0) {
-                    const int bw = bc1 - bc0 + 1;
-                    const int ncell = (br1 - br0 + 1) * bw;
                     const long long o1 = g.gmin + (long long)t1 * T;
                     const long long o2 = g.gmin + (long long)t2 * T;
-                    for (int cidx = threadIdx.x; cidx < ncell; cidx += kThreads) {
-                        const int rr = br0 + cidx / bw, cc = bc0 + cidx % bw;
-                        const long long g1 = o1 + rr, g2 = o2 + cc;
-                        const bool on_grid = g1 <= g.gmax && g2 <= g.gmax;
-                        const float sgn = ((g1 + g2) & 1) ? -1.0f : 1.0f;
-                        const long long cell = (g1 - g.gmin) * g.G + (g2 - g.gmin);
+                    const long long row_lim = g.gmax - o1;  // rows rr <= row_lim lie on the grid
+                    const int col_lim = (int)min((long long)bc1, g.gmax - o2);
+                    const long long plane0 = (long long)(slab - slab_lo) * sp.K + term0;
+                    if constexpr (C::RS % 4 == 0) {
+                        // four cells per lane: 16-byte shared loads and stores, 16-byte reductions
+                        // of two interleaved complex cells where the plane row allows
+                        const int q0 = bc0 >> 2, nq = (bc1 >> 2) - q0 + 1;
+                        for (int rr = br0 + warp; rr <= br1; rr += kWarps) {
+                            const bool row_on = rr <= row_lim;
+                            const long long g1 = o1 + rr;
+                            const long long rbase = plane0 * GG + (g1 - g.gmin) * g.G + (o2 - g.gmin);
+                            float2* prow = planes + rbase;
+                            // cc is a multiple of 4, so the sign of cell cc + j is s0 for even j
+                            const float s0 = ((g1 + o2) & 1) ? -inv_scale : inv_scale;
+                            int* trow = tile + rr * C::RS;
+                            for (int gi = lane; gi < nq; gi += 32) {
+                                const int cc = (q0 + gi) * 4;
 #pragma unroll
-                        for (int t = 0; t < KC; ++t) {
-                            int* pl = tile + (size_t)t * 2 * C::PLANE + rr * C::RS + cc;
-                            const int ire = pl[0], iim = pl[C::PLANE];
-                            if (on_grid && (ire | iim)) {
-                                const long long plane = (long long)(slab - slab_lo) * sp.K + term0 + t;
-                                const float s = sgn * inv_scale;
-                                red_add_v2(planes + plane * GG + cell, s * (float)ire, s * (float)iim);
+                                for (int t = 0; t < KC; ++t) {
+                                    int* pl = trow + (size_t)t * 2 * C::PLANE + cc;
+                                    const int4 a = *reinterpret_cast<int4*>(pl);
+                                    const int4 b = *reinterpret_cast<int4*>(pl + C::PLANE);
+                                    *reinterpret_cast<int4*>(pl) = make_int4(0, 0, 0, 0);
+                                    *reinterpret_cast<int4*>(pl + C::PLANE) = make_int4(0, 0, 0, 0);
+                                    if (!row_on || !(a.x | a.y | a.z | a.w | b.x | b.y | b.z | b.w)) continue;
+                                    const float r0 = s0 * (float)a.x, i0 = s0 * (float)b.x;
+                                    const float r1 = -s0 * (float)a.y, i1 = -s0 * (float)b.y;
+                                    const float r2 = s0 * (float)a.z, i2 = s0 * (float)b.z;
+                                    const float r3 = -s0 * (float)a.w, i3 = -s0 * (float)b.w;
+                                    float2* p = prow + (long long)t * GG + cc;
+                                    if (cc + 3 <= col_lim && ((rbase + (long long)t * GG) & 1) == 0) {
+                                        red_add_v4(p, r0, i0, r1, i1);
+                                        red_add_v4(p + 2, r2, i2, r3, i3);
+                                    } else {
+                                        if (cc <= col_lim) red_add_v2(p, r0, i0);
+                                        if (cc + 1 <= col_lim) red_add_v2(p + 1, r1, i1);
+                                        if (cc + 2 <= col_lim) red_add_v2(p + 2, r2, i2);
+                                        if (cc + 3 <= col_lim) red_add_v2(p + 3, r3, i3);
+                                    }
+                                }
                             }
-                            pl[0] = 0;
-                            pl[C::PLANE] = 0;
+                        }
+                    } else {
+                        for (int rr = br0 + warp; rr <= br1; rr += kWarps) {
+                            const bool row_on = rr <= row_lim;
+                            const long long g1 = o1 + rr;
+                            float2* prow = planes + plane0 * GG + (g1 - g.gmin) * g.G + (o2 - g.gmin);
+                            const int par = (int)((g1 + o2) & 1);
+                            int* trow = tile + rr * C::RS;
+                            for (int cc = bc0 + lane; cc <= bc1; cc += 32) {
+                                const bool on = row_on && cc <= col_lim;
+                                const float s = ((par ^ cc) & 1) ? -inv_scale : inv_scale;
+#pragma unroll
+                                for (int t = 0; t < KC; ++t) {
+                                    int* pl = trow + (size_t)t * 2 * C::PLANE + cc;
+                                    const int ire = pl[0], iim = pl[C::PLANE];
+                                    if (on && (ire | iim))
+                                        red_add_v2(prow + (long long)t * GG + cc, s * (float)ire, s * (float)iim);
+                                    pl[0] = 0;
+                                    pl[C::PLANE] = 0;
+                                }
+                            }
                         }
                     }
                 }
@@ -323,9 +424,9 @@ int launch_variant(const SampleRec* d_rec, const float* d_rec_s, const unsigned 
         configured = true;
     }
     int per_sm = 0;
-    SVDI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, C::SMEM));
+    SVDI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::NT, C::SMEM));
     if (per_sm < 1) per_sm = 1;
-    kern<<<sm_count * per_sm, kThreads, C::SMEM, st>>>(d_rec, d_rec_s, d_offsets, key_lo, key_hi, slab_lo,
+    kern<<<sm_count * per_sm, C::NT, C::SMEM, st>>>(d_rec, d_rec_s, d_offsets, key_lo, key_hi, slab_lo,
                                                         g, sp, poly, d_planes, term0, chunk);
     SVDI_LAUNCHED();
     return SVDI_OK;
