@@ -72,7 +72,8 @@ __global__ void __launch_bounds__(kThreads) k_histogram(SampleSource src, GridGe
 __global__ void __launch_bounds__(1024) k_scan(const unsigned int* __restrict__ counts, int n_keys,
                                               unsigned int* __restrict__ offsets,
                                               unsigned int* __restrict__ cursor,
-                                              unsigned int* __restrict__ kb_offsets, int kb_size) {
+                                              unsigned int* __restrict__ kb_offsets, int kb_size,
+                                              unsigned int* __restrict__ chunk_key, int chunk_size) {
     __shared__ unsigned int part[1024];
     __shared__ unsigned int kpart[1024];
     const int t = threadIdx.x;
@@ -95,11 +96,19 @@ __global__ void __launch_bounds__(1024) k_scan(const unsigned int* __restrict__ 
         kpart[t] += kv;
         __syncthreads();
     }
+    const unsigned int total = part[1023];
+    const unsigned int n_chunks = chunk_key ? (total + chunk_size - 1) / chunk_size : 0u;
+    for (unsigned int ch = t; ch < n_chunks; ch += 1024) chunk_key[ch] = 0u;
+    __syncthreads();
     unsigned int run = part[t] - s, krun = kpart[t] - ks;
     for (int k = b; k < e; ++k) {
         const unsigned int c = counts[k];
         offsets[k] = run;
         cursor[k] = run;
+        if (chunk_key && c) {  // marks the first chunk that starts inside this key's records
+            const unsigned int ch = (run + chunk_size - 1) / chunk_size;
+            if ((unsigned long long)ch * chunk_size < (unsigned long long)run + c) chunk_key[ch] = (unsigned int)k;
+        }
         run += c;
         if (kb_offsets) {
             kb_offsets[k] = krun;
@@ -110,13 +119,35 @@ __global__ void __launch_bounds__(1024) k_scan(const unsigned int* __restrict__ 
         offsets[n_keys] = part[1023];
         if (kb_offsets) kb_offsets[n_keys] = kpart[1023];
     }
+    if (!chunk_key) return;
+    // chunks without a mark start inside the key of the last mark before them: a running maximum
+    // (keys increase along the records) over contiguous chunk ranges, then across threads
+    __syncthreads();
+    const unsigned int cper = (n_chunks + 1023) / 1024;
+    const unsigned int cb = t * cper, ce = min(n_chunks, cb + cper);
+    unsigned int m = 0;
+    for (unsigned int ch = cb; ch < ce; ++ch) m = max(m, chunk_key[ch]);
+    part[t] = m;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        const unsigned int v = (t >= off) ? part[t - off] : 0u;
+        __syncthreads();
+        part[t] = max(part[t], v);
+        __syncthreads();
+    }
+    m = t ? part[t - 1] : 0u;
+    for (unsigned int ch = cb; ch < ce; ++ch) {
+        m = max(m, chunk_key[ch]);
+        chunk_key[ch] = m;
+    }
 }
 
 // Scatter: block-aggregated reservation of output ranges per key, then 16-byte record writes.
 __global__ void __launch_bounds__(kThreads) k_scatter(SampleSource src, GridGeom g, SlabParams sp,
                                                      unsigned int* __restrict__ cursor, int n_keys,
                                                      SampleRec* __restrict__ rec, float* __restrict__ rec_s,
-                                                     unsigned int* __restrict__ vmax) {
+                                                     unsigned int* __restrict__ vmax,
+                                                     unsigned int* __restrict__ keymax) {
     extern __shared__ unsigned int sh[];  // [n_keys] counts, then [n_keys] bases
     unsigned int* cnt = sh;
     unsigned int* base = sh + n_keys;
@@ -167,7 +198,9 @@ __global__ void __launch_bounds__(kThreads) k_scatter(SampleSource src, GridGeom
             r.vim = __fmul_rn(src.vi[idx], src.inv_det);
             rec[pos] = r;
             if (rec_s) rec_s[pos] = kr[i].s;
-            vm = fmaxf(vm, fmaxf(fabsf(r.vre), fabsf(r.vim)));
+            const float m = fmaxf(fabsf(r.vre), fabsf(r.vim));
+            vm = fmaxf(vm, m);
+            if (keymax && m > 0.0f) atomicMax(&keymax[key], __float_as_uint(m));
         }
         if (use_smem) __syncthreads();
     }
@@ -249,7 +282,8 @@ constexpr int kVisPitch = kUnitRows + 1;   // float2 pitch of a staged channel (
 __global__ void __launch_bounds__(kThreads) k_scatter_sep(SampleSource src, SepMap m, GridGeom g, SlabParams sp,
                                                          unsigned int* __restrict__ cursor,
                                                          SampleRec* __restrict__ rec, float* __restrict__ rec_s,
-                                                         unsigned int* __restrict__ vmax) {
+                                                         unsigned int* __restrict__ vmax,
+                                                         unsigned int* __restrict__ keymax) {
     __shared__ float2 stage[kThreads / 32][32 * kVisPitch];
     float2* my = stage[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
@@ -303,7 +337,12 @@ __global__ void __launch_bounds__(kThreads) k_scatter_sep(SampleSource src, SepM
                 r.vim = __fmul_rn(v.y, src.inv_det);
                 rec[pos] = r;
                 if (rec_s) rec_s[pos] = kr.s;
-                vm = fmaxf(vm, fmaxf(fabsf(r.vre), fabsf(r.vim)));
+                const float m = fmaxf(fabsf(r.vre), fabsf(r.vim));
+                vm = fmaxf(vm, m);
+                if (keymax) {  // the group's maximum, one atomic per group
+                    const unsigned int gm = __reduce_max_sync(peers, __float_as_uint(m));
+                    if (lane == leader && gm) atomicMax(&keymax[key], gm);
+                }
             }
         }
     }
@@ -364,22 +403,23 @@ int launch_histogram(const SampleSource& src, const GridGeom& g, const SlabParam
 }
 
 int launch_scan(const unsigned int* d_counts, int n_keys, unsigned int* d_offsets,
-                unsigned int* d_cursor, cudaStream_t st, unsigned int* d_kb_offsets, int kb_size) {
-    k_scan<<<1, 1024, 0, st>>>(d_counts, n_keys, d_offsets, d_cursor, d_kb_offsets, kb_size);
+                unsigned int* d_cursor, cudaStream_t st, unsigned int* d_kb_offsets, int kb_size,
+                unsigned int* d_chunk_key, int chunk_size) {
+    k_scan<<<1, 1024, 0, st>>>(d_counts, n_keys, d_offsets, d_cursor, d_kb_offsets, kb_size, d_chunk_key, chunk_size);
     SVDI_LAUNCHED();
     return SVDI_OK;
 }
 
 int launch_scatter(const SampleSource& src, const GridGeom& g, const SlabParams& sp,
                    unsigned int* d_cursor, int n_keys, SampleRec* d_rec, float* d_rec_s,
-                   unsigned int* d_vmax, cudaStream_t st) {
+                   unsigned int* d_vmax, cudaStream_t st, unsigned int* d_keymax) {
     if (use_sep(src)) {
         const SepMap m = sep_map(src);
         const long long units = (long long)m.nrt * m.nch;
         long long blocks = (units + kThreads / 32 - 1) / (kThreads / 32);
         if (blocks > 148 * 8) blocks = 148 * 8;
         if (blocks < 1) blocks = 1;
-        k_scatter_sep<<<(int)blocks, kThreads, 0, st>>>(src, m, g, sp, d_cursor, d_rec, d_rec_s, d_vmax);
+        k_scatter_sep<<<(int)blocks, kThreads, 0, st>>>(src, m, g, sp, d_cursor, d_rec, d_rec_s, d_vmax, d_keymax);
         SVDI_LAUNCHED();
         return SVDI_OK;
     }
@@ -392,7 +432,7 @@ int launch_scatter(const SampleSource& src, const GridGeom& g, const SlabParams&
     long long blocks = (src.n + kChunk - 1) / kChunk;
     if (blocks > 148 * 16) blocks = 148 * 16;
     if (blocks < 1) blocks = 1;
-    k_scatter<<<(int)blocks, kThreads, smem, st>>>(src, g, sp, d_cursor, n_keys, d_rec, d_rec_s, d_vmax);
+    k_scatter<<<(int)blocks, kThreads, smem, st>>>(src, g, sp, d_cursor, n_keys, d_rec, d_rec_s, d_vmax, d_keymax);
     SVDI_LAUNCHED();
     return SVDI_OK;
 }

@@ -108,7 +108,7 @@ struct svdi_engine {
     svdi::DevBuf in_bin, in_vin;
     // intermediates
     svdi::DevBuf vr, vi, q, s, vin64, vin32, stats, partial, counts, offsets, cursor, dropped, rec,
-        rec_s, planes, corr, image, cheb_err, bin_out, grid_keep, tc_status, kb_offsets, acc;
+        rec_s, planes, corr, image, cheb_err, bin_out, grid_keep, tc_status, kb_offsets, acc, chunk_key, keymax;
     size_t sz_vr = 0, sz_q = 0, sz_s = 0, sz_off = 0, sz_rec = 0, sz_rec_s = 0, sz_grid = 0, sz_mom = 0;
     const float* cur_vr = nullptr;
     const float* cur_vi = nullptr;
@@ -540,10 +540,17 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     SVDI_CUDA(cudaMemsetAsync(e->dropped.p, 0, 8, st));
     SVDI_TRY(launch_histogram(src, g, sp, e->counts.as<unsigned int>(), n_keys,
                               e->dropped.as<unsigned long long>(), st));
-    if (use_tc) SVDI_TRY(e->kb_offsets.ensure((size_t)(n_keys + 1) * 4));
+    if (use_tc) {
+        SVDI_TRY(e->kb_offsets.ensure((size_t)(n_keys + 1) * 4));
+    } else {  // the FP32 gridder's chunk table and per-key maxima
+        SVDI_TRY(e->chunk_key.ensure(((size_t)std::max<long long>(n, 1) / kGridChunk + 2) * 4));
+        SVDI_TRY(e->keymax.ensure((size_t)n_keys * 4));
+        SVDI_CUDA(cudaMemsetAsync(e->keymax.p, 0, (size_t)n_keys * 4, st));
+    }
     SVDI_TRY(launch_scan(e->counts.as<unsigned int>(), n_keys, e->offsets.as<unsigned int>(),
                          e->cursor.as<unsigned int>(), st,
-                         use_tc ? e->kb_offsets.as<unsigned int>() : nullptr, kTcKBlock));
+                         use_tc ? e->kb_offsets.as<unsigned int>() : nullptr, kTcKBlock,
+                         use_tc ? nullptr : e->chunk_key.as<unsigned int>(), kGridChunk));
     // tensor-core gridder: [0] give-up status, [1] max |record value| (float bits) from the scatter
     if (use_tc) {
         SVDI_TRY(e->tc_status.ensure(4 * sizeof(unsigned int)));
@@ -552,7 +559,8 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     if (vis_ready) SVDI_CUDA(cudaStreamWaitEvent(st, vis_ready, 0));
     SVDI_TRY(launch_scatter(src, g, sp, e->cursor.as<unsigned int>(), n_keys, e->rec.as<SampleRec>(),
                             need_s ? e->rec_s.as<float>() : nullptr,
-                            use_tc ? e->tc_status.as<unsigned int>() + 1 : nullptr, st));
+                            use_tc ? e->tc_status.as<unsigned int>() + 1 : nullptr, st,
+                            use_tc ? nullptr : e->keymax.as<unsigned int>()));
     if (timed) SVDI_CUDA(cudaEventRecord(e->ev[2], st));
 
     // slab batches: grid -> FFT -> recombine
@@ -596,7 +604,8 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
                                     e->sm_count, st));
         } else {
             SVDI_TRY(launch_grid_fp32(e->rec.as<SampleRec>(), need_s ? e->rec_s.as<float>() : nullptr,
-                                      e->offsets.as<unsigned int>(), n_keys, s0 * tiles2, s1 * tiles2, s0, g,
+                                      e->offsets.as<unsigned int>(), e->chunk_key.as<unsigned int>(),
+                                      e->keymax.as<unsigned int>(), n_keys, s0 * tiles2, s1 * tiles2, s0, g,
                                       sp, e->poly, e->planes.as<float2>(), e->sm_count, st));
         }
         if (o.keep_grid && s0 == 0) {

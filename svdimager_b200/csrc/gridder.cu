@@ -89,13 +89,12 @@ struct TileCfg {
 template <int W, int T, int KC>
 __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
     const SampleRec* __restrict__ rec, const float* __restrict__ rec_s,
-    const unsigned int* __restrict__ offsets, int key_lo, int key_hi, int slab_lo, GridGeom g,
-    SlabParams sp, EsPoly poly, float2* __restrict__ planes, int term0, unsigned int chunk) {
+    const unsigned int* __restrict__ offsets, const unsigned int* __restrict__ chunk_key,
+    const unsigned int* __restrict__ keymax, int key_lo, int key_hi, int slab_lo, GridGeom g,
+    SlabParams sp, EsPoly poly, float2* __restrict__ planes, int term0) {
     using C = TileCfg<W, T, KC>;
     extern __shared__ int tile[];    // [KC][2][R][RS] 32-bit fixed-point accumulators
-    __shared__ unsigned int seg_max; // max |v| of the segment (float bits; non-negative)
     __shared__ int bbox[4];          // row min, row max, col min, col max
-    __shared__ int seg_key;
     // per-warp staging of the decoded batch: {u_x, u_y, vre, vim} and {fast-path base, s}
     constexpr int kThreads = C::NT, kWarps = C::NW;
     __shared__ float4 st_f[kWarps][33];  // 32 samples + the zero pad
@@ -133,50 +132,32 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
     }
     __syncthreads();
 
+    // chunks of kGridChunk records at absolute record positions (the first and last ones of the
+    // key range may be partial); the scan's table gives each chunk's first key
     const unsigned int rec_lo = offsets[key_lo], rec_hi = offsets[key_hi];
-    const unsigned int n_chunks = (rec_hi - rec_lo + chunk - 1) / chunk;
+    const unsigned int ch_lo = rec_lo / kGridChunk, ch_hi = (rec_hi + kGridChunk - 1) / kGridChunk;
     const long long GG = g.G * g.G;
     const int tiles2 = g.ntile * g.ntile2;
     const bool need_s = !(KC == 1 && term0 == 0);
 
-    for (unsigned int ch = blockIdx.x; ch < n_chunks; ch += gridDim.x) {
-        const unsigned int c_beg = rec_lo + ch * chunk;
-        const unsigned int c_end = min(rec_hi, c_beg + chunk);
-        if (threadIdx.x == 0) {  // last key in [key_lo, key_hi) with offsets[key] <= c_beg
-            int lo = key_lo, hi = key_hi;  // offsets[key_hi] = rec_hi > c_beg
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (offsets[mid] <= c_beg) lo = mid; else hi = mid;
-            }
-            seg_key = lo;
-        }
-        __syncthreads();
-        int key = seg_key;
+    for (unsigned int ch = ch_lo + blockIdx.x; ch < ch_hi; ch += gridDim.x) {
+        const unsigned int c_beg = max(rec_lo, ch * kGridChunk);
+        const unsigned int c_end = min(rec_hi, (ch + 1) * kGridChunk);
+        int key = max(key_lo, (int)chunk_key[ch]);
         while (key < key_hi && offsets[key] < c_end) {
             const unsigned int s_beg = max(c_beg, offsets[key]);
             const unsigned int s_end = min(c_end, offsets[key + 1]);
             if (s_beg < s_end) {
                 const int slab = key / tiles2;
                 const int t1 = (key / g.ntile2) % g.ntile, t2 = key % g.ntile2;
-                // Fixed-point scale of the segment: 0.999 * 2^(22 - e) with max|v| < 2^e, so every
-                // contribution (|psi psi T_n| <= 1 up to the polynomial's 1e-7) stays inside the
-                // exact-rounding range |x| < 2^22 and the <= 512 samples of a segment cannot
-                // overflow a 32-bit cell (512 * 2^22 = 2^31).
-                if (threadIdx.x == 0) seg_max = 0u;
-                __syncthreads();
-                {
-                    float m = 0.0f;
-                    for (unsigned int k = s_beg + threadIdx.x; k < s_end; k += kThreads) {
-                        const SampleRec q = rec[k];
-                        m = fmaxf(m, fmaxf(fabsf(q.vre), fabsf(q.vim)));
-                    }
-                    const unsigned int mb = __reduce_max_sync(0xffffffffu, __float_as_uint(m));
-                    if (lane == 0) atomicMax(&seg_max, mb);
-                }
-                __syncthreads();
+                // Fixed-point scale of the segment: 0.999 * 2^(22 - e) with max|v| < 2^e for the
+                // key's largest record (the scatter's per-key maximum), so every contribution
+                // (|psi psi T_n| <= 1 up to the polynomial's 1e-7) stays inside the exact-rounding
+                // range |x| < 2^22 and the <= 512 samples of a segment cannot overflow a 32-bit
+                // cell (512 * 2^22 = 2^31).
                 float scale = 0.0f, inv_scale = 0.0f;
                 {
-                    const float vmax = __uint_as_float(seg_max);
+                    const float vmax = __uint_as_float(keymax[key]);
                     if (vmax > 0.0f && vmax < 3.0e38f) {
                         int ex;
                         frexpf(vmax, &ex);  // vmax = f 2^ex, f in [0.5, 1)
@@ -413,9 +394,9 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
 }
 template <int W, int T, int KC>
 int launch_variant(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d_offsets,
+                   const unsigned int* d_chunk_key, const unsigned int* d_keymax,
                    int key_lo, int key_hi, int slab_lo, const GridGeom& g, const SlabParams& sp,
-                   const EsPoly& poly, float2* d_planes, int term0, unsigned int chunk, int sm_count,
-                   cudaStream_t st) {
+                   const EsPoly& poly, float2* d_planes, int term0, int sm_count, cudaStream_t st) {
     using C = TileCfg<W, T, KC>;
     auto kern = k_grid_fp32<W, T, KC>;
     static bool configured = false;  // per instantiation
@@ -426,34 +407,35 @@ int launch_variant(const SampleRec* d_rec, const float* d_rec_s, const unsigned 
     int per_sm = 0;
     SVDI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::NT, C::SMEM));
     if (per_sm < 1) per_sm = 1;
-    kern<<<sm_count * per_sm, C::NT, C::SMEM, st>>>(d_rec, d_rec_s, d_offsets, key_lo, key_hi, slab_lo,
-                                                        g, sp, poly, d_planes, term0, chunk);
+    kern<<<sm_count * per_sm, C::NT, C::SMEM, st>>>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, key_lo,
+                                                     key_hi, slab_lo, g, sp, poly, d_planes, term0);
     SVDI_LAUNCHED();
     return SVDI_OK;
 }
 
 template <int W>
-int launch_w(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d_offsets, int key_lo,
-             int key_hi, int slab_lo, const GridGeom& g, const SlabParams& sp, const EsPoly& poly,
-             float2* d_planes, int sm_count, cudaStream_t st) {
-    const unsigned int chunk = 512;  // <= 512 samples per tile segment: no 32-bit overflow
+int launch_w(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d_offsets,
+             const unsigned int* d_chunk_key, const unsigned int* d_keymax, int key_lo, int key_hi,
+             int slab_lo, const GridGeom& g, const SlabParams& sp, const EsPoly& poly, float2* d_planes,
+             int sm_count, cudaStream_t st) {
+    static_assert(kGridChunk <= 512, "<= 512 samples per tile segment: no 32-bit overflow");
     if (g.T == 64) {
         for (int t0 = 0; t0 < sp.K; ++t0)
-            SVDI_TRY((launch_variant<W, 64, 1>(d_rec, d_rec_s, d_offsets, key_lo, key_hi, slab_lo, g, sp,
-                                               poly, d_planes, t0, chunk, sm_count, st)));
+            SVDI_TRY((launch_variant<W, 64, 1>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, key_lo, key_hi,
+                                               slab_lo, g, sp, poly, d_planes, t0, sm_count, st)));
         return SVDI_OK;
     }
     if (g.T == 32) {
         int t0 = 0;
         for (; t0 + 8 <= sp.K; t0 += 8)
-            SVDI_TRY((launch_variant<W, 32, 8>(d_rec, d_rec_s, d_offsets, key_lo, key_hi, slab_lo, g, sp,
-                                               poly, d_planes, t0, chunk, sm_count, st)));
+            SVDI_TRY((launch_variant<W, 32, 8>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, key_lo, key_hi,
+                                               slab_lo, g, sp, poly, d_planes, t0, sm_count, st)));
         for (; t0 + 4 <= sp.K; t0 += 4)
-            SVDI_TRY((launch_variant<W, 32, 4>(d_rec, d_rec_s, d_offsets, key_lo, key_hi, slab_lo, g, sp,
-                                               poly, d_planes, t0, chunk, sm_count, st)));
+            SVDI_TRY((launch_variant<W, 32, 4>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, key_lo, key_hi,
+                                               slab_lo, g, sp, poly, d_planes, t0, sm_count, st)));
         for (; t0 < sp.K; ++t0)
-            SVDI_TRY((launch_variant<W, 32, 1>(d_rec, d_rec_s, d_offsets, key_lo, key_hi, slab_lo, g, sp,
-                                               poly, d_planes, t0, chunk, sm_count, st)));
+            SVDI_TRY((launch_variant<W, 32, 1>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, key_lo, key_hi,
+                                               slab_lo, g, sp, poly, d_planes, t0, sm_count, st)));
         return SVDI_OK;
     }
     set_error("gridder: tile size must be 32 or 64");
@@ -463,18 +445,19 @@ int launch_w(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d
 }  // namespace
 
 int launch_grid_fp32(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d_offsets,
+                     const unsigned int* d_chunk_key, const unsigned int* d_keymax,
                      int n_keys, int key_lo, int key_hi, int slab_lo, const GridGeom& g,
                      const SlabParams& sp, const EsPoly& poly, float2* d_planes, int sm_count,
                      cudaStream_t st) {
-    if (key_lo < 0 || key_hi > n_keys || key_lo >= key_hi) {
-        set_error("gridder: bad key range");
+    if (key_lo < 0 || key_hi > n_keys || key_lo >= key_hi || !d_chunk_key || !d_keymax) {
+        set_error("gridder: bad key range or missing chunk table");
         return SVDI_ERR_INTERNAL;
     }
     switch (g.W) {
-        case 6: return launch_w<6>(d_rec, d_rec_s, d_offsets, key_lo, key_hi, slab_lo, g, sp, poly, d_planes, sm_count, st);
-        case 8: return launch_w<8>(d_rec, d_rec_s, d_offsets, key_lo, key_hi, slab_lo, g, sp, poly, d_planes, sm_count, st);
-        case 10: return launch_w<10>(d_rec, d_rec_s, d_offsets, key_lo, key_hi, slab_lo, g, sp, poly, d_planes, sm_count, st);
-        case 12: return launch_w<12>(d_rec, d_rec_s, d_offsets, key_lo, key_hi, slab_lo, g, sp, poly, d_planes, sm_count, st);
+        case 6: return launch_w<6>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, key_lo, key_hi, slab_lo, g, sp, poly, d_planes, sm_count, st);
+        case 8: return launch_w<8>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, key_lo, key_hi, slab_lo, g, sp, poly, d_planes, sm_count, st);
+        case 10: return launch_w<10>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, key_lo, key_hi, slab_lo, g, sp, poly, d_planes, sm_count, st);
+        case 12: return launch_w<12>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, key_lo, key_hi, slab_lo, g, sp, poly, d_planes, sm_count, st);
         default:
             set_error("gridder: ES support must be one of 6, 8, 10, 12");
             return SVDI_ERR_UNSUPPORTED;

@@ -131,14 +131,17 @@ struct SampleSource {
 int launch_histogram(const SampleSource& src, const GridGeom& g, const SlabParams& sp,
                      unsigned int* d_counts, int n_keys, unsigned long long* d_dropped,
                      cudaStream_t st);
-// d_kb_offsets (optional): exclusive scan of ceil(count / kb_size) per key, n_keys + 1 entries
+// d_kb_offsets (optional): exclusive scan of ceil(count / kb_size) per key, n_keys + 1 entries.
+// d_chunk_key (optional): for every chunk c of chunk_size records, the last key whose records
+// start at or before c * chunk_size (ceil(total / chunk_size) entries, total = offsets[n_keys]).
 int launch_scan(const unsigned int* d_counts, int n_keys, unsigned int* d_offsets,
                 unsigned int* d_cursor, cudaStream_t st, unsigned int* d_kb_offsets = nullptr,
-                int kb_size = 32);
+                int kb_size = 32, unsigned int* d_chunk_key = nullptr, int chunk_size = 512);
 // d_vmax (optional, zeroed by the caller): receives max(|vre|, |vim|) over the records as float bits
+// d_keymax (optional, n_keys entries zeroed by the caller): the same maximum per key
 int launch_scatter(const SampleSource& src, const GridGeom& g, const SlabParams& sp,
                    unsigned int* d_cursor, int n_keys, SampleRec* d_rec, float* d_rec_s,
-                   unsigned int* d_vmax, cudaStream_t st);
+                   unsigned int* d_vmax, cudaStream_t st, unsigned int* d_keymax = nullptr);
 
 // gridder_tc.cu: split-precision tcgen05 gridder (one moment plane, support <= 8)
 constexpr int kTcTileRows = 56;    // tile rows: footprint origins; 64-row accumulator with halo
@@ -157,7 +160,11 @@ int launch_grid_tc(const SampleRec* d_rec, const unsigned int* d_offsets, const 
                    cudaStream_t st);
 
 // gridder.cu
+// d_chunk_key, d_keymax: the scan's chunk table (chunks of kGridChunk records) and the scatter's
+// per-key max |value|
+constexpr int kGridChunk = 512;
 int launch_grid_fp32(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d_offsets,
+                     const unsigned int* d_chunk_key, const unsigned int* d_keymax,
                      int n_keys, int key_lo, int key_hi, int slab_lo, const GridGeom& g,
                      const SlabParams& sp, const EsPoly& poly, float2* d_planes, int sm_count,
                      cudaStream_t st);
