@@ -31,7 +31,9 @@ constexpr int kSmemKeyLimit = 24576;                // keys aggregated in shared
 // Per-block shared-memory histogram (warp-aggregated), flushed once per block.
 __global__ void __launch_bounds__(kThreads) k_histogram(SampleSource src, GridGeom g, SlabParams sp,
                                                        unsigned int* __restrict__ counts, int n_keys,
-                                                       unsigned long long* __restrict__ dropped) {
+                                                       unsigned long long* __restrict__ dropped,
+                                                       const DevPlan* __restrict__ plan) {
+    if (plan) sp = plan->sp;
     extern __shared__ unsigned int sh[];
     const bool use_smem = n_keys <= kSmemKeyLimit;
     if (use_smem) {
@@ -147,7 +149,12 @@ __global__ void __launch_bounds__(kThreads) k_scatter(SampleSource src, GridGeom
                                                      unsigned int* __restrict__ cursor, int n_keys,
                                                      SampleRec* __restrict__ rec, float* __restrict__ rec_s,
                                                      unsigned int* __restrict__ vmax,
-                                                     unsigned int* __restrict__ keymax) {
+                                                     unsigned int* __restrict__ keymax,
+                                                     const DevPlan* __restrict__ plan) {
+    if (plan) {
+        sp = plan->sp;
+        src.inv_det = plan->inv_det;
+    }
     extern __shared__ unsigned int sh[];  // [n_keys] counts, then [n_keys] bases
     unsigned int* cnt = sh;
     unsigned int* base = sh + n_keys;
@@ -232,7 +239,9 @@ __device__ inline void unit_of(long long u, const SepMap& m, int& rt, int& ch) {
 
 __global__ void __launch_bounds__(kThreads) k_histogram_sep(SampleSource src, SepMap m, GridGeom g, SlabParams sp,
                                                            unsigned int* __restrict__ counts, int n_keys,
-                                                           unsigned long long* __restrict__ dropped) {
+                                                           unsigned long long* __restrict__ dropped,
+                                                           const DevPlan* __restrict__ plan) {
+    if (plan) sp = plan->sp;
     extern __shared__ unsigned int sh[];
     const bool use_smem = n_keys <= kSmemKeyLimit;
     if (use_smem) {
@@ -283,7 +292,12 @@ __global__ void __launch_bounds__(kThreads) k_scatter_sep(SampleSource src, SepM
                                                          unsigned int* __restrict__ cursor,
                                                          SampleRec* __restrict__ rec, float* __restrict__ rec_s,
                                                          unsigned int* __restrict__ vmax,
-                                                         unsigned int* __restrict__ keymax) {
+                                                         unsigned int* __restrict__ keymax,
+                                                         const DevPlan* __restrict__ plan) {
+    if (plan) {
+        sp = plan->sp;
+        src.inv_det = plan->inv_det;
+    }
     __shared__ float2 stage[kThreads / 32][32 * kVisPitch];
     float2* my = stage[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
@@ -372,7 +386,7 @@ bool use_sep(const SampleSource& src) {
 
 int launch_histogram(const SampleSource& src, const GridGeom& g, const SlabParams& sp,
                      unsigned int* d_counts, int n_keys, unsigned long long* d_dropped,
-                     cudaStream_t st) {
+                     cudaStream_t st, const DevPlan* d_plan) {
     const size_t smem = n_keys <= kSmemKeyLimit ? (size_t)n_keys * 4 : 0;
     static size_t configured = 48 * 1024;  // the attribute is raised once, to the largest size used
     if (smem > configured) {
@@ -390,14 +404,14 @@ int launch_histogram(const SampleSource& src, const GridGeom& g, const SlabParam
         long long blocks = (units + kThreads / 32 - 1) / (kThreads / 32);
         if (blocks > 148 * 4) blocks = 148 * 4;   // a few units per warp: the shared histogram is flushed once
         if (blocks < 1) blocks = 1;
-        k_histogram_sep<<<(int)blocks, kThreads, smem, st>>>(src, m, g, sp, d_counts, n_keys, d_dropped);
+        k_histogram_sep<<<(int)blocks, kThreads, smem, st>>>(src, m, g, sp, d_counts, n_keys, d_dropped, d_plan);
         SVDI_LAUNCHED();
         return SVDI_OK;
     }
     long long blocks = (src.n + kThreads - 1) / kThreads;
     if (blocks > 148 * 8) blocks = 148 * 8;
     if (blocks < 1) blocks = 1;
-    k_histogram<<<(int)blocks, kThreads, smem, st>>>(src, g, sp, d_counts, n_keys, d_dropped);
+    k_histogram<<<(int)blocks, kThreads, smem, st>>>(src, g, sp, d_counts, n_keys, d_dropped, d_plan);
     SVDI_LAUNCHED();
     return SVDI_OK;
 }
@@ -412,14 +426,15 @@ int launch_scan(const unsigned int* d_counts, int n_keys, unsigned int* d_offset
 
 int launch_scatter(const SampleSource& src, const GridGeom& g, const SlabParams& sp,
                    unsigned int* d_cursor, int n_keys, SampleRec* d_rec, float* d_rec_s,
-                   unsigned int* d_vmax, cudaStream_t st, unsigned int* d_keymax) {
+                   unsigned int* d_vmax, cudaStream_t st, unsigned int* d_keymax, const DevPlan* d_plan) {
     if (use_sep(src)) {
         const SepMap m = sep_map(src);
         const long long units = (long long)m.nrt * m.nch;
         long long blocks = (units + kThreads / 32 - 1) / (kThreads / 32);
         if (blocks > 148 * 8) blocks = 148 * 8;
         if (blocks < 1) blocks = 1;
-        k_scatter_sep<<<(int)blocks, kThreads, 0, st>>>(src, m, g, sp, d_cursor, d_rec, d_rec_s, d_vmax, d_keymax);
+        k_scatter_sep<<<(int)blocks, kThreads, 0, st>>>(src, m, g, sp, d_cursor, d_rec, d_rec_s, d_vmax, d_keymax,
+                                                        d_plan);
         SVDI_LAUNCHED();
         return SVDI_OK;
     }
@@ -432,7 +447,8 @@ int launch_scatter(const SampleSource& src, const GridGeom& g, const SlabParams&
     long long blocks = (src.n + kChunk - 1) / kChunk;
     if (blocks > 148 * 16) blocks = 148 * 16;
     if (blocks < 1) blocks = 1;
-    k_scatter<<<(int)blocks, kThreads, smem, st>>>(src, g, sp, d_cursor, n_keys, d_rec, d_rec_s, d_vmax, d_keymax);
+    k_scatter<<<(int)blocks, kThreads, smem, st>>>(src, g, sp, d_cursor, n_keys, d_rec, d_rec_s, d_vmax, d_keymax,
+                                                   d_plan);
     SVDI_LAUNCHED();
     return SVDI_OK;
 }

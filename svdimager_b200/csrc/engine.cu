@@ -108,13 +108,23 @@ struct svdi_engine {
     svdi::DevBuf in_bin, in_vin;
     // intermediates
     svdi::DevBuf vr, vi, q, s, vin64, vin32, stats, partial, counts, offsets, cursor, dropped, rec,
-        rec_s, planes, corr, image, cheb_err, bin_out, grid_keep, tc_status, kb_offsets, acc, chunk_key, keymax;
+        rec_s, planes, corr, image, cheb_err, bin_out, grid_keep, tc_status, kb_offsets, acc, chunk_key, keymax,
+        plan_buf;
     size_t sz_vr = 0, sz_q = 0, sz_s = 0, sz_off = 0, sz_rec = 0, sz_rec_s = 0, sz_grid = 0, sz_mom = 0;
     const float* cur_vr = nullptr;
     const float* cur_vi = nullptr;
     const double* cur_q = nullptr;
     const double* cur_s = nullptr;
-    double* h_stats = nullptr;  // pinned
+    double* h_stats = nullptr;  // pinned: ST_COUNT statistics, then the 9 entries of Vin
+    // Speculative plan: a call with the same shape as the last one launches its gridding with the
+    // last call's slab and Chebyshev counts (the slab geometry itself computed on the device from
+    // this call's statistics) and checks the counts against its own host decision afterwards,
+    // imaging again in the rare case they differ. The device never waits for the host decision.
+    bool spec_valid = false, spec_archive = false, spec_bin = false;
+    long long spec_N = 0, spec_n = 0, spec_R = 0;
+    float spec_cell = 0.0f;
+    svdi::SlabParams spec_sp{};
+    cudaEvent_t ev_stats = nullptr;
     // Completion of the last call, read lazily (finish_pending): the device-API call returns once
     // its work is enqueued, so that the host can enqueue the next snapshot meanwhile.
     unsigned long long* h_ndrop = nullptr;  // pinned: dropped-sample count of the last call
@@ -150,6 +160,7 @@ struct svdi_engine {
         if (h_stats) cudaFreeHost(h_stats);
         if (h_ndrop) cudaFreeHost(h_ndrop);
         if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_stats) cudaEventDestroy(ev_stats);
         if (ev_vis) cudaEventDestroy(ev_vis);
         if (side) cudaStreamDestroy(side);
         if (stream && own_stream) cudaStreamDestroy(stream);
@@ -172,7 +183,8 @@ int engine_init(svdi_engine* e, const svdi_options* opt) {
     SVDI_CUDA(cudaStreamCreateWithPriority(&e->side, cudaStreamNonBlocking, prio_low));
     SVDI_CUDA(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
     SVDI_CUDA(cudaEventCreateWithFlags(&e->ev_vis, cudaEventDisableTiming));
-    SVDI_CUDA(cudaMallocHost(&e->h_stats, ST_COUNT * sizeof(double)));
+    SVDI_CUDA(cudaEventCreateWithFlags(&e->ev_stats, cudaEventDisableTiming));
+    SVDI_CUDA(cudaMallocHost(&e->h_stats, (ST_COUNT + 9) * sizeof(double)));
     SVDI_CUDA(cudaMallocHost(&e->h_ndrop, 2 * sizeof(unsigned long long)));
     for (auto& ev : e->ev) SVDI_CUDA(cudaEventCreate(&ev));
     return SVDI_OK;
@@ -242,17 +254,9 @@ int choose_slabs(svdi_engine* e, bool archive, double r3min, double r3max, doubl
     const svdi_options& o = e->opt;
     const double half_range = std::max(0.5 * (r3max - r3min), 1.0e-6);
     alpha_max = 2.0 * kPi * mt3 * half_range;
-    if (archive) {  // archive/FIPkernels.cu:327-366: one slab centred on the range
-        const double centre = 0.5 * (r3max + r3min);
-        sp.nslab = 1;
-        sp.r3_min = centre - half_range;
-        sp.slab_width = 2.0 * half_range;
-        sp.slab_half = half_range;
-        sp.inv_half = 1.0 / half_range;
-        slab_alpha = alpha_max;
-    } else {  // SVDIntegratedImager.cu:973-991
+    int nslab = 1;  // archive/FIPkernels.cu:327-366: one slab centred on the range
+    if (!archive) {  // SVDIntegratedImager.cu:973-991
         const double r3_range = std::max(r3max - r3min, 2.0e-6);
-        int nslab;
         if (o.k_rule == SVDI_KRULE_TARGET && o.target_alpha <= 0) {
             // minimise the number of moment planes nslab * K(alpha_slab) at the error target
             int best_n = 1, best_p = 1 << 30;
@@ -271,13 +275,9 @@ int choose_slabs(svdi_engine* e, bool archive, double r3min, double r3max, doubl
             nslab = (int)std::ceil(std::max(alpha_max, 0.0) / read_target_alpha(o));
             if (nslab < 1) nslab = 1;
         }
-        sp.nslab = nslab;
-        sp.r3_min = r3min;
-        sp.slab_width = r3_range / nslab;
-        sp.slab_half = std::max(0.5 * sp.slab_width, 1.0e-6);
-        sp.inv_half = 1.0 / sp.slab_half;
-        slab_alpha = 2.0 * kPi * mt3 * sp.slab_half;
     }
+    slab_params_for(archive, nslab, 0, r3min, r3max, sp);
+    slab_alpha = 2.0 * kPi * mt3 * sp.slab_half;
     int K = kChebMaxMoments;
     std::vector<double> err;
     switch (o.k_rule) {
@@ -449,11 +449,28 @@ int finish_pending(svdi_engine* e) {
     return SVDI_OK;
 }
 
+// The host decision from the statistics and Vin read back into h_stats: 1 / |det|, w range, slab
+// and Chebyshev configuration.
+int host_decision(svdi_engine* e, bool archive, SampleSource& src, SlabParams& sp, double& alpha_max,
+                  double& slab_alpha, double& r3min, double& r3max, double& mt3) {
+    r3min = e->h_stats[ST_R3_MIN];
+    r3max = e->h_stats[ST_R3_MAX];
+    mt3 = e->h_stats[ST_MAX_T3];
+    std::memcpy(e->last.vin, e->h_stats + ST_COUNT, 9 * sizeof(double));
+    const double det = basis_det(e->last.vin);
+    if (!(det > 0.0) || !std::isfinite(det)) {
+        set_error("degenerate basis: |V00 V11 - V01 V10| is zero");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    src.inv_det = (float)(1.0 / det);
+    return choose_slabs(e, archive, r3min, r3max, mt3, sp, alpha_max, slab_alpha);
+}
+
 // vis_ready (optional): event after which src.vr / src.vi hold the collapsed visibilities; only
 // the scatter reads them.
 int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, float cell_f,
                float* d_out, const ExecPlan* fixed = nullptr, ExecPlan* record = nullptr,
-               unsigned int* d_status_out = nullptr, cudaEvent_t vis_ready = nullptr) {
+               unsigned int* d_status_out = nullptr, cudaEvent_t vis_ready = nullptr, bool allow_spec = true) {
     cudaStream_t st = e->stream;
     const svdi_options& o = e->opt;
     const double cell = (double)cell_f;
@@ -462,6 +479,8 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     if (timed) e->pending = false;         // the previous call's statistics are superseded
     SlabParams sp{};
     double alpha_max = 0, slab_alpha = 0, r3min = 0, r3max = 0, mt3 = 0;
+    const DevPlan* dplan = nullptr;  // speculative: slab geometry and 1 / |det| from the device
+    size_t spec_bslabs = 0;
     if (fixed) {
         src.inv_det = fixed->inv_det;
         sp = fixed->sp;
@@ -475,19 +494,25 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
         SVDI_TRY(launch_t3_stats(e->vin64.as<double>(), N, cell, e->partial.as<double>(), kPartialCap,
                                  e->stats.as<double>(), st));
         SVDI_CUDA(cudaMemcpyAsync(e->h_stats, e->stats.p, ST_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st));
-        SVDI_CUDA(cudaMemcpyAsync(e->last.vin, e->vin64.p, 9 * sizeof(double), cudaMemcpyDeviceToHost, st));
-        SVDI_CUDA(cudaStreamSynchronize(st));
-        r3min = e->h_stats[ST_R3_MIN];
-        r3max = e->h_stats[ST_R3_MAX];
-        mt3 = e->h_stats[ST_MAX_T3];
-        const double* V = e->last.vin;
-        const double det = std::fabs(V[0] * V[4] - V[1] * V[3]);
-        if (!(det > 0.0) || !std::isfinite(det)) {
-            set_error("degenerate basis: |V00 V11 - V01 V10| is zero");
-            return SVDI_ERR_INVALID_ARGUMENT;
+        SVDI_CUDA(cudaMemcpyAsync(e->h_stats + ST_COUNT, e->vin64.p, 9 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        bool spec = allow_spec && !record && e->spec_valid && e->spec_archive == archive && e->spec_N == N &&
+                    e->spec_cell == cell_f && e->spec_n == n && e->spec_R == src.R &&
+                    e->spec_bin == (src.bin != nullptr);
+        if (spec) {  // one batch of all slabs only
+            spec_bslabs = batch_slabs_for(e, e->spec_sp.nslab, e->spec_sp.K, grid_size(N, o.sigma));
+            spec = (int)spec_bslabs >= e->spec_sp.nslab;
         }
-        src.inv_det = (float)(1.0 / det);
-        SVDI_TRY(choose_slabs(e, archive, r3min, r3max, mt3, sp, alpha_max, slab_alpha));
+        if (spec) {
+            SVDI_CUDA(cudaEventRecord(e->ev_stats, st));
+            sp = e->spec_sp;
+            SVDI_TRY(e->plan_buf.ensure(sizeof(DevPlan)));
+            SVDI_TRY(launch_plan(e->stats.as<double>(), e->vin64.as<double>(), archive, sp.nslab, sp.K,
+                                 e->plan_buf.as<DevPlan>(), st));
+            dplan = e->plan_buf.as<DevPlan>();
+        } else {
+            SVDI_CUDA(cudaStreamSynchronize(st));
+            SVDI_TRY(host_decision(e, archive, src, sp, alpha_max, slab_alpha, r3min, r3max, mt3));
+        }
     }
 
     GridGeom g{};
@@ -539,7 +564,7 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     SVDI_CUDA(cudaMemsetAsync(e->counts.p, 0, (size_t)n_keys * 4, st));
     SVDI_CUDA(cudaMemsetAsync(e->dropped.p, 0, 8, st));
     SVDI_TRY(launch_histogram(src, g, sp, e->counts.as<unsigned int>(), n_keys,
-                              e->dropped.as<unsigned long long>(), st));
+                              e->dropped.as<unsigned long long>(), st, dplan));
     if (use_tc) {
         SVDI_TRY(e->kb_offsets.ensure((size_t)(n_keys + 1) * 4));
     } else {  // the FP32 gridder's chunk table and per-key maxima
@@ -560,11 +585,11 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     SVDI_TRY(launch_scatter(src, g, sp, e->cursor.as<unsigned int>(), n_keys, e->rec.as<SampleRec>(),
                             need_s ? e->rec_s.as<float>() : nullptr,
                             use_tc ? e->tc_status.as<unsigned int>() + 1 : nullptr, st,
-                            use_tc ? nullptr : e->keymax.as<unsigned int>()));
+                            use_tc ? nullptr : e->keymax.as<unsigned int>(), dplan));
     if (timed) SVDI_CUDA(cudaEventRecord(e->ev[2], st));
 
     // slab batches: grid -> FFT -> recombine
-    const size_t bslabs = fixed ? fixed->bslabs : batch_slabs_for(e, sp.nslab, sp.K, g.G);
+    const size_t bslabs = fixed ? fixed->bslabs : (dplan ? spec_bslabs : batch_slabs_for(e, sp.nslab, sp.K, g.G));
     if (record) {
         record->inv_det = src.inv_det;
         record->sp = sp;
@@ -622,7 +647,7 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
         bp.r3_min = sp.r3_min + (double)s0 * sp.slab_width;
         SVDI_TRY(launch_recombine(e->planes.as<float2>(), g, N, cell, e->vin64.as<double>(), bp,
                                   e->corr.as<float>(), 1.0 / (double)n, o.reprojection, o.presplat, d_out,
-                                  st, multi_batch ? e->acc.as<double>() : nullptr, s1 == sp.nslab));
+                                  st, multi_batch ? e->acc.as<double>() : nullptr, s1 == sp.nslab, dplan));
         if (!timed) continue;
         SVDI_CUDA(cudaEventRecord(e->ev[6], st));
         if (!multi_batch) continue;  // one batch: its stage times are read when the call completes
@@ -634,6 +659,30 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
         ms_grid += a;
         ms_fft += b;
         ms_img += c;
+    }
+    if (dplan) {  // the host decision of this call, taken while the device images
+        SVDI_CUDA(cudaEventSynchronize(e->ev_stats));
+        SlabParams real{};
+        const int rc = host_decision(e, archive, src, real, alpha_max, slab_alpha, r3min, r3max, mt3);
+        if (rc != SVDI_OK) {
+            e->spec_valid = false;
+            return rc;
+        }
+        if (real.nslab != sp.nslab || real.K != sp.K) {  // other counts: image again with them
+            e->spec_valid = false;
+            return image_core(e, archive, src, N, cell_f, d_out, nullptr, nullptr, d_status_out, vis_ready, false);
+        }
+        sp = real;  // the same bits as the device plan (slab_params_for, basis_det)
+    }
+    if (!fixed && !record) {
+        e->spec_valid = true;
+        e->spec_archive = archive;
+        e->spec_bin = src.bin != nullptr;
+        e->spec_N = N;
+        e->spec_cell = cell_f;
+        e->spec_n = n;
+        e->spec_R = src.R;
+        e->spec_sp = sp;
     }
     e->last_src = src;
     e->last_g = g;

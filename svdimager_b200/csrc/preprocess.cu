@@ -487,6 +487,20 @@ int launch_t3_stats(const double* d_vin64, long long N, double cell, double* d_p
     return SVDI_OK;
 }
 
+__global__ void k_plan(const double* __restrict__ stats, const double* __restrict__ vin, int archive,
+                       int nslab, int K, DevPlan* __restrict__ plan) {
+    if (threadIdx.x != 0) return;
+    slab_params_for(archive != 0, nslab, K, stats[ST_R3_MIN], stats[ST_R3_MAX], plan->sp);
+    plan->inv_det = (float)(1.0 / basis_det(vin));  // inf or NaN for a degenerate basis, which the host rejects
+}
+
+int launch_plan(const double* d_stats, const double* d_vin64, bool archive, int nslab, int K,
+                DevPlan* d_plan, cudaStream_t st) {
+    k_plan<<<1, 32, 0, st>>>(d_stats, d_vin64, archive ? 1 : 0, nslab, K, d_plan);
+    SVDI_LAUNCHED();
+    return SVDI_OK;
+}
+
 int launch_cheb_errors(double amax, int na, int ns, int kmax, unsigned long long* d_err,
                        cudaStream_t st) {
     if (kmax > kErrMaxK || kmax < 1 || na < 1 || ns < 2) {

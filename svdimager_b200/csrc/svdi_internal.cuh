@@ -54,6 +54,46 @@ struct SlabParams {
     double slab_half;
 };
 
+// Continuous slab parameters of nslab slabs over the w range [r3min, r3max] (SVDIntegratedImager.cu:
+// 973-991; the archive path's single centred slab, archive/FIPkernels.cu:327-366). One definition
+// for the host decision and the device plan, so that both give the same bits.
+__host__ __device__ inline void slab_params_for(bool archive, int nslab, int K, double r3min, double r3max,
+                                                SlabParams& sp) {
+    const double half_range = fmax(0.5 * (r3max - r3min), 1.0e-6);
+    sp.nslab = nslab;
+    sp.K = K;
+    if (archive) {
+        const double centre = 0.5 * (r3max + r3min);
+        sp.r3_min = centre - half_range;
+        sp.slab_width = 2.0 * half_range;
+        sp.slab_half = half_range;
+        sp.inv_half = 1.0 / half_range;
+    } else {
+        const double r3_range = fmax(r3max - r3min, 2.0e-6);
+        sp.r3_min = r3min;
+        sp.slab_width = r3_range / nslab;
+        sp.slab_half = fmax(0.5 * sp.slab_width, 1.0e-6);
+        sp.inv_half = 1.0 / sp.slab_half;
+    }
+}
+
+// |V00 V11 - V01 V10| of the row-major basis, rounded once per operation on host and device.
+__host__ __device__ inline double basis_det(const double* V) {
+#ifdef __CUDA_ARCH__
+    return fabs(__dsub_rn(__dmul_rn(V[0], V[4]), __dmul_rn(V[1], V[3])));
+#else
+    const volatile double a = V[0] * V[4], b = V[1] * V[3];
+    return fabs(a - b);
+#endif
+}
+
+// The slab parameters and 1 / |det| of one snapshot computed on the device from its statistics,
+// for kernels launched before the host has read the statistics back.
+struct DevPlan {
+    SlabParams sp;
+    float inv_det;
+};
+
 // ES kernel as W polynomial pieces in the fractional position: piece i evaluates
 // psi((i - (W/2 - 1) - f) / (W/2)) for f in [0, 1).
 struct EsPoly {
@@ -113,6 +153,9 @@ int launch_t3_stats(const double* d_vin64, long long N, double cell, double* d_p
                     int partial_cap, double* d_stats, cudaStream_t st);
 int launch_cheb_errors(double amax, int na, int ns, int kmax, unsigned long long* d_err,
                        cudaStream_t st);
+// The device plan for nslab slabs and K terms from the statistics (ST_R3_MIN, ST_R3_MAX) and Vin.
+int launch_plan(const double* d_stats, const double* d_vin64, bool archive, int nslab, int K,
+                DevPlan* d_plan, cudaStream_t st);
 
 // binning.cu
 struct SampleSource {
@@ -128,9 +171,10 @@ struct SampleSource {
     long long n;
     float inv_det;
 };
+// d_plan (optional): slab parameters and 1 / |det| read on the device instead of sp and src.inv_det
 int launch_histogram(const SampleSource& src, const GridGeom& g, const SlabParams& sp,
                      unsigned int* d_counts, int n_keys, unsigned long long* d_dropped,
-                     cudaStream_t st);
+                     cudaStream_t st, const DevPlan* d_plan = nullptr);
 // d_kb_offsets (optional): exclusive scan of ceil(count / kb_size) per key, n_keys + 1 entries.
 // d_chunk_key (optional): for every chunk c of chunk_size records, the last key whose records
 // start at or before c * chunk_size (ceil(total / chunk_size) entries, total = offsets[n_keys]).
@@ -141,7 +185,8 @@ int launch_scan(const unsigned int* d_counts, int n_keys, unsigned int* d_offset
 // d_keymax (optional, n_keys entries zeroed by the caller): the same maximum per key
 int launch_scatter(const SampleSource& src, const GridGeom& g, const SlabParams& sp,
                    unsigned int* d_cursor, int n_keys, SampleRec* d_rec, float* d_rec_s,
-                   unsigned int* d_vmax, cudaStream_t st, unsigned int* d_keymax = nullptr);
+                   unsigned int* d_vmax, cudaStream_t st, unsigned int* d_keymax = nullptr,
+                   const DevPlan* d_plan = nullptr);
 
 // gridder_tc.cu: split-precision tcgen05 gridder (one moment plane, support <= 8)
 constexpr int kTcTileRows = 56;    // tile rows: footprint origins; 64-row accumulator with halo
@@ -176,6 +221,7 @@ void build_es_poly(int W, double beta, EsPoly* out);
 int launch_recombine(const float2* d_moments, const GridGeom& g, long long N, double cell,
                      const double* d_vin64, const SlabParams& sp, const float* d_corr,
                      double inv_n_total, int reprojection, int presplat, float* d_out,
-                     cudaStream_t st, double* d_acc = nullptr, bool final_batch = true);
+                     cudaStream_t st, double* d_acc = nullptr, bool final_batch = true,
+                     const DevPlan* d_plan = nullptr);
 
 }  // namespace svdi
