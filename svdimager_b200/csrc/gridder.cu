@@ -9,11 +9,13 @@
 //
 // Accumulation is 32-bit fixed point: on sm_100a a float atomicAdd to shared memory executes as a
 // load + compare-and-swap loop (~3 clk per warp instruction, ~6 under inter-warp overlap, measured),
-// whereas red.shared.add.u32 is native (~1 clk). Each tile segment holds <= 512 samples and gets
-// the scale 0.999 * 2^(22 - e) (max|v| < 2^e), so every contribution stays below 2^22 and no cell
-// can overflow (512 * 2^22 = 2^31); each contribution is rounded to an integer by one FMA against
-// 1.5 * 2^23. The quantisation step is <= 2^-21 max|v| of the segment. Integer sums are
-// order-independent, so a tile segment's contribution is deterministic.
+// whereas red.shared.add.u32 is native (~1 clk). A tile segment (the records of one key within one
+// chunk of kGridChunk records) gets the scale 0.999 * 2^s with s = min(22 - e, 31 - e_sum) for
+// max|v| < 2^e over the key and sum max(|v_re|, |v_im|) < 2^e_sum over the chunk: every contribution
+// stays below 2^22 (one FMA against 1.5 * 2^23 rounds it to an integer exactly) and no cell sum can
+// reach 2^31, since |psi psi| <= 1. On ordinary data the sum bound leaves s = 22 - e, a quantisation
+// step of 2^-22 max|v|. Integer sums are order-independent, so a segment's contribution is
+// deterministic.
 //
 // Inner loop: one warp per sample. Lanes 0..W-1 evaluate the W x-weights and lanes W..2W-1 the
 // W y-weights from a piecewise polynomial of the ES kernel (degree kPolyDeg in the fractional
@@ -95,6 +97,7 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
     using C = TileCfg<W, T, KC>;
     extern __shared__ int tile[];    // [KC][2][R][RS] 32-bit fixed-point accumulators
     __shared__ int bbox[4];          // row min, row max, col min, col max
+    __shared__ float chunk_part[TileCfg<W, T, KC>::NW];  // per-warp partial sums of the chunk
     // per-warp staging of the decoded batch: {u_x, u_y, vre, vim} and {fast-path base, s}
     constexpr int kThreads = C::NT, kWarps = C::NW;
     __shared__ float4 st_f[kWarps][33];  // 32 samples + the zero pad
@@ -144,24 +147,37 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
         const unsigned int c_beg = max(rec_lo, ch * kGridChunk);
         const unsigned int c_end = min(rec_hi, (ch + 1) * kGridChunk);
         int key = max(key_lo, (int)chunk_key[ch]);
+        // sum of max(|v_re|, |v_im|) over the chunk (fixed reduction order: the same in every thread)
+        float csum = 0.0f;
+        {
+            float part = 0.0f;
+            for (unsigned int k = c_beg + threadIdx.x; k < c_end; k += kThreads) {
+                const SampleRec q = rec[k];
+                part += fmaxf(fabsf(q.vre), fabsf(q.vim));
+            }
+            for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+            if (lane == 0) chunk_part[warp] = part;
+            __syncthreads();
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) csum += chunk_part[w];
+        }
         while (key < key_hi && offsets[key] < c_end) {
             const unsigned int s_beg = max(c_beg, offsets[key]);
             const unsigned int s_end = min(c_end, offsets[key + 1]);
             if (s_beg < s_end) {
                 const int slab = key / tiles2;
                 const int t1 = (key / g.ntile2) % g.ntile, t2 = key % g.ntile2;
-                // Fixed-point scale of the segment: 0.999 * 2^(22 - e) with max|v| < 2^e for the
-                // key's largest record (the scatter's per-key maximum), so every contribution
-                // (|psi psi T_n| <= 1 up to the polynomial's 1e-7) stays inside the exact-rounding
-                // range |x| < 2^22 and the <= 512 samples of a segment cannot overflow a 32-bit
-                // cell (512 * 2^22 = 2^31).
+                // Fixed-point scale of the segment (header comment): the key's largest record (the
+                // scatter's per-key maximum) bounds each contribution, the chunk's sum every cell
+                // (|psi psi T_n| <= 1 up to the polynomial's 1e-7, inside the 0.999 margin).
                 float scale = 0.0f, inv_scale = 0.0f;
                 {
                     const float vmax = __uint_as_float(keymax[key]);
-                    if (vmax > 0.0f && vmax < 3.0e38f) {
-                        int ex;
+                    if (vmax > 0.0f && vmax < 3.0e38f && csum < 3.0e38f) {
+                        int ex, es;
                         frexpf(vmax, &ex);  // vmax = f 2^ex, f in [0.5, 1)
-                        scale = ldexpf(0.999f, 22 - ex);
+                        frexpf(csum, &es);
+                        scale = ldexpf(0.999f, min(kGridScaleBits - ex, 31 - es));
                         inv_scale = 1.0f / scale;
                     }
                 }
@@ -418,7 +434,7 @@ int launch_w(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d
              const unsigned int* d_chunk_key, const unsigned int* d_keymax, int key_lo, int key_hi,
              int slab_lo, const GridGeom& g, const SlabParams& sp, const EsPoly& poly, float2* d_planes,
              int sm_count, cudaStream_t st) {
-    static_assert(kGridChunk <= 512, "<= 512 samples per tile segment: no 32-bit overflow");
+
     if (g.T == 64) {
         for (int t0 = 0; t0 < sp.K; ++t0)
             SVDI_TRY((launch_variant<W, 64, 1>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, key_lo, key_hi,

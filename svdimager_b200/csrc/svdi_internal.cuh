@@ -207,7 +207,10 @@ int launch_grid_tc(const SampleRec* d_rec, const unsigned int* d_offsets, const 
 // gridder.cu
 // d_chunk_key, d_keymax: the scan's chunk table (chunks of kGridChunk records) and the scatter's
 // per-key max |value|
-constexpr int kGridChunk = 512;
+constexpr int kGridChunk = 1024;
+// Fixed-point contributions of the FP32 gridder stay below 2^kGridScaleBits (exact rounding with
+// one FMA needs < 2^22)
+constexpr int kGridScaleBits = 22;
 int launch_grid_fp32(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d_offsets,
                      const unsigned int* d_chunk_key, const unsigned int* d_keymax,
                      int n_keys, int key_lo, int key_hi, int slab_lo, const GridGeom& g,
