@@ -100,8 +100,10 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
     __shared__ float chunk_part[TileCfg<W, T, KC>::NW];  // per-warp partial sums of the chunk
     // per-warp staging of the decoded batch: {u_x, u_y, vre, vim} and {fast-path base, s}
     constexpr int kThreads = C::NT, kWarps = C::NW;
-    __shared__ float4 st_f[kWarps][33];  // 32 samples + the zero pad
-    __shared__ int2 st_i[kWarps][33];
+    // per-warp staging of the decoded batch (32 samples + the zero pad): the polynomial arguments
+    // {u_x, u_y}, and {v_re, v_im, shared address of the footprint origin, Chebyshev argument}
+    __shared__ float2 st_u[kWarps][33];
+    __shared__ float4 st_v[kWarps][33];
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int HW = W / 2;
@@ -128,6 +130,7 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
         pass_on[p] = lane_cell && i < W;
     }
     const unsigned int tile_s = (unsigned int)__cvta_generic_to_shared(tile);
+    const unsigned int lane_off_bytes = 4u * (unsigned int)lane_off;
 
     for (int i = threadIdx.x; i < KC * 2 * C::PLANE; i += kThreads) tile[i] = 0;
     if (threadIdx.x == 0) {
@@ -201,14 +204,15 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
                     const int nfast = __popc(fast_mask);
                     if (valid && !rare) {
                         const int pos = __popc(fast_mask & ((1u << lane) - 1u));
-                        st_f[warp][pos] = make_float4(fmaf(2.0f, (float)fxq * (1.0f / 16777216.0f), -1.0f),
-                                                      fmaf(2.0f, (float)fyq * (1.0f / 16777216.0f), -1.0f),
-                                                      r.vre * scale, r.vim * scale);
-                        st_i[warp][pos] = make_int2(r0 * C::RS + c0, __float_as_int(sv));
+                        st_u[warp][pos] = make_float2(fmaf(2.0f, (float)fxq * (1.0f / 16777216.0f), -1.0f),
+                                                      fmaf(2.0f, (float)fyq * (1.0f / 16777216.0f), -1.0f));
+                        st_v[warp][pos] = make_float4(r.vre * scale, r.vim * scale,
+                                                      __uint_as_float(tile_s + 4u * (unsigned int)(r0 * C::RS + c0)),
+                                                      sv);
                     }
                     if (lane == 0) {
-                        st_f[warp][nfast] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                        st_i[warp][nfast] = make_int2(0, 0);
+                        st_u[warp][nfast] = make_float2(0.0f, 0.0f);
+                        st_v[warp][nfast] = make_float4(0.0f, 0.0f, __uint_as_float(tile_s), 0.0f);
                     }
                     // bounding box of the batch (one warp reduction per 32 samples)
                     const int rlo = valid ? max(0, fxq ? r0 : r0 - 1) : C::R;
@@ -228,38 +232,37 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
                     // ---- fast path: W x W footprint, polynomial weights, no bounds checks
                     constexpr int STEP = PAIR ? 2 : 1;
                     if (!need_s) {
+#pragma unroll 2
                         for (int j = 0; j < nfast; j += STEP) {
-                            const float4 su = st_f[warp][PAIR ? j + (lane >> 4) : j];
+                            const float2 su = st_u[warp][PAIR ? j + (lane >> 4) : j];
                             const float u = is_x ? su.x : su.y;
                             float w = coef[kPolyDeg];
 #pragma unroll
                             for (int d = kPolyDeg - 1; d >= 0; --d) w = fmaf(w, u, coef[d]);
 #pragma unroll
                             for (int h = 0; h < STEP; ++h) {
-                                const float4 sf = st_f[warp][j + h];
-                                const int base = st_i[warp][j + h].x;
+                                const float4 sf = st_v[warp][j + h];
                                 const float wy = __shfl_sync(0xffffffffu, w, 16 * h + W + lb);
-                                const unsigned int a = tile_s + 4u * (unsigned int)(base + lane_off);
+                                const unsigned int a = __float_as_uint(sf.z) + lane_off_bytes;
 #pragma unroll
                                 grid_passes<0, PASSES, RPP, C::RS, C::PLANE, kAllLanes>(
-                                    a, w, wy, sf.z, sf.w, 16 * h, wx_src, pass_on);
+                                    a, w, wy, sf.x, sf.y, 16 * h, wx_src, pass_on);
                             }
                         }
                     } else {
                         for (int j = 0; j < nfast; j += STEP) {
-                            const float4 su = st_f[warp][PAIR ? j + (lane >> 4) : j];
+                            const float2 su = st_u[warp][PAIR ? j + (lane >> 4) : j];
                             const float u = is_x ? su.x : su.y;
                             float w = coef[kPolyDeg];
 #pragma unroll
                             for (int d = kPolyDeg - 1; d >= 0; --d) w = fmaf(w, u, coef[d]);
 #pragma unroll
                             for (int h = 0; h < STEP; ++h) {
-                                const float4 sf = st_f[warp][j + h];
-                                const int2 si = st_i[warp][j + h];
+                                const float4 sf = st_v[warp][j + h];
                                 const float wy = __shfl_sync(0xffffffffu, w, 16 * h + W + lb);
                                 float tv[KC];
                                 {
-                                    const float s = __int_as_float(si.y);
+                                    const float s = sf.w;
                                     float tm2 = 1.0f, tm1 = s;
                                     for (int t = 0; t < term0 + KC; ++t) {
                                         const float tn = t == 0 ? 1.0f : (t == 1 ? s : 2.0f * s * tm1 - tm2);
@@ -267,14 +270,14 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
                                         if (t >= term0) tv[t - term0] = tn;
                                     }
                                 }
-                                const int base = si.x + lane_off;
+                                const int base = (int)((__float_as_uint(sf.z) - tile_s) >> 2) + lane_off;
 #pragma unroll
                                 for (int p = 0; p < PASSES; ++p) {
                                     const float wx = __shfl_sync(0xffffffffu, w, 16 * h + wx_src[p]);
                                     if (pass_on[p]) {
                                         const float kv = wx * wy;
                                         int* pl = tile + base + p * RPP * C::RS;
-                                        const float ar = kv * sf.z, ai = kv * sf.w;
+                                        const float ar = kv * sf.x, ai = kv * sf.y;
 #pragma unroll
                                         for (int t = 0; t < KC; ++t) {
                                             atomicAdd(pl + (size_t)t * 2 * C::PLANE, fx_round(fmaf(ar, tv[t], kMagic)));
