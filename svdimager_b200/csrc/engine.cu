@@ -642,7 +642,9 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
         } else {
             SVDI_TRY(launch_grid_fp32(e->rec.as<SampleRec>(), need_s ? e->rec_s.as<float>() : nullptr,
                                       e->offsets.as<unsigned int>(), e->chunk_key.as<unsigned int>(),
-                                      e->keymax.as<unsigned int>(), n_keys, s0 * tiles2, s1 * tiles2, s0, g,
+                                      e->keymax.as<unsigned int>(),
+                                      e->chunk_key.as<unsigned int>() + (size_t)std::max<long long>(n, 1) / kGridChunk + 1,
+                                      n_keys, s0 * tiles2, s1 * tiles2, s0, g,
                                       sp, e->poly, e->planes.as<float2>(), e->sm_count, st));
         }
         if (o.keep_grid && s0 == 0) {

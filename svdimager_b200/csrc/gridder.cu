@@ -88,16 +88,103 @@ struct TileCfg {
     static_assert((RS % 32) == (W % 32), "row stride must be == W (mod 32)");
 };
 
+// Reduces the integer region's bounding box, times inv_scale, into the moment plane of key `key`
+// (checkerboard sign, clipped to the grid) and zeroes it behind. The region's accumulation must
+// be complete (the caller synchronises the CTA before and after).
+template <class C, int T, int KC>
+__device__ __forceinline__ void flush_region(int* __restrict__ tile, const int* bbox, int key, int slab_lo,
+                                             int term0, float inv_scale, const GridGeom& g, const SlabParams& sp,
+                                             float2* __restrict__ planes, int warp, int lane) {
+    constexpr int kWarps = C::NW;
+    const long long GG = g.G * g.G;
+    const int tiles2 = g.ntile * g.ntile2;
+    const int slab = key / tiles2;
+    const int t1 = (key / g.ntile2) % g.ntile, t2 = key % g.ntile2;
+    // flush the bounding box: checkerboard sign, clip to the grid, zero behind. Warps
+    // take rows, lanes consecutive columns (coalesced reductions along a plane row);
+    // the row's plane pointer, parity and on-grid test are computed once per row.
+    const int br0 = bbox[0], br1 = min(bbox[1], C::R - 1);
+    const int bc0 = bbox[2], bc1 = min(bbox[3], C::R - 1);
+    if (br1 >= br0 && bc1 >= bc0) {
+        const long long o1 = g.gmin + (long long)t1 * T;
+        const long long o2 = g.gmin + (long long)t2 * T;
+        const long long row_lim = g.gmax - o1;  // rows rr <= row_lim lie on the grid
+        const int col_lim = (int)min((long long)bc1, g.gmax - o2);
+        const long long plane0 = (long long)(slab - slab_lo) * sp.K + term0;
+        if constexpr (C::RS % 4 == 0) {
+            // four cells per lane: 16-byte shared loads and stores, 16-byte reductions
+            // of two interleaved complex cells where the plane row allows
+            const int q0 = bc0 >> 2, nq = (bc1 >> 2) - q0 + 1;
+            for (int rr = br0 + warp; rr <= br1; rr += kWarps) {
+                const bool row_on = rr <= row_lim;
+                const long long g1 = o1 + rr;
+                const long long rbase = plane0 * GG + (g1 - g.gmin) * g.G + (o2 - g.gmin);
+                float2* prow = planes + rbase;
+                // cc is a multiple of 4, so the sign of cell cc + j is s0 for even j
+                const float s0 = ((g1 + o2) & 1) ? -inv_scale : inv_scale;
+                int* trow = tile + rr * C::RS;
+                for (int gi = lane; gi < nq; gi += 32) {
+                    const int cc = (q0 + gi) * 4;
+#pragma unroll
+                    for (int t = 0; t < KC; ++t) {
+                        int* pl = trow + (size_t)t * 2 * C::PLANE + cc;
+                        const int4 a = *reinterpret_cast<int4*>(pl);
+                        const int4 b = *reinterpret_cast<int4*>(pl + C::PLANE);
+                        *reinterpret_cast<int4*>(pl) = make_int4(0, 0, 0, 0);
+                        *reinterpret_cast<int4*>(pl + C::PLANE) = make_int4(0, 0, 0, 0);
+                        if (!row_on || !(a.x | a.y | a.z | a.w | b.x | b.y | b.z | b.w)) continue;
+                        const float r0 = s0 * (float)a.x, i0 = s0 * (float)b.x;
+                        const float r1 = -s0 * (float)a.y, i1 = -s0 * (float)b.y;
+                        const float r2 = s0 * (float)a.z, i2 = s0 * (float)b.z;
+                        const float r3 = -s0 * (float)a.w, i3 = -s0 * (float)b.w;
+                        float2* p = prow + (long long)t * GG + cc;
+                        if (cc + 3 <= col_lim && ((rbase + (long long)t * GG) & 1) == 0) {
+                            red_add_v4(p, r0, i0, r1, i1);
+                            red_add_v4(p + 2, r2, i2, r3, i3);
+                        } else {
+                            if (cc <= col_lim) red_add_v2(p, r0, i0);
+                            if (cc + 1 <= col_lim) red_add_v2(p + 1, r1, i1);
+                            if (cc + 2 <= col_lim) red_add_v2(p + 2, r2, i2);
+                            if (cc + 3 <= col_lim) red_add_v2(p + 3, r3, i3);
+                        }
+                    }
+                }
+            }
+        } else {
+            for (int rr = br0 + warp; rr <= br1; rr += kWarps) {
+                const bool row_on = rr <= row_lim;
+                const long long g1 = o1 + rr;
+                float2* prow = planes + plane0 * GG + (g1 - g.gmin) * g.G + (o2 - g.gmin);
+                const int par = (int)((g1 + o2) & 1);
+                int* trow = tile + rr * C::RS;
+                for (int cc = bc0 + lane; cc <= bc1; cc += 32) {
+                    const bool on = row_on && cc <= col_lim;
+                    const float s = ((par ^ cc) & 1) ? -inv_scale : inv_scale;
+#pragma unroll
+                    for (int t = 0; t < KC; ++t) {
+                        int* pl = trow + (size_t)t * 2 * C::PLANE + cc;
+                        const int ire = pl[0], iim = pl[C::PLANE];
+                        if (on && (ire | iim))
+                            red_add_v2(prow + (long long)t * GG + cc, s * (float)ire, s * (float)iim);
+                        pl[0] = 0;
+                        pl[C::PLANE] = 0;
+                    }
+                }
+            }
+        }
+    }
+}
+
 template <int W, int T, int KC>
 __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
     const SampleRec* __restrict__ rec, const float* __restrict__ rec_s,
     const unsigned int* __restrict__ offsets, const unsigned int* __restrict__ chunk_key,
-    const unsigned int* __restrict__ keymax, int key_lo, int key_hi, int slab_lo, GridGeom g,
-    SlabParams sp, EsPoly poly, float2* __restrict__ planes, int term0) {
+    const unsigned int* __restrict__ keymax, unsigned int* __restrict__ work, int key_lo, int key_hi,
+    int slab_lo, GridGeom g, SlabParams sp, EsPoly poly, float2* __restrict__ planes, int term0) {
     using C = TileCfg<W, T, KC>;
     extern __shared__ int tile[];    // [KC][2][R][RS] 32-bit fixed-point accumulators
     __shared__ int bbox[4];          // row min, row max, col min, col max
-    __shared__ float chunk_part[TileCfg<W, T, KC>::NW];  // per-warp partial sums of the chunk
+    __shared__ float chunk_part[2][TileCfg<W, T, KC>::NW];  // per-warp partial sums of the chunk
     // per-warp staging of the decoded batch: {u_x, u_y, vre, vim} and {fast-path base, s}
     constexpr int kThreads = C::NT, kWarps = C::NW;
     // per-warp staging of the decoded batch (32 samples + the zero pad): the polynomial arguments
@@ -142,11 +229,27 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
     // key range may be partial); the scan's table gives each chunk's first key
     const unsigned int rec_lo = offsets[key_lo], rec_hi = offsets[key_hi];
     const unsigned int ch_lo = rec_lo / kGridChunk, ch_hi = (rec_hi + kGridChunk - 1) / kGridChunk;
-    const long long GG = g.G * g.G;
-    const int tiles2 = g.ntile * g.ntile2;
     const bool need_s = !(KC == 1 && term0 == 0);
 
-    for (unsigned int ch = ch_lo + blockIdx.x; ch < ch_hi; ch += gridDim.x) {
+    // A CTA takes chunks from a global counter (runs of kRun consecutive chunks; measured on the
+    // precision snapshot: 1 is fastest, longer runs of one key leave a tail). A segment that
+    // continues the key accumulated in the region joins it (one fixed-point scale) while the
+    // running sum bound holds; otherwise the region is reduced into the plane first.
+    constexpr unsigned int kRun = 1;
+    int run_key = -1;  // key accumulated in the region (-1: none); the same in every thread
+    float run_scale = 0.0f, run_inv = 0.0f, run_sum = 0.0f;
+    const unsigned int n_ch = ch_hi - ch_lo;
+    unsigned int it = 0;
+    __shared__ unsigned int s_run;
+    for (;;) {
+    if (threadIdx.x == 0) s_run = atomicAdd(work, 1u);
+    __syncthreads();
+    const unsigned int run = s_run;
+    __syncthreads();
+    if ((unsigned long long)run * kRun >= n_ch) break;
+    const unsigned int q_end = min(n_ch, (run + 1) * kRun);
+    for (unsigned int q = run * kRun; q < q_end; ++q, ++it) {
+        const unsigned int ch = ch_lo + q;
         const unsigned int c_beg = max(rec_lo, ch * kGridChunk);
         const unsigned int c_end = min(rec_hi, (ch + 1) * kGridChunk);
         int key = max(key_lo, (int)chunk_key[ch]);
@@ -159,31 +262,44 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
                 part += fmaxf(fabsf(q.vre), fabsf(q.vim));
             }
             for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-            if (lane == 0) chunk_part[warp] = part;
+            if (lane == 0) chunk_part[it & 1][warp] = part;  // two buffers: no race with the next chunk
             __syncthreads();
 #pragma unroll
-            for (int w = 0; w < kWarps; ++w) csum += chunk_part[w];
+            for (int w = 0; w < kWarps; ++w) csum += chunk_part[it & 1][w];
         }
         while (key < key_hi && offsets[key] < c_end) {
             const unsigned int s_beg = max(c_beg, offsets[key]);
             const unsigned int s_end = min(c_end, offsets[key + 1]);
             if (s_beg < s_end) {
-                const int slab = key / tiles2;
-                const int t1 = (key / g.ntile2) % g.ntile, t2 = key % g.ntile2;
-                // Fixed-point scale of the segment (header comment): the key's largest record (the
-                // scatter's per-key maximum) bounds each contribution, the chunk's sum every cell
-                // (|psi psi T_n| <= 1 up to the polynomial's 1e-7, inside the 0.999 margin).
-                float scale = 0.0f, inv_scale = 0.0f;
-                {
+                // join the region's run of this key, or reduce the region and start a new run
+                if (!(key == run_key && (run_sum + csum) * run_scale < 0.998f * 2147483648.0f)) {
+                    if (run_key >= 0) {
+                        __syncthreads();
+                        flush_region<C, T, KC>(tile, bbox, run_key, slab_lo, term0, run_inv, g, sp, planes, warp, lane);
+                        __syncthreads();
+                        if (threadIdx.x == 0) {
+                            bbox[0] = C::R; bbox[1] = -1; bbox[2] = C::R; bbox[3] = -1;
+                        }
+                        __syncthreads();
+                    }
+                    // Fixed-point scale of the run (header comment): the key's largest record (the
+                    // scatter's per-key maximum) bounds each contribution, the sum over the run's
+                    // chunks every cell (|psi psi T_n| <= 1 up to the polynomial's 1e-7).
+                    run_key = key;
+                    run_sum = 0.0f;
+                    run_scale = 0.0f;
+                    run_inv = 0.0f;
                     const float vmax = __uint_as_float(keymax[key]);
                     if (vmax > 0.0f && vmax < 3.0e38f && csum < 3.0e38f) {
                         int ex, es;
                         frexpf(vmax, &ex);  // vmax = f 2^ex, f in [0.5, 1)
                         frexpf(csum, &es);
-                        scale = ldexpf(0.999f, min(kGridScaleBits - ex, 31 - es));
-                        inv_scale = 1.0f / scale;
+                        run_scale = ldexpf(0.999f, min(kGridScaleBits - ex, 31 - es));
+                        run_inv = 1.0f / run_scale;
                     }
                 }
+                run_sum += csum;
+                const float scale = run_scale;
                 for (unsigned int b0 = s_beg + warp * 32; b0 < s_end; b0 += kWarps * 32) {
                     // ---- decode this lane's record once per batch
                     const unsigned int my = b0 + lane;
@@ -244,7 +360,6 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
                                 const float4 sf = st_v[warp][j + h];
                                 const float wy = __shfl_sync(0xffffffffu, w, 16 * h + W + lb);
                                 const unsigned int a = __float_as_uint(sf.z) + lane_off_bytes;
-#pragma unroll
                                 grid_passes<0, PASSES, RPP, C::RS, C::PLANE, kAllLanes>(
                                     a, w, wy, sf.x, sf.y, 16 * h, wx_src, pass_on);
                             }
@@ -328,92 +443,19 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
                     __syncwarp();
                 }
                 __syncthreads();
-                // flush the bounding box: checkerboard sign, clip to the grid, zero behind. Warps
-                // take rows, lanes consecutive columns (coalesced reductions along a plane row);
-                // the row's plane pointer, parity and on-grid test are computed once per row.
-                const int br0 = bbox[0], br1 = min(bbox[1], C::R - 1);
-                const int bc0 = bbox[2], bc1 = min(bbox[3], C::R - 1);
-                if (br1 >= br0 && bc1 >= bc0) {
-                    const long long o1 = g.gmin + (long long)t1 * T;
-                    const long long o2 = g.gmin + (long long)t2 * T;
-                    const long long row_lim = g.gmax - o1;  // rows rr <= row_lim lie on the grid
-                    const int col_lim = (int)min((long long)bc1, g.gmax - o2);
-                    const long long plane0 = (long long)(slab - slab_lo) * sp.K + term0;
-                    if constexpr (C::RS % 4 == 0) {
-                        // four cells per lane: 16-byte shared loads and stores, 16-byte reductions
-                        // of two interleaved complex cells where the plane row allows
-                        const int q0 = bc0 >> 2, nq = (bc1 >> 2) - q0 + 1;
-                        for (int rr = br0 + warp; rr <= br1; rr += kWarps) {
-                            const bool row_on = rr <= row_lim;
-                            const long long g1 = o1 + rr;
-                            const long long rbase = plane0 * GG + (g1 - g.gmin) * g.G + (o2 - g.gmin);
-                            float2* prow = planes + rbase;
-                            // cc is a multiple of 4, so the sign of cell cc + j is s0 for even j
-                            const float s0 = ((g1 + o2) & 1) ? -inv_scale : inv_scale;
-                            int* trow = tile + rr * C::RS;
-                            for (int gi = lane; gi < nq; gi += 32) {
-                                const int cc = (q0 + gi) * 4;
-#pragma unroll
-                                for (int t = 0; t < KC; ++t) {
-                                    int* pl = trow + (size_t)t * 2 * C::PLANE + cc;
-                                    const int4 a = *reinterpret_cast<int4*>(pl);
-                                    const int4 b = *reinterpret_cast<int4*>(pl + C::PLANE);
-                                    *reinterpret_cast<int4*>(pl) = make_int4(0, 0, 0, 0);
-                                    *reinterpret_cast<int4*>(pl + C::PLANE) = make_int4(0, 0, 0, 0);
-                                    if (!row_on || !(a.x | a.y | a.z | a.w | b.x | b.y | b.z | b.w)) continue;
-                                    const float r0 = s0 * (float)a.x, i0 = s0 * (float)b.x;
-                                    const float r1 = -s0 * (float)a.y, i1 = -s0 * (float)b.y;
-                                    const float r2 = s0 * (float)a.z, i2 = s0 * (float)b.z;
-                                    const float r3 = -s0 * (float)a.w, i3 = -s0 * (float)b.w;
-                                    float2* p = prow + (long long)t * GG + cc;
-                                    if (cc + 3 <= col_lim && ((rbase + (long long)t * GG) & 1) == 0) {
-                                        red_add_v4(p, r0, i0, r1, i1);
-                                        red_add_v4(p + 2, r2, i2, r3, i3);
-                                    } else {
-                                        if (cc <= col_lim) red_add_v2(p, r0, i0);
-                                        if (cc + 1 <= col_lim) red_add_v2(p + 1, r1, i1);
-                                        if (cc + 2 <= col_lim) red_add_v2(p + 2, r2, i2);
-                                        if (cc + 3 <= col_lim) red_add_v2(p + 3, r3, i3);
-                                    }
-                                }
-                            }
-                        }
-                    } else {
-                        for (int rr = br0 + warp; rr <= br1; rr += kWarps) {
-                            const bool row_on = rr <= row_lim;
-                            const long long g1 = o1 + rr;
-                            float2* prow = planes + plane0 * GG + (g1 - g.gmin) * g.G + (o2 - g.gmin);
-                            const int par = (int)((g1 + o2) & 1);
-                            int* trow = tile + rr * C::RS;
-                            for (int cc = bc0 + lane; cc <= bc1; cc += 32) {
-                                const bool on = row_on && cc <= col_lim;
-                                const float s = ((par ^ cc) & 1) ? -inv_scale : inv_scale;
-#pragma unroll
-                                for (int t = 0; t < KC; ++t) {
-                                    int* pl = trow + (size_t)t * 2 * C::PLANE + cc;
-                                    const int ire = pl[0], iim = pl[C::PLANE];
-                                    if (on && (ire | iim))
-                                        red_add_v2(prow + (long long)t * GG + cc, s * (float)ire, s * (float)iim);
-                                    pl[0] = 0;
-                                    pl[C::PLANE] = 0;
-                                }
-                            }
-                        }
-                    }
-                }
-                __syncthreads();
-                if (threadIdx.x == 0) {
-                    bbox[0] = C::R; bbox[1] = -1; bbox[2] = C::R; bbox[3] = -1;
-                }
-                __syncthreads();
             }
             ++key;
         }
     }
+    }
+    if (run_key >= 0) {
+        __syncthreads();
+        flush_region<C, T, KC>(tile, bbox, run_key, slab_lo, term0, run_inv, g, sp, planes, warp, lane);
+    }
 }
 template <int W, int T, int KC>
 int launch_variant(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d_offsets,
-                   const unsigned int* d_chunk_key, const unsigned int* d_keymax,
+                   const unsigned int* d_chunk_key, const unsigned int* d_keymax, unsigned int* d_work,
                    int key_lo, int key_hi, int slab_lo, const GridGeom& g, const SlabParams& sp,
                    const EsPoly& poly, float2* d_planes, int term0, int sm_count, cudaStream_t st) {
     using C = TileCfg<W, T, KC>;
@@ -426,34 +468,35 @@ int launch_variant(const SampleRec* d_rec, const float* d_rec_s, const unsigned 
     int per_sm = 0;
     SVDI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::NT, C::SMEM));
     if (per_sm < 1) per_sm = 1;
-    kern<<<sm_count * per_sm, C::NT, C::SMEM, st>>>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, key_lo,
-                                                     key_hi, slab_lo, g, sp, poly, d_planes, term0);
+    SVDI_CUDA(cudaMemsetAsync(d_work, 0, sizeof(unsigned int), st));
+    kern<<<sm_count * per_sm, C::NT, C::SMEM, st>>>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, d_work,
+                                                     key_lo, key_hi, slab_lo, g, sp, poly, d_planes, term0);
     SVDI_LAUNCHED();
     return SVDI_OK;
 }
 
 template <int W>
 int launch_w(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d_offsets,
-             const unsigned int* d_chunk_key, const unsigned int* d_keymax, int key_lo, int key_hi,
-             int slab_lo, const GridGeom& g, const SlabParams& sp, const EsPoly& poly, float2* d_planes,
-             int sm_count, cudaStream_t st) {
+             const unsigned int* d_chunk_key, const unsigned int* d_keymax, unsigned int* d_work, int key_lo,
+             int key_hi, int slab_lo, const GridGeom& g, const SlabParams& sp, const EsPoly& poly,
+             float2* d_planes, int sm_count, cudaStream_t st) {
 
     if (g.T == 64) {
         for (int t0 = 0; t0 < sp.K; ++t0)
-            SVDI_TRY((launch_variant<W, 64, 1>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, key_lo, key_hi,
+            SVDI_TRY((launch_variant<W, 64, 1>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, d_work, key_lo, key_hi,
                                                slab_lo, g, sp, poly, d_planes, t0, sm_count, st)));
         return SVDI_OK;
     }
     if (g.T == 32) {
         int t0 = 0;
         for (; t0 + 8 <= sp.K; t0 += 8)
-            SVDI_TRY((launch_variant<W, 32, 8>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, key_lo, key_hi,
+            SVDI_TRY((launch_variant<W, 32, 8>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, d_work, key_lo, key_hi,
                                                slab_lo, g, sp, poly, d_planes, t0, sm_count, st)));
         for (; t0 + 4 <= sp.K; t0 += 4)
-            SVDI_TRY((launch_variant<W, 32, 4>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, key_lo, key_hi,
+            SVDI_TRY((launch_variant<W, 32, 4>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, d_work, key_lo, key_hi,
                                                slab_lo, g, sp, poly, d_planes, t0, sm_count, st)));
         for (; t0 < sp.K; ++t0)
-            SVDI_TRY((launch_variant<W, 32, 1>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, key_lo, key_hi,
+            SVDI_TRY((launch_variant<W, 32, 1>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, d_work, key_lo, key_hi,
                                                slab_lo, g, sp, poly, d_planes, t0, sm_count, st)));
         return SVDI_OK;
     }
@@ -464,19 +507,19 @@ int launch_w(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d
 }  // namespace
 
 int launch_grid_fp32(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d_offsets,
-                     const unsigned int* d_chunk_key, const unsigned int* d_keymax,
+                     const unsigned int* d_chunk_key, const unsigned int* d_keymax, unsigned int* d_work,
                      int n_keys, int key_lo, int key_hi, int slab_lo, const GridGeom& g,
                      const SlabParams& sp, const EsPoly& poly, float2* d_planes, int sm_count,
                      cudaStream_t st) {
-    if (key_lo < 0 || key_hi > n_keys || key_lo >= key_hi || !d_chunk_key || !d_keymax) {
+    if (key_lo < 0 || key_hi > n_keys || key_lo >= key_hi || !d_chunk_key || !d_keymax || !d_work) {
         set_error("gridder: bad key range or missing chunk table");
         return SVDI_ERR_INTERNAL;
     }
     switch (g.W) {
-        case 6: return launch_w<6>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, key_lo, key_hi, slab_lo, g, sp, poly, d_planes, sm_count, st);
-        case 8: return launch_w<8>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, key_lo, key_hi, slab_lo, g, sp, poly, d_planes, sm_count, st);
-        case 10: return launch_w<10>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, key_lo, key_hi, slab_lo, g, sp, poly, d_planes, sm_count, st);
-        case 12: return launch_w<12>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, key_lo, key_hi, slab_lo, g, sp, poly, d_planes, sm_count, st);
+        case 6: return launch_w<6>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, d_work, key_lo, key_hi, slab_lo, g, sp, poly, d_planes, sm_count, st);
+        case 8: return launch_w<8>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, d_work, key_lo, key_hi, slab_lo, g, sp, poly, d_planes, sm_count, st);
+        case 10: return launch_w<10>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, d_work, key_lo, key_hi, slab_lo, g, sp, poly, d_planes, sm_count, st);
+        case 12: return launch_w<12>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, d_work, key_lo, key_hi, slab_lo, g, sp, poly, d_planes, sm_count, st);
         default:
             set_error("gridder: ES support must be one of 6, 8, 10, 12");
             return SVDI_ERR_UNSUPPORTED;

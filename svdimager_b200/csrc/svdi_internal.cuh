@@ -211,8 +211,9 @@ constexpr int kGridChunk = 1024;
 // Fixed-point contributions of the FP32 gridder stay below 2^kGridScaleBits (exact rounding with
 // one FMA needs < 2^22)
 constexpr int kGridScaleBits = 22;
+// d_work: one counter the launch resets and its CTAs take runs of chunks from
 int launch_grid_fp32(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d_offsets,
-                     const unsigned int* d_chunk_key, const unsigned int* d_keymax,
+                     const unsigned int* d_chunk_key, const unsigned int* d_keymax, unsigned int* d_work,
                      int n_keys, int key_lo, int key_hi, int slab_lo, const GridGeom& g,
                      const SlabParams& sp, const EsPoly& poly, float2* d_planes, int sm_count,
                      cudaStream_t st);
