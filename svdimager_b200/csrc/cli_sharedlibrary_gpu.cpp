@@ -44,7 +44,8 @@ int main(int argc, char** argv) {
         }
         std::cout << "Time elapsed: " << std::chrono::duration<double, std::milli>(t1 - t0).count() << " ms"
                   << std::endl;
-        svdi_io::write_fits_2d(out, dirty.data(), (long)image_size, (long)image_size);
+        svdi_io::write_fits_2d(out, dirty.data(), (long)image_size, (long)image_size,
+                               svdi_io::wcs_cards_from_env((long)image_size, cell_size));
         return 0;
     } catch (const std::exception& ex) {
         std::cerr << "sharedlibrary_gpu failed: " << ex.what() << "\n";

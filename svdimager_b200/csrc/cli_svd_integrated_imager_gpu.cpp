@@ -54,7 +54,8 @@ int main(int argc, char** argv) {
         const int st = svdi_fipipe_device(&dev, dirty.data(), image_size, cell_size);
         svdi_free_device_buffers(&dev);
         if (st != 0) throw std::runtime_error(std::string("FIpipeDevice failed: ") + svdi_last_error());
-        svdi_io::write_fits_2d(output_name, dirty.data(), (long)image_size, (long)image_size);
+        svdi_io::write_fits_2d(output_name, dirty.data(), (long)image_size, (long)image_size,
+                               svdi_io::wcs_cards_from_env((long)image_size, cell_size));
         const auto total_stop = std::chrono::high_resolution_clock::now();
         std::cerr << "Wrote image FITS: " << output_name << '\n';
         std::cout << "Total pipeline time: "

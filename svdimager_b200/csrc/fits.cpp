@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <map>
@@ -105,9 +106,52 @@ std::vector<float> read_fits_image(const std::string& path, long naxes[2]) {
     return out;
 }
 
-void write_fits_2d(const std::string& path, const float* values, long axis0, long axis1) {
+std::string num_card(const std::string& key, double v) {
+    char buf[32];
+    std::snprintf(buf, sizeof(buf), "%.15E", v);
+    return card(key, buf);
+}
+
+std::string str_card(const std::string& key, const std::string& v) {
+    std::string q = "'" + v;
+    if (q.size() < 9) q.resize(9, ' ');
+    q += "'";
+    std::string s = key;
+    s.resize(8, ' ');
+    s += "= " + q;
+    s.resize(80, ' ');
+    return s;
+}
+
+std::vector<std::string> sin_wcs_cards(long image_size, double cell_rad, double ra_deg, double dec_deg) {
+    const double cell_deg = cell_rad * 180.0 / 3.14159265358979323846;
+    const double crpix = (double)(image_size / 2) + 1.0;  // FITS pixels count from 1
+    return {str_card("CTYPE1", "RA---SIN"), num_card("CRVAL1", ra_deg), num_card("CRPIX1", crpix),
+            num_card("CDELT1", -cell_deg),   str_card("CUNIT1", "deg"),
+            str_card("CTYPE2", "DEC--SIN"), num_card("CRVAL2", dec_deg), num_card("CRPIX2", crpix),
+            num_card("CDELT2", cell_deg),    str_card("CUNIT2", "deg"),
+            str_card("RADESYS", "ICRS"),     num_card("EQUINOX", 2000.0), str_card("BUNIT", "JY/BEAM")};
+}
+
+std::vector<std::string> wcs_cards_from_env(long image_size, double cell_rad) {
+    const char* env = std::getenv("SVDI_FITS_WCS");
+    if (!env || !*env) return {};
+    double ra = 0.0, dec = 0.0;
+    char tail = 0;
+    if (std::sscanf(env, "%lf,%lf%c", &ra, &dec, &tail) != 2 || !(dec >= -90.0 && dec <= 90.0))
+        throw std::runtime_error("SVDI_FITS_WCS must be \"ra_deg,dec_deg\"");
+    return sin_wcs_cards(image_size, cell_rad, ra, dec);
+}
+
+void write_fits_2d(const std::string& path, const float* values, long axis0, long axis1,
+                   const std::vector<std::string>& extra_cards) {
     std::string h = card("SIMPLE", "T") + card("BITPIX", "-32") + card("NAXIS", "2") +
                     card("NAXIS1", std::to_string(axis0)) + card("NAXIS2", std::to_string(axis1));
+    for (const auto& c : extra_cards) {
+        std::string cc = c;
+        cc.resize(80, ' ');
+        h += cc;
+    }
     std::string endc = "END";
     endc.resize(80, ' ');
     h += endc;

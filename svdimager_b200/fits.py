@@ -5,6 +5,8 @@ which uses cfitsio with TFLOAT conversion) and both CLIs write a 2-D FLOAT_IMG
 (SVDIntegratedImager.cu:153-176, archive/pipe_interface.cpp:98-137)."""
 from __future__ import annotations
 
+import math
+
 import numpy as np
 
 BLOCK = 2880
@@ -49,6 +51,19 @@ def write_fits(path: str, data: np.ndarray, extra_cards=None):
         f.write(head + body)
 
 
+def sin_wcs_cards(image_size: int, cell_rad: float, ra_deg: float, dec_deg: float):
+    """World-coordinate cards of an N x N SIN-projected dirty image (FITS WCS paper II), for
+    write_fits(extra_cards=...): reference pixel at the image centre (0-based N // 2, the imager's
+    phase centre), cell_rad per pixel, RA decreasing along axis 1 as the imager lays the image
+    out, phase centre (ra_deg, dec_deg). The CLIs add the same cards when SVDI_FITS_WCS is set."""
+    cell_deg = math.degrees(cell_rad)
+    crpix = float(image_size // 2 + 1)
+    return [("CTYPE1", "RA---SIN"), ("CRVAL1", float(ra_deg)), ("CRPIX1", crpix), ("CDELT1", -cell_deg),
+            ("CUNIT1", "deg"), ("CTYPE2", "DEC--SIN"), ("CRVAL2", float(dec_deg)), ("CRPIX2", crpix),
+            ("CDELT2", cell_deg), ("CUNIT2", "deg"), ("RADESYS", "ICRS"), ("EQUINOX", 2000.0),
+            ("BUNIT", "JY/BEAM")]
+
+
 def read_header(raw: bytes):
     hdr, pos = {}, 0
     while True:
@@ -62,10 +77,22 @@ def read_header(raw: bytes):
             if key == "END":
                 return hdr, pos
             if c[8:10] == "= ":
-                val = c[10:].split("/")[0].strip()
-                if val.startswith("'"):
-                    val = val.strip("'").strip()
-                elif val in ("T", "F"):
+                raw_val = c[10:].strip()
+                if raw_val.startswith("'"):  # quoted string ('' is a quote); a comment may follow
+                    j, out = 1, []
+                    while j < len(raw_val):
+                        if raw_val[j] == "'":
+                            if j + 1 < len(raw_val) and raw_val[j + 1] == "'":
+                                out.append("'")
+                                j += 2
+                                continue
+                            break
+                        out.append(raw_val[j])
+                        j += 1
+                    hdr[key] = "".join(out).rstrip()
+                    continue
+                val = raw_val.split("/")[0].strip()
+                if val in ("T", "F"):
                     val = val == "T"
                 else:
                     try:

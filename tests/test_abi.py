@@ -59,6 +59,19 @@ def test_fits_round_trip(tmp_path):
     assert np.allclose(fits.read_fits(p, np.float64), d)
 
 
+def test_fits_sin_wcs_cards(tmp_path):
+    from svdimager_b200 import fits
+    p = str(tmp_path / "w.fits")
+    a = np.zeros((8, 8), np.float32)
+    fits.write_fits(p, a, extra_cards=fits.sin_wcs_cards(8, 1e-3, 150.0, -30.0))
+    with open(p, "rb") as f:
+        hdr, _ = fits.read_header(f.read())
+    assert hdr["CTYPE1"] == "RA---SIN" and hdr["CTYPE2"] == "DEC--SIN" and hdr["BUNIT"] == "JY/BEAM"
+    assert hdr["CRPIX1"] == 5.0 and hdr["CRVAL2"] == -30.0
+    assert abs(hdr["CDELT1"] + np.degrees(1e-3)) < 1e-15 and abs(hdr["CDELT2"] - np.degrees(1e-3)) < 1e-15
+    assert np.array_equal(fits.read_fits(p), a)
+
+
 def test_cli_usage_exit_codes():
     b = os.path.join(ROOT, "svdimager_b200", "bin")
     r = subprocess.run([os.path.join(b, "sharedlibrary_gpu")], capture_output=True, text=True)

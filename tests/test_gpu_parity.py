@@ -374,6 +374,35 @@ def test_archive_cli_round_trip(cuda_device, tmp_path):
     assert O.rel_rms(img, ref) < 1e-6
 
 
+def test_archive_cli_writes_sin_wcs_on_request(cuda_device, tmp_path):
+    """With SVDI_FITS_WCS="ra,dec" the CLIs add SIN world coordinates to the header; the image
+    itself is unchanged (the reference writes bare images, which stays the default)."""
+    from svdimager_b200 import fits
+    visr, visi, b, v, N, cell = _quartet()
+    paths = {}
+    for name, arr in (("Visreal", visr), ("Visimag", visi), ("B", b), ("V", v)):
+        paths[name] = str(tmp_path / f"{name}.fits")
+        fits.write_fits(paths[name], arr.astype(np.float64))
+    exe = os.path.join(os.path.dirname(api.HERE), "svdimager_b200", "bin", "sharedlibrary_gpu")
+    outs = {}
+    for tag, extra in (("bare", {}), ("wcs", {"SVDI_FITS_WCS": "150.5,-30.25"})):
+        outs[tag] = str(tmp_path / f"{tag}.fits")
+        env = {k: val for k, val in os.environ.items() if k != "SVDI_FITS_WCS"}
+        env.update(extra)
+        r = subprocess.run([exe, paths["Visreal"], paths["Visimag"], paths["B"], paths["V"], str(N), str(len(visr)),
+                            repr(cell), outs[tag]], capture_output=True, text=True, env=env)
+        assert r.returncode == 0, r.stderr
+    with open(outs["wcs"], "rb") as f:
+        hdr, _ = fits.read_header(f.read())
+    with open(outs["bare"], "rb") as f:
+        bare, _ = fits.read_header(f.read())
+    assert "CTYPE1" not in bare
+    assert hdr["CTYPE1"] == "RA---SIN" and hdr["CTYPE2"] == "DEC--SIN"
+    assert hdr["CRVAL1"] == 150.5 and hdr["CRVAL2"] == -30.25 and hdr["CRPIX1"] == N // 2 + 1
+    assert abs(hdr["CDELT2"] - math.degrees(float(np.float32(cell)))) < 1e-12
+    assert O.rel_rms(fits.read_fits(outs["wcs"]), fits.read_fits(outs["bare"])) < 1e-6
+
+
 def test_integrated_cli_round_trip(cuda_device, tmp_path):
     """svd_integrated_imager_gpu on a snapshot bundle equals the engine on the same snapshot."""
     from svdimager_b200 import bundle, fits
