@@ -105,6 +105,11 @@ int svdi_fipipe_device(const svdi_device_buffers* dev, float* dirty_image, size_
 /* Replaces free_device_preprocess_buffers (SVDIntegratedImager.cu:855-865). */
 void svdi_free_device_buffers(svdi_device_buffers* dev);
 
+/* Copies `bytes` from a device array of svdi_device_buffers (or any device pointer of this process)
+ * into host memory and waits for the copy; for callers without their own CUDA runtime. No
+ * counterpart in the reference (its callers read DevicePreprocessBuffers with cudaMemcpy). */
+int svdi_copy_to_host(void* host_dst, const void* device_src, size_t bytes);
+
 /* ---- engine (device-resident, reusable) -------------------------------------------------- */
 /* New export: the reference allocates, plans and frees on every call (SVDIntegratedImager.cu:1630-
  * 1676); an engine keeps grids, cuFFT plans, bins and staging buffers resident between calls. */

@@ -37,7 +37,7 @@ EXPORTED_SYMBOLS = (
     "svdi_kernel_launch_count", "svdi_bin_samples_noalloc", "svdi_server_create",
     "svdi_server_submit", "svdi_server_wait", "svdi_server_poll", "svdi_server_stats",
     "svdi_server_destroy", "svdi_engine_dft_pixels", "svdi_batch_create", "svdi_batch_launch",
-    "svdi_batch_check", "svdi_batch_plan", "svdi_batch_destroy", "_Z6FIpipePfS_S_S_S_mmf",
+    "svdi_batch_check", "svdi_batch_plan", "svdi_batch_destroy", "svdi_copy_to_host", "_Z6FIpipePfS_S_S_S_mmf",
 )
 NOALLOC_MAX_KEYS = 16384
 
@@ -138,6 +138,7 @@ def lib():
         L.svdi_fipipe_device.argtypes = [ctypes.POINTER(DeviceBuffers), P, sz, f]
         L.svdi_free_device_buffers.argtypes = [ctypes.POINTER(DeviceBuffers)]
         L.svdi_free_device_buffers.restype = None
+        L.svdi_copy_to_host.argtypes = [P, P, sz]
         L.svdi_default_options.argtypes = [ctypes.POINTER(Options)]
         L.svdi_default_options.restype = None
         L.svdi_engine_create.argtypes = [ctypes.POINTER(Options), ctypes.POINTER(P)]
@@ -398,6 +399,14 @@ def preprocess_measurement_set_gpu(snap, want_bin: bool = False) -> PreprocessBu
     b = DeviceBuffers()
     _check(lib().svdi_preprocess_measurement_set(ctypes.byref(h), ctypes.byref(b), int(want_bin)))
     return PreprocessBuffers(b, keep)
+
+
+def copy_to_host(out: np.ndarray, device_ptr: int) -> np.ndarray:
+    """Fill the contiguous numpy array `out` from a device address (svdi_copy_to_host)."""
+    if not out.flags.c_contiguous:
+        raise ValueError("out must be C-contiguous")
+    _check(lib().svdi_copy_to_host(_ptr(out), ctypes.c_void_p(device_ptr), out.nbytes))
+    return out
 
 
 def FIpipeDevice(buffers: PreprocessBuffers, image_size: int, cell_size: float) -> np.ndarray:

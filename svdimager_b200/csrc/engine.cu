@@ -1245,6 +1245,16 @@ int svdi_fipipe_device(const svdi_device_buffers* dev, float* dirty_image, size_
     return SVDI_OK;
 }
 
+int svdi_copy_to_host(void* host_dst, const void* device_src, size_t bytes) {
+    g_last_error.clear();
+    if (!host_dst || !device_src) {
+        set_error("null pointer argument");
+        return SVDI_ERR_INVALID_ARGUMENT;
+    }
+    SVDI_CUDA(cudaMemcpy(host_dst, device_src, bytes, cudaMemcpyDeviceToHost));
+    return SVDI_OK;
+}
+
 void svdi_free_device_buffers(svdi_device_buffers* dev) {
     if (!dev) return;
     if (dev->internal) {
