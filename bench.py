@@ -201,7 +201,9 @@ def batching_phase(api, local, n_snapshots=256, launches=3, seed_offset=0):
     t_tune = time.perf_counter() - t_tune
     chosen = [t for t in trials if all(t.options[k] == best[k] for k in ("support", "sigma", "gridder", "tile"))][0]
     imgs = torch.zeros((n_snapshots, N, N), dtype=torch.float32, device=dev)
-    stream = torch.cuda.current_stream(dev)
+    # an explicit stream: the graphs are launched on it and the events recorded on it (a null
+    # stream would launch them on the engine's own stream, outside the timed events)
+    stream = torch.cuda.Stream(dev)
     out = {"snapshots": n_snapshots, "image": f"{N}^2, cell {cell} rad", "total_vis": int(nvis.sum()),
            "vis_per_snapshot": [int(nvis.min()), int(nvis.max())], "generation_s": round(t_gen, 1),
            "autotune": {"seconds": round(t_tune, 2), "candidates": len(trials),
@@ -230,6 +232,35 @@ def batching_phase(api, local, n_snapshots=256, launches=3, seed_offset=0):
         out[name] = {"ms_per_batch": round(ms, 3), "snapshots_per_s": round(n_snapshots / (ms * 1e-3), 1),
                      "vis_per_s": round(float(nvis.sum()) / (ms * 1e-3), 1), "graph_launches_per_batch": 1,
                      "plan_and_capture_s": round(t_cap, 2)}
+        b.close()
+        e.close()
+    # the same 256 snapshots as two half batches (alternate snapshots) on two engines whose graphs
+    # run on their own streams at the same time
+    halves = [descs[0::2], descs[1::2]]
+    engines = [api.Engine(**best) for _ in halves]
+    himgs = [torch.zeros((len(h), N, N), dtype=torch.float32, device=dev) for h in halves]
+    batches = [api.Batch(e, h, N, cell, im.data_ptr()) for e, h, im in zip(engines, halves, himgs)]
+    streams = [torch.cuda.Stream(dev) for _ in halves]
+    for b, st_ in zip(batches, streams):
+        b.launch(st_.cuda_stream)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for st_ in streams:
+        st_.wait_event(e0)
+    for _ in range(launches):
+        for b, st_ in zip(batches, streams):
+            b.launch(st_.cuda_stream)
+    for st_ in streams:
+        stream.wait_stream(st_)
+    e1.record(stream)
+    for b in batches:
+        b.check()
+    ms = e0.elapsed_time(e1) / launches
+    out["tuned_two_streams"] = {"ms_per_batch": round(ms, 3), "snapshots_per_s": round(n_snapshots / (ms * 1e-3), 1),
+                                "vis_per_s": round(float(nvis.sum()) / (ms * 1e-3), 1),
+                                "graph_launches_per_batch": len(batches)}
+    for b, e in zip(batches, engines):
         b.close()
         e.close()
     return out

@@ -495,6 +495,9 @@ int launch_w(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d
         for (; t0 + 4 <= sp.K; t0 += 4)
             SVDI_TRY((launch_variant<W, 32, 4>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, d_work, key_lo, key_hi,
                                                slab_lo, g, sp, poly, d_planes, t0, sm_count, st)));
+        for (; t0 + 2 <= sp.K; t0 += 2)
+            SVDI_TRY((launch_variant<W, 32, 2>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, d_work, key_lo, key_hi,
+                                               slab_lo, g, sp, poly, d_planes, t0, sm_count, st)));
         for (; t0 < sp.K; ++t0)
             SVDI_TRY((launch_variant<W, 32, 1>(d_rec, d_rec_s, d_offsets, d_chunk_key, d_keymax, d_work, key_lo, key_hi,
                                                slab_lo, g, sp, poly, d_planes, t0, sm_count, st)));

@@ -447,3 +447,16 @@ def test_precision_config_properties(cuda_device):
     err = O.rel_rms(R[py, px], d)
     print("precision: K", st["num_terms"], "slabs", st["num_slabs"], "rel RMS vs FP64 DFT", err)
     assert err < IMG_TOL
+
+
+@pytest.mark.parametrize("K", [2, 3, 5])
+def test_fixed_order_tile32_matches_oracle(cuda_device, small_snapshot, K):
+    """Fixed Chebyshev orders on 32x32 tiles: the gridder covers K terms with its 8-, 4-, 2- and
+    1-term variants (K = 2: one two-term pass; 3: two plus one; 5: four plus one)."""
+    s = small_snapshot
+    with api.Engine(k_rule=api.KRULE_FIXED, fixed_k=K, tile=32) as e:
+        img = e.image(s)
+        st = e.stats()
+    assert st["num_terms"] == K and st["tile"] == 32
+    o = O.image_sii(s, k_rule=K)
+    assert O.rel_rms(img, o.image) < IMG_TOL
