@@ -322,7 +322,19 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
                         const int pos = __popc(fast_mask & ((1u << lane) - 1u));
                         st_u[warp][pos] = make_float2(fmaf(2.0f, (float)fxq * (1.0f / 16777216.0f), -1.0f),
                                                       fmaf(2.0f, (float)fyq * (1.0f / 16777216.0f), -1.0f));
-                        st_v[warp][pos] = make_float4(r.vre * scale, r.vim * scale,
+                        // one term per launch: T_term0(s) is folded into the sample's values here, so
+                        // the plain inner loop below grids it (|T_n(s)| <= 1 keeps the scale bound)
+                        float tn = 1.0f;
+                        if (KC == 1 && term0 > 0) {
+                            float tm2 = 1.0f, tm1 = sv;
+                            tn = sv;
+                            for (int t = 2; t <= term0; ++t) {
+                                tn = 2.0f * sv * tm1 - tm2;
+                                tm2 = tm1;
+                                tm1 = tn;
+                            }
+                        }
+                        st_v[warp][pos] = make_float4(r.vre * scale * tn, r.vim * scale * tn,
                                                       __uint_as_float(tile_s + 4u * (unsigned int)(r0 * C::RS + c0)),
                                                       sv);
                     }
@@ -347,7 +359,7 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
                     __syncwarp();
                     // ---- fast path: W x W footprint, polynomial weights, no bounds checks
                     constexpr int STEP = PAIR ? 2 : 1;
-                    if (!need_s) {
+                    if (KC == 1) {
 #pragma unroll 2
                         for (int j = 0; j < nfast; j += STEP) {
                             const float2 su = st_u[warp][PAIR ? j + (lane >> 4) : j];
