@@ -191,6 +191,7 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
     // {u_x, u_y}, and {v_re, v_im, shared address of the footprint origin, Chebyshev argument}
     __shared__ float2 st_u[kWarps][33];
     __shared__ float4 st_v[kWarps][33];
+    __shared__ float2 st_t[kWarps][33];  // KC > 1: T_term0(s), T_term0+1(s) of the staged sample
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int HW = W / 2;
@@ -322,23 +323,29 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
                         const int pos = __popc(fast_mask & ((1u << lane) - 1u));
                         st_u[warp][pos] = make_float2(fmaf(2.0f, (float)fxq * (1.0f / 16777216.0f), -1.0f),
                                                       fmaf(2.0f, (float)fyq * (1.0f / 16777216.0f), -1.0f));
-                        // one term per launch: T_term0(s) is folded into the sample's values here, so
-                        // the plain inner loop below grids it (|T_n(s)| <= 1 keeps the scale bound)
-                        float tn = 1.0f;
-                        if (KC == 1 && term0 > 0) {
-                            float tm2 = 1.0f, tm1 = sv;
-                            tn = sv;
-                            for (int t = 2; t <= term0; ++t) {
-                                tn = 2.0f * sv * tm1 - tm2;
+                        // Chebyshev terms of the sample, once per sample (lane-parallel): one term per
+                        // launch is folded into the sample's values, so the plain inner loop below grids
+                        // it (|T_n(s)| <= 1 keeps the scale bound); KC > 1 stages T_term0 and
+                        // T_term0+1, from which the inner loop runs the recurrence KC - 2 steps
+                        float tn = 1.0f, tn1 = sv;
+                        if (need_s) {
+                            float tm2 = 1.0f, tm1 = sv;  // T_0, T_1
+                            for (int t = 2; t <= term0 + 1; ++t) {
+                                const float tt = 2.0f * sv * tm1 - tm2;
                                 tm2 = tm1;
-                                tm1 = tn;
+                                tm1 = tt;
                             }
+                            tn = term0 == 0 ? 1.0f : tm2;  // T_term0
+                            tn1 = term0 == 0 ? sv : tm1;    // T_term0+1
+                            if (KC > 1) st_t[warp][pos] = make_float2(tn, tn1);
                         }
+                        if (KC > 1) tn = 1.0f;
                         st_v[warp][pos] = make_float4(r.vre * scale * tn, r.vim * scale * tn,
                                                       __uint_as_float(tile_s + 4u * (unsigned int)(r0 * C::RS + c0)),
                                                       sv);
                     }
                     if (lane == 0) {
+                        st_t[warp][nfast] = make_float2(0.0f, 0.0f);
                         st_u[warp][nfast] = make_float2(0.0f, 0.0f);
                         st_v[warp][nfast] = make_float4(0.0f, 0.0f, __uint_as_float(tile_s), 0.0f);
                     }
@@ -390,12 +397,11 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
                                 float tv[KC];
                                 {
                                     const float s = sf.w;
-                                    float tm2 = 1.0f, tm1 = s;
-                                    for (int t = 0; t < term0 + KC; ++t) {
-                                        const float tn = t == 0 ? 1.0f : (t == 1 ? s : 2.0f * s * tm1 - tm2);
-                                        if (t >= 2) { tm2 = tm1; tm1 = tn; }
-                                        if (t >= term0) tv[t - term0] = tn;
-                                    }
+                                    const float2 t01 = st_t[warp][j + h];
+                                    tv[0] = t01.x;
+                                    if (KC > 1) tv[KC > 1 ? 1 : 0] = t01.y;
+#pragma unroll
+                                    for (int t = 2; t < KC; ++t) tv[t] = 2.0f * s * tv[t - 1] - tv[t - 2];
                                 }
                                 const int base = (int)((__float_as_uint(sf.z) - tile_s) >> 2) + lane_off;
 #pragma unroll
