@@ -219,6 +219,8 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
     }
     const unsigned int tile_s = (unsigned int)__cvta_generic_to_shared(tile);
     const unsigned int lane_off_bytes = 4u * (unsigned int)lane_off;
+    // this lane's polynomial argument in the staged pair {u_x, u_y} of sample j: u_arg[2 j]
+    const float* u_arg = reinterpret_cast<const float*>(&st_u[warp][0]) + (PAIR ? 2 * (lane >> 4) : 0) + (is_x ? 0 : 1);
 
     for (int i = threadIdx.x; i < KC * 2 * C::PLANE; i += kThreads) tile[i] = 0;
     if (threadIdx.x == 0) {
@@ -369,8 +371,7 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
                     if (KC == 1) {
 #pragma unroll 2
                         for (int j = 0; j < nfast; j += STEP) {
-                            const float2 su = st_u[warp][PAIR ? j + (lane >> 4) : j];
-                            const float u = is_x ? su.x : su.y;
+                            const float u = u_arg[2 * j];
                             float w = coef[kPolyDeg];
 #pragma unroll
                             for (int d = kPolyDeg - 1; d >= 0; --d) w = fmaf(w, u, coef[d]);
@@ -385,8 +386,7 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
                         }
                     } else {
                         for (int j = 0; j < nfast; j += STEP) {
-                            const float2 su = st_u[warp][PAIR ? j + (lane >> 4) : j];
-                            const float u = is_x ? su.x : su.y;
+                            const float u = u_arg[2 * j];
                             float w = coef[kPolyDeg];
 #pragma unroll
                             for (int d = kPolyDeg - 1; d >= 0; --d) w = fmaf(w, u, coef[d]);

@@ -14,7 +14,8 @@ constexpr double kCLight = 299792458.0;  // SVDIntegratedImager.cu:382
 constexpr double kPi = 3.14159265358979323846;
 constexpr int kMaxTerms = 64;            // Chebyshev terms the kernels support
 constexpr int kMaxSupport = 16;          // ES support the kernels support
-constexpr int kPolyDeg = 11;             // degree of the piecewise ES polynomials
+constexpr int kPolyDeg = 8;              // degree of the piecewise ES polynomials (FP32 error
+                                         // within 3e-8 of degree 11 for W = 6..12)
 constexpr int kQuantBits = 24;           // grid positions are quantised to 2^-24 cells
 
 // Record of one binned sample (16 bytes). xq/yq: quantised position relative to the tile origin,

@@ -18,7 +18,7 @@ from tests.conftest import snapshot
 pytestmark = pytest.mark.gpu
 
 IMG_TOL = 1e-5
-# Grid planes against the FP64 oracle grid: FP32 ES weights (polynomial, <= 1e-7) and the tile
+# Grid planes against the FP64 oracle grid: FP32 ES weights (degree-8 polynomial, <= 1.2e-7) and the tile
 # accumulator's fixed-point step (<= 2^-21 of the tile segment's max |v| per contribution).
 GRID_TOL = 4e-6
 
