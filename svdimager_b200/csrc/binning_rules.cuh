@@ -23,16 +23,16 @@ __device__ inline int tile_div(int x, int T) {
     return t;
 }
 
-// Q = floor(p 2^24) split exactly in FP64 into cell = floor(p) = Q >> 24 and frac = Q & (2^24 - 1):
-// p 2^24 and cell 2^24 are exact (power-of-two scaling), Q - cell 2^24 is an exact difference of
-// integers below 2^53. |p| >= 1e9 lies beyond every grid (G < 2^24) and is dropped under both edge
-// rules, like the contract's 1e15 bound; within it every integer fits 32 bits (tiles T <= 64).
+// Q = floor(p 2^24) split into cell = floor(p) = Q >> 24 and frac = Q & (2^24 - 1): p 2^24 is exact
+// (power-of-two scaling) and one round-down conversion to a 64-bit integer gives Q exactly
+// (|Q| < 1e9 2^24 < 2^54), so the split is integer arithmetic. |p| >= 1e9 lies beyond every grid
+// (G < 2^24) and is dropped under both edge rules, like the contract's 1e15 bound; within it every
+// cell fits 32 bits (tiles T <= 64).
 __device__ inline bool quantise_axis(double p, const GridGeom& g, int T, int& tile, int& qrel) {
     if (!(fabs(p) < 1e9)) return false;
-    const double Qd = floor(p * 16777216.0);
-    const double celld = floor(Qd * (1.0 / 16777216.0));
-    const int cell = (int)celld;
-    const int frac = (int)fma(celld, -16777216.0, Qd);
+    const long long Q = __double2ll_rd(p * 16777216.0);
+    const int cell = (int)(Q >> 24);
+    const int frac = (int)(Q & 0xFFFFFF);
     const int hw = g.W / 2;
     const int gmin = (int)g.gmin, gmax = (int)g.gmax;
     int lo = frac ? cell - (hw - 1) : cell - hw;
