@@ -100,9 +100,8 @@ __device__ __forceinline__ void flush_region(int* __restrict__ tile, const int* 
     const int tiles2 = g.ntile * g.ntile2;
     const int slab = key / tiles2;
     const int t1 = (key / g.ntile2) % g.ntile, t2 = key % g.ntile2;
-    // flush the bounding box: checkerboard sign, clip to the grid, zero behind. Warps
-    // take rows, lanes consecutive columns (coalesced reductions along a plane row);
-    // the row's plane pointer, parity and on-grid test are computed once per row.
+    // flush the bounding box: checkerboard sign, clip to the grid, zero behind. Consecutive
+    // threads take consecutive cells of a row (coalesced reductions along a plane row).
     const int br0 = bbox[0], br1 = min(bbox[1], C::R - 1);
     const int bc0 = bbox[2], bc1 = min(bbox[3], C::R - 1);
     if (br1 >= br0 && bc1 >= bc0) {
@@ -112,18 +111,30 @@ __device__ __forceinline__ void flush_region(int* __restrict__ tile, const int* 
         const int col_lim = (int)min((long long)bc1, g.gmax - o2);
         const long long plane0 = (long long)(slab - slab_lo) * sp.K + term0;
         if constexpr (C::RS % 4 == 0) {
-            // four cells per lane: 16-byte shared loads and stores, 16-byte reductions
-            // of two interleaved complex cells where the plane row allows
-            const int q0 = bc0 >> 2, nq = (bc1 >> 2) - q0 + 1;
-            for (int rr = br0 + warp; rr <= br1; rr += kWarps) {
-                const bool row_on = rr <= row_lim;
-                const long long g1 = o1 + rr;
-                const long long rbase = plane0 * GG + (g1 - g.gmin) * g.G + (o2 - g.gmin);
+            // four cells per thread: 16-byte shared loads and stores, 16-byte reductions of two
+            // interleaved complex cells where the plane row allows. The CTA's threads take the
+            // box's (row, quad) pairs in row-major order (a region row holds fewer quads than a
+            // warp has lanes), stepping NT pairs at a time with an incremental row/quad split.
+            const int q0 = bc0 >> 2, nq = (bc1 >> 2) - q0 + 1, nr = br1 - br0 + 1;
+            const int tid = warp * 32 + lane;
+            const int dr = C::NT / nq, dq = C::NT - dr * nq;
+            int ri = tid / nq, gi = tid - ri * nq;
+            const int row_lim_i = (int)max(-1LL, min((long long)C::R, row_lim));
+            const long long base0 = plane0 * GG + (o1 - g.gmin) * g.G + (o2 - g.gmin);
+            const int par0 = (int)((o1 + o2) & 1);
+            for (; ri < nr; ri += dr, gi += dq) {
+                if (gi >= nq) {
+                    gi -= nq;
+                    if (++ri >= nr) break;
+                }
+                const int rr = br0 + ri;
+                const bool row_on = rr <= row_lim_i;
+                const long long rbase = base0 + (long long)(rr * (int)g.G);
                 float2* prow = planes + rbase;
                 // cc is a multiple of 4, so the sign of cell cc + j is s0 for even j
-                const float s0 = ((g1 + o2) & 1) ? -inv_scale : inv_scale;
+                const float s0 = ((par0 ^ rr) & 1) ? -inv_scale : inv_scale;
                 int* trow = tile + rr * C::RS;
-                for (int gi = lane; gi < nq; gi += 32) {
+                {
                     const int cc = (q0 + gi) * 4;
 #pragma unroll
                     for (int t = 0; t < KC; ++t) {
