@@ -388,17 +388,8 @@ int launch_histogram(const SampleSource& src, const GridGeom& g, const SlabParam
                      unsigned int* d_counts, int n_keys, unsigned long long* d_dropped,
                      cudaStream_t st, const DevPlan* d_plan) {
     const size_t smem = n_keys <= kSmemKeyLimit ? (size_t)n_keys * 4 : 0;
-    static size_t configured = 48 * 1024;  // the attribute is raised once, to the largest size used
-    if (smem > configured) {
-        SVDI_CUDA(cudaFuncSetAttribute(k_histogram, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured = smem;
-    }
     if (use_sep(src)) {
-        static size_t configured_sep = 48 * 1024;
-        if (smem > configured_sep) {
-            SVDI_CUDA(cudaFuncSetAttribute(k_histogram_sep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            configured_sep = smem;
-        }
+        SVDI_TRY(ensure_dynamic_smem((const void*)k_histogram_sep, smem));
         const SepMap m = sep_map(src);
         const long long units = (long long)m.nrt * m.nch;
         long long blocks = (units + kThreads / 32 - 1) / (kThreads / 32);
@@ -408,6 +399,7 @@ int launch_histogram(const SampleSource& src, const GridGeom& g, const SlabParam
         SVDI_LAUNCHED();
         return SVDI_OK;
     }
+    SVDI_TRY(ensure_dynamic_smem((const void*)k_histogram, smem));
     long long blocks = (src.n + kThreads - 1) / kThreads;
     if (blocks > 148 * 8) blocks = 148 * 8;
     if (blocks < 1) blocks = 1;
@@ -439,11 +431,7 @@ int launch_scatter(const SampleSource& src, const GridGeom& g, const SlabParams&
         return SVDI_OK;
     }
     const size_t smem = n_keys <= kSmemKeyLimit / 2 ? (size_t)n_keys * 8 : 0;
-    static size_t configured = 48 * 1024;  // the attribute is raised once, to the largest size used
-    if (smem > configured) {
-        SVDI_CUDA(cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured = smem;
-    }
+    SVDI_TRY(ensure_dynamic_smem((const void*)k_scatter, smem));
     long long blocks = (src.n + kChunk - 1) / kChunk;
     if (blocks > 148 * 16) blocks = 148 * 16;
     if (blocks < 1) blocks = 1;

@@ -30,6 +30,26 @@ static thread_local std::string g_last_error;
 static std::atomic<uint64_t> g_launches{0};
 
 void set_error(const std::string& msg) { g_last_error = msg; }
+
+int ensure_dynamic_smem(const void* func, size_t bytes, bool carveout_max) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, size_t> limit;  // (kernel, device) -> bytes set
+    int dev = 0;
+    SVDI_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = limit.find({func, dev});
+    const bool first = it == limit.end();
+    if (!first && it->second >= bytes) return SVDI_OK;
+    // set explicitly even below 48 KiB: without it the default limit is 48 KiB minus the kernel's
+    // static shared memory
+    if (bytes > 0)
+        SVDI_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    if (carveout_max && first)
+        SVDI_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared));
+    limit[{func, dev}] = bytes;
+    return SVDI_OK;
+}
 void note_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
 
 namespace {

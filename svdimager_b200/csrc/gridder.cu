@@ -489,11 +489,7 @@ int launch_variant(const SampleRec* d_rec, const float* d_rec_s, const unsigned 
                    const EsPoly& poly, float2* d_planes, int term0, int sm_count, cudaStream_t st) {
     using C = TileCfg<W, T, KC>;
     auto kern = k_grid_fp32<W, T, KC>;
-    static bool configured = false;  // per instantiation
-    if (!configured) {
-        SVDI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
-        configured = true;
-    }
+    SVDI_TRY(ensure_dynamic_smem((const void*)kern, C::SMEM));
     int per_sm = 0;
     SVDI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::NT, C::SMEM));
     if (per_sm < 1) per_sm = 1;

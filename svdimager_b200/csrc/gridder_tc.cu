@@ -913,15 +913,9 @@ int launch_grid_tc(const SampleRec* d_rec, const unsigned int* d_offsets, const 
         set_error("tensor-core gridder: needs even support <= 8 and 56 x 8 tiles in groups of 4");
         return SVDI_ERR_UNSUPPORTED;
     }
-    static int per_sm = -1;  // configured and checked once per process
-    if (per_sm < 0) {
-        SVDI_CUDA(cudaFuncSetAttribute(k_grid_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
-        SVDI_CUDA(cudaFuncSetAttribute(k_grid_tc, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                       (int)cudaSharedmemCarveoutMaxShared));
-        int n = 0;
-        SVDI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_grid_tc, kThreads, kSmemBytes));
-        per_sm = n;
-    }
+    SVDI_TRY(ensure_dynamic_smem((const void*)k_grid_tc, kSmemBytes, true));
+    int per_sm = 0;
+    SVDI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grid_tc, kThreads, kSmemBytes));
     if (per_sm < 1) {
         set_error("tensor-core gridder: kernel does not fit on an SM");
         return SVDI_ERR_UNSUPPORTED;

@@ -110,6 +110,12 @@ void note_launch(int n = 1);
 // ---- status helpers ------------------------------------------------------------------------
 void set_error(const std::string& msg);
 
+// Raises kernel `func`'s dynamic shared-memory limit on the current device to at least `bytes`
+// (and, with carveout_max, asks for the largest shared-memory carveout), once per kernel and
+// device. Thread-safe: engines image from several host threads, and the limit only ever grows, so
+// a launch that needed less stays valid while another thread raises it. Returns an SVDI status.
+int ensure_dynamic_smem(const void* func, size_t bytes, bool carveout_max = false);
+
 #define SVDI_CUDA(call)                                                                       \
     do {                                                                                      \
         cudaError_t e__ = (call);                                                             \
