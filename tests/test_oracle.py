@@ -186,3 +186,62 @@ def test_oracle_matches_reference_binary_golden_wide_cell():
     assert O.rel_rms(img.image, z["image_precise"]) < 1e-5
     assert O.rel_rms(img.image, z["image"]) < 1e-4
     assert int(z["K"]) == img.sc.K
+
+
+def _contract_key(p1, p2, G, W, T, edge_mode):
+    """Binning contract for one sample at grid position (p1, p2), exact rational arithmetic:
+    Q = floor(p 2^24), cell = Q >> 24, footprint [cell - (W/2 - 1), cell + W/2] (one cell wider
+    on the low side when the position is an exact integer), clipped to [-G/2, (G-1)/2] or dropped
+    (strict); tile = (low end - gmin) // T; record coordinate Q - tile origin 2^24."""
+    from fractions import Fraction
+    gmin, gmax, hw = -(G // 2), (G - 1) // 2, W // 2
+    ntile = (G + T - 1) // T
+    tiles, qrel = [], []
+    for p in (p1, p2):
+        if not abs(p) < 1e9:
+            return -1, None
+        Q = math.floor(Fraction(p) * 2**24)
+        cell, frac = Q >> 24, Q & 0xFFFFFF
+        lo, hi = (cell - (hw - 1) if frac else cell - hw), cell + hw
+        if edge_mode == 1 and (lo < gmin or hi > gmax):
+            return -1, None
+        lo, hi = max(lo, gmin), min(hi, gmax)
+        if lo > hi:
+            return -1, None
+        t = (lo - gmin) // T
+        tiles.append(t)
+        qrel.append(Q - (gmin + t * T) * 2**24)
+    return tiles[0] * ntile + tiles[1], qrel
+
+
+@pytest.mark.parametrize("edge_mode", [0, 1])
+def test_tile_keys_contract_at_edge_positions(edge_mode):
+    """The oracle's tile keys and record coordinates against an exact restatement of the binning
+    contract at the positions where a floating-point split could go wrong: exact integers, values
+    an ulp either side of them, tiny negatives, tile boundaries, both grid edges, and positions far
+    off the grid. The device rule (one round-down conversion of p 2^24 to a 64-bit integer) is the
+    same integer arithmetic; the GPU parity tests compare its records with these bit for bit."""
+    G, W, T = 384, 8, 64
+    gmin, gmax = -(G // 2), (G - 1) // 2
+    pts = [0.0, -0.0, 1.0, -1.0, 0.5, -0.5, 5e-300, -5e-300, 1e-12, -1e-12, 3.0 - 2**-40, 3.0 + 2**-40,
+           -3.0 - 2**-40, -3.0 + 2**-40, 2**-24, -(2**-24), 2**-25, -(2**-25)]
+    for b in range(gmin, gmax + 1, T):   # tile boundaries of the footprint's low end (lo = p - 3)
+        pts += [b + 3.0, b + 3.0 - 2**-30, b + 3.0 + 2**-30, b + 4.0 - 2**-30]
+    for e in (gmin, gmax):                # both grid edges under clipping and strict rules
+        pts += [e - 4.5, e - 4.0, e - 3.0, e - 0.25, e, e + 0.25, e + 3.0, e + 4.0, e + 4.5]
+    pts += [1e9, -1e9, 2e9, 1e15, float("inf"), float("-inf"), float("nan")]
+    rng = np.random.default_rng(7)
+    pts += list(rng.uniform(gmin - 8, gmax + 8, 64))
+    pts = np.array(pts, np.float64)
+    p1, p2 = np.repeat(pts, len(pts)), np.tile(pts, len(pts))
+    r = np.stack([p1, p2, np.zeros_like(p1)], axis=1)
+    sc = O.SlabConfig(0.0, 1.0, 0.0, 0.0, 1, 1.0, 0.5, 2.0, 0.0, 1)
+    keys, xq, yq, _ = O.tile_keys(r, 1.0, G, W, T, edge_mode, sc, records=True)
+    n_kept = 0
+    for k in range(len(p1)):
+        key, q = _contract_key(float(p1[k]), float(p2[k]), G, W, T, edge_mode)
+        assert keys[k] == key, (p1[k], p2[k], keys[k], key)
+        if key >= 0:
+            n_kept += 1
+            assert (int(xq[k]), int(yq[k])) == (q[0], q[1]), (p1[k], p2[k])
+    assert n_kept > len(p1) // 4
