@@ -290,6 +290,41 @@ def test_edge_clipping_and_integer_positions(cuda_device):
     assert O.rel_rms(img, o.image) < IMG_TOL
 
 
+def _piled_quartet():
+    """50,000 samples on one (non-integer) grid position with large, nearly coherent values, beside
+    10,000 ordinary samples: the pile's chunks carry a value sum ~2^10 times their maximum, so the
+    fixed-point scale is set by the chunk sum (31 - e_sum) and consecutive chunks of the pile cannot
+    share one accumulation run without exceeding 2^31."""
+    N, cell, G = 64, 2e-3, 96
+    scale = float(np.float32(cell)) * G
+    rng = np.random.default_rng(11)
+    n_pile, n_rest = 50_000, 10_000
+    b = np.empty((n_pile + n_rest, 3))
+    b[:n_pile] = np.array([7.37, -11.61, 0.0]) / scale
+    b[n_pile:] = rng.uniform(-1.0, 1.0, (n_rest, 3)) * (G / 2 - 6) / scale
+    b[:, 2] = rng.uniform(-1e-3, 1e-3, n_pile + n_rest)
+    visr = np.concatenate([3.0e4 + rng.normal(0, 30.0, n_pile), rng.normal(size=n_rest)]).astype(np.float32)
+    visi = np.concatenate([rng.normal(0, 30.0, n_pile), rng.normal(size=n_rest)]).astype(np.float32)
+    v = np.eye(3, dtype=np.float32)
+    return visr, visi, b.astype(np.float32), v, N, cell, G, scale
+
+
+def test_samples_piled_on_one_position(cuda_device):
+    """Coincident samples (the domain's collisions): one tile key holds most of the snapshot, the
+    chunk-sum bound sets the fixed-point scale and the pile is flushed chunk by chunk. Records are
+    bit-exact; grid planes and image match the FP64 oracle."""
+    visr, visi, b, v, N, cell, G, scale = _piled_quartet()
+    with api.Engine(api.archive_options(coord_mode=api.COORD_REF32, keep_grid=1)) as e:
+        img = e.fipipe(visr, visi, b, v, N, cell)
+        st = e.stats()
+        _check_binning(e, st, b.astype(np.float64), visr, visi, cell, coord_mode=1)
+        grid = e.buffer(api.BUF_GRID).reshape(-1, G, G)
+    o = O.image_fipk(visr, visi, b, v, N, cell, coord_mode=1)
+    og = O.grid(b.astype(np.float64), visr, visi, scale, G, o.sc, 1.0, coord_mode=1)
+    assert np.linalg.norm(grid - og) / np.linalg.norm(og) < GRID_TOL
+    assert O.rel_rms(img, o.image) < IMG_TOL
+
+
 @pytest.mark.parametrize("N", [255, 100, 64])
 def test_odd_and_small_image_sizes(cuda_device, N):
     s = synth.make_snapshot("small", n_rows_limit=3000, nchan=8)
