@@ -28,6 +28,27 @@ def test_collapse_matches_reference_formula(small_snapshot):
     assert np.all(vr[both] == 0) and np.all(vi[both] == 0)
 
 
+def test_collapse_flagged_nan_follows_reference_arithmetic():
+    """Non-finite data under a flag: the reference multiplies the flagged polarisation by its zero
+    weight (SVDIntegratedImager.cu:606-612), so NaN or Inf data there still yield NaN whenever the
+    other polarisation carries weight, and 0 only when both are flagged."""
+    from types import SimpleNamespace
+    nan, inf = np.float32(np.nan), np.float32(np.inf)
+    f32 = lambda *x: np.array(x, np.float32)
+    s = SimpleNamespace(
+        num_samples=5,
+        vis0_real=f32(nan, inf, 1.0, nan, 2.0), vis0_imag=f32(0.5, 0.5, nan, nan, 0.0),
+        vis3_real=f32(3.0, 3.0, 3.0, nan, 4.0), vis3_imag=f32(1.0, 1.0, 1.0, nan, 0.0),
+        flag0=np.array([1, 1, 0, 1, 0], np.uint8), flag3=np.array([0, 0, 0, 1, 0], np.uint8),
+        weight0=f32(1, 1, 1, 1, 1), weight3=f32(1, 1, 1, 1, 1))
+    vr, vi = O.collapse(s)
+    assert np.isnan(vr[0]) and vi[0] == np.float32(1.0)    # NaN * 0 is NaN
+    assert np.isnan(vr[1]) and vi[1] == np.float32(1.0)    # Inf * 0 is NaN
+    assert vr[2] == np.float32(2.0) and np.isnan(vi[2])    # unflagged NaN propagates
+    assert vr[3] == 0 and vi[3] == 0                       # both flagged: 0, whatever the data
+    assert vr[4] == np.float32(3.0) and vi[4] == 0
+
+
 def test_preprocess_against_numpy_and_pca(small_snapshot):
     s = small_snapshot
     vin, q, sv, ev = O.preprocess64(s)
