@@ -266,3 +266,24 @@ def test_tile_keys_contract_at_edge_positions(edge_mode):
             n_kept += 1
             assert (int(xq[k]), int(yq[k])) == (q[0], q[1]), (p1[k], p2[k])
     assert n_kept > len(p1) // 4
+
+
+@pytest.mark.parametrize("N,cell,tilt", [(256, 4e-4, 0.0), (255, 4e-4, 0.3), (512, 3e-3, -0.8), (64, 2e-2, 1.2)])
+def test_t3_statistics_against_numpy(N, cell, tilt):
+    """max |t3| and the valid-pixel count over the rotated-frame pixels (SII:1029-1077, pixel
+    offsets from the imaging kernel's integer centre), against a vectorised numpy restatement; and
+    max |t3| equals its value at the smallest or largest valid radicand, since t3 is monotone in it."""
+    c, s = math.cos(tilt), math.sin(tilt)
+    vin = np.array([[c, 0.0, s], [0.0, 1.0, 0.0], [-s, 0.0, c]])
+    m, valid = O.t3_stats(vin, N, cell)
+    y, x = np.mgrid[0:N, 0:N]
+    t1, t2 = cell * (y - N // 2), cell * (x - N // 2)
+    v13, v23, v33 = vin[0, 2], vin[1, 2], vin[2, 2]
+    ra = 1.0 - (t1 + v13) ** 2 - (t2 + v23) ** 2
+    ok = ra >= 0
+    t3 = -v33 + (1.0 if v33 >= 0 else -1.0) * np.sqrt(ra[ok])
+    assert valid == int(ok.sum()) > 0
+    assert abs(m - np.abs(t3).max()) <= 1e-15 * max(1.0, m)
+    ends = [ra[ok].min(), ra[ok].max()]
+    at_ends = max(abs(-v33 + (1.0 if v33 >= 0 else -1.0) * math.sqrt(r)) for r in ends)
+    assert abs(m - at_ends) <= 1e-15 * max(1.0, m)
