@@ -277,6 +277,19 @@ int svdi_server_stats(svdi_server* s, size_t* queued, size_t* hbm_in_use, size_t
 /* Drains the queue, joins the workers, frees the engines. */
 void svdi_server_destroy(svdi_server* s);
 
+/* The serving handle under its short names: svdi_create makes a server with
+ * SVDI_DEFAULT_SLOTS resident engines, an automatic HBM budget (80 % of the free device memory)
+ * and no fault injection; svdi_submit / svdi_poll / svdi_wait / svdi_destroy are
+ * svdi_server_submit / _poll / _wait / _destroy. Status codes, no exceptions across the ABI;
+ * submit, poll and wait may be called from any thread. */
+#define SVDI_DEFAULT_SLOTS 3
+int svdi_create(const svdi_options* opt, svdi_server** out);
+int svdi_submit(svdi_server* s, const svdi_host_ms* ms, size_t image_size, float cell_size,
+                float* dirty_image, uint64_t* ticket);
+int svdi_poll(svdi_server* s, uint64_t ticket, int* done);
+int svdi_wait(svdi_server* s, uint64_t ticket, double timeout_s, svdi_request_info* info);
+void svdi_destroy(svdi_server* s);
+
 /* ---- allocation-free binning --------------------------------------------------------------- */
 /* No counterpart in the reference. For callers that must not allocate device memory once they
  * run: a correlator's real-time loop that reserves all of its device memory at start-up and

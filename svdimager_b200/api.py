@@ -38,6 +38,7 @@ EXPORTED_SYMBOLS = (
     "svdi_server_submit", "svdi_server_wait", "svdi_server_poll", "svdi_server_stats",
     "svdi_server_destroy", "svdi_engine_dft_pixels", "svdi_batch_create", "svdi_batch_launch",
     "svdi_batch_check", "svdi_batch_plan", "svdi_batch_destroy", "svdi_copy_to_host", "_Z6FIpipePfS_S_S_S_mmf",
+    "svdi_create", "svdi_submit", "svdi_poll", "svdi_wait", "svdi_destroy",
 )
 NOALLOC_MAX_KEYS = 16384
 

@@ -272,6 +272,23 @@ int svdi_server_stats(svdi_server* s, size_t* queued, size_t* hbm_in_use, size_t
     return SVDI_OK;
 }
 
+int svdi_create(const svdi_options* opt, svdi_server** out) {
+    return svdi_server_create(opt, SVDI_DEFAULT_SLOTS, 0, 0, out);
+}
+
+int svdi_submit(svdi_server* s, const svdi_host_ms* ms, size_t image_size, float cell_size, float* dirty_image,
+                uint64_t* ticket) {
+    return svdi_server_submit(s, ms, image_size, cell_size, dirty_image, ticket);
+}
+
+int svdi_poll(svdi_server* s, uint64_t ticket, int* done) { return svdi_server_poll(s, ticket, done); }
+
+int svdi_wait(svdi_server* s, uint64_t ticket, double timeout_s, svdi_request_info* info) {
+    return svdi_server_wait(s, ticket, timeout_s, info);
+}
+
+void svdi_destroy(svdi_server* s) { svdi_server_destroy(s); }
+
 void svdi_server_destroy(svdi_server* s) {
     if (!s) return;
     {

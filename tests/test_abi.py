@@ -47,6 +47,29 @@ def test_error_reporting_without_gpu():
     assert ei.value.status == 1
 
 
+def test_short_name_serving_handle_checks_arguments():
+    """svdi_create / svdi_submit / svdi_poll / svdi_wait / svdi_destroy forward to the server entries:
+    null handles and outputs are refused with SVDI_ERR_INVALID_ARGUMENT before any device call."""
+    import ctypes
+    from svdimager_b200 import api
+    L = api.lib()
+    P = ctypes.c_void_p
+    L.svdi_create.argtypes = [P, P]
+    L.svdi_submit.argtypes = [P, P, ctypes.c_size_t, ctypes.c_float, P, P]
+    L.svdi_poll.argtypes = [P, ctypes.c_uint64, P]
+    L.svdi_wait.argtypes = [P, ctypes.c_uint64, ctypes.c_double, P]
+    L.svdi_destroy.argtypes = [P]
+    L.svdi_destroy.restype = None
+    opt = api.default_options()
+    assert L.svdi_create(ctypes.addressof(opt), None) == 1
+    done, ticket = ctypes.c_int(0), ctypes.c_uint64(0)
+    assert L.svdi_submit(None, None, 16, 1e-3, None, ctypes.addressof(ticket)) == 1
+    assert L.svdi_poll(None, 1, ctypes.addressof(done)) == 1
+    assert L.svdi_wait(None, 1, 0.0, None) == 1
+    assert L.svdi_last_error()
+    L.svdi_destroy(None)  # a null handle is ignored
+
+
 def test_fits_round_trip(tmp_path):
     from svdimager_b200 import fits
     a = np.arange(12, dtype=np.float32).reshape(3, 4) * 0.5
