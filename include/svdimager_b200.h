@@ -305,10 +305,14 @@ void svdi_destroy(svdi_server* s);
  * 2 * SVDI_NOALLOC_MAX_KEYS + 4 words (128 KiB) that every GPU loading this library holds until
  * the process exits; more tile keys than SVDI_NOALLOC_MAX_KEYS are rejected with
  * SVDI_ERR_UNSUPPORTED. The first call on a device looks the array's address up
- * (cudaGetSymbolAddress): make it before any stream capture. Every call shares the array, so
- * calls whose work overlaps on the GPU (other streams, threads or processes on the same device)
- * race; serialise them. Asynchronous on cuda_stream (NULL = legacy default stream); allocates
- * no device memory. */
+ * (cudaGetSymbolAddress): make it before any stream capture. With CUDA's default lazy module
+ * loading that first call is also what loads this library's kernels and the array onto the
+ * device, which takes device memory once: make the first call at start-up, outside the
+ * real-time loop, or set CUDA_MODULE_LOADING=EAGER. The address is kept for the life of the
+ * process, so do not cudaDeviceReset a device after calling this on it. Every call shares the
+ * array, so calls whose work overlaps on the GPU (other streams or threads on the same device)
+ * race; serialise them. Asynchronous on cuda_stream (NULL = legacy default stream); after the
+ * first call on a device it allocates no device memory. */
 #define SVDI_NOALLOC_MAX_KEYS 16384
 int svdi_bin_samples_noalloc(const float* d_bin, const float* d_vis_real, const float* d_vis_imag,
                              size_t num_samples, size_t image_size, float cell_size, int tile,

@@ -393,7 +393,7 @@ int launch_histogram(const SampleSource& src, const GridGeom& g, const SlabParam
         const SepMap m = sep_map(src);
         const long long units = (long long)m.nrt * m.nch;
         long long blocks = (units + kThreads / 32 - 1) / (kThreads / 32);
-        if (blocks > 148 * 4) blocks = 148 * 4;   // a few units per warp: the shared histogram is flushed once
+        if (blocks > 4LL * current_sm_count()) blocks = 4LL * current_sm_count();   // a few units per warp: the shared histogram is flushed once
         if (blocks < 1) blocks = 1;
         k_histogram_sep<<<(int)blocks, kThreads, smem, st>>>(src, m, g, sp, d_counts, n_keys, d_dropped, d_plan);
         SVDI_LAUNCHED();
@@ -401,7 +401,7 @@ int launch_histogram(const SampleSource& src, const GridGeom& g, const SlabParam
     }
     SVDI_TRY(ensure_dynamic_smem((const void*)k_histogram, smem));
     long long blocks = (src.n + kThreads - 1) / kThreads;
-    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks > 8LL * current_sm_count()) blocks = 8LL * current_sm_count();
     if (blocks < 1) blocks = 1;
     k_histogram<<<(int)blocks, kThreads, smem, st>>>(src, g, sp, d_counts, n_keys, d_dropped, d_plan);
     SVDI_LAUNCHED();
@@ -423,7 +423,7 @@ int launch_scatter(const SampleSource& src, const GridGeom& g, const SlabParams&
         const SepMap m = sep_map(src);
         const long long units = (long long)m.nrt * m.nch;
         long long blocks = (units + kThreads / 32 - 1) / (kThreads / 32);
-        if (blocks > 148 * 8) blocks = 148 * 8;
+        if (blocks > 8LL * current_sm_count()) blocks = 8LL * current_sm_count();
         if (blocks < 1) blocks = 1;
         k_scatter_sep<<<(int)blocks, kThreads, 0, st>>>(src, m, g, sp, d_cursor, d_rec, d_rec_s, d_vmax, d_keymax,
                                                         d_plan);
@@ -433,7 +433,7 @@ int launch_scatter(const SampleSource& src, const GridGeom& g, const SlabParams&
     const size_t smem = n_keys <= kSmemKeyLimit / 2 ? (size_t)n_keys * 8 : 0;
     SVDI_TRY(ensure_dynamic_smem((const void*)k_scatter, smem));
     long long blocks = (src.n + kChunk - 1) / kChunk;
-    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (blocks > 16LL * current_sm_count()) blocks = 16LL * current_sm_count();
     if (blocks < 1) blocks = 1;
     k_scatter<<<(int)blocks, kThreads, smem, st>>>(src, g, sp, d_cursor, n_keys, d_rec, d_rec_s, d_vmax, d_keymax,
                                                    d_plan);

@@ -50,6 +50,19 @@ int ensure_dynamic_smem(const void* func, size_t bytes, bool carveout_max) {
     limit[{func, dev}] = bytes;
     return SVDI_OK;
 }
+int current_sm_count() {
+    static std::mutex mu;
+    static std::map<int, int> count;  // device -> SM count
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = count.find(dev);
+    if (it != count.end()) return it->second;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    count[dev] = sms;
+    return sms;
+}
 void note_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
 
 namespace {

@@ -23,7 +23,8 @@ static __device__ __align__(256) unsigned int g_noalloc_scratch[2 * kNoallocMaxK
 std::mutex g_scratch_mu;
 unsigned int* g_scratch_ptr[kMaxDevices] = {};
 
-// Device address of the scratch array for the current device; resolved once per device.
+// Device address of the scratch array for the current device; resolved once per device and kept
+// for the life of the process (a cudaDeviceReset of that device would leave it stale).
 int scratch_for_current_device(unsigned int** out) {
     int dev = 0;
     SVDI_CUDA(cudaGetDevice(&dev));
@@ -49,6 +50,7 @@ extern "C" int svdi_bin_samples_noalloc(const float* d_bin, const float* d_vis_r
                                         float inv_det, void* d_records, uint32_t* d_offsets,
                                         size_t offsets_capacity, void* cuda_stream) {
     using namespace svdi;
+    set_error("");  // a successful call leaves no message from an earlier failed one
     if (!d_bin || !d_vis_real || !d_vis_imag || !d_records || !d_offsets) {
         set_error("null pointer argument");
         return SVDI_ERR_INVALID_ARGUMENT;

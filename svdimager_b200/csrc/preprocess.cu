@@ -435,9 +435,7 @@ int launch_collapse(const float* v0r, const float* v0i, const float* v3r, const 
     auto al = [](const void* p, uintptr_t a) { return ((uintptr_t)p & (a - 1)) == 0; };
     if (al(v0r, 16) && al(v0i, 16) && al(v3r, 16) && al(v3i, 16) && al(w0, 16) && al(w3, 16) && al(outr, 16) &&
         al(outi, 16) && al(f0, 4) && al(f3, 4)) {
-        int dev = 0, sms = 148;
-        if (cudaGetDevice(&dev) == cudaSuccess)
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int sms = current_sm_count();
         long long b = ((n >> 2) + kThreads - 1) / kThreads;
         if (b > (long long)sms * 4) b = (long long)sms * 4;   // 4 of the 8 resident 256-thread blocks per SM
         if (b < 1) b = 1;
@@ -448,7 +446,7 @@ int launch_collapse(const float* v0r, const float* v0i, const float* v3r, const 
             reinterpret_cast<const float4*>(w0), reinterpret_cast<const float4*>(w3),
             reinterpret_cast<float4*>(outr), reinterpret_cast<float4*>(outi), n);
     } else {
-        k_collapse<<<grid_for(n, 148 * 16), kThreads, 0, st>>>(v0r, v0i, v3r, v3i, f0, f3, w0, w3, outr, outi, n);
+        k_collapse<<<grid_for(n, 16 * current_sm_count()), kThreads, 0, st>>>(v0r, v0i, v3r, v3i, f0, f3, w0, w3, outr, outi, n);
     }
     SVDI_LAUNCHED();
     return SVDI_OK;
@@ -456,7 +454,7 @@ int launch_collapse(const float* v0r, const float* v0i, const float* v3r, const 
 
 int launch_expand_bin(const double* d_q, const double* d_s, long long R, long long C, float* d_bin,
                       cudaStream_t st) {
-    k_expand_bin<<<grid_for(R * C, 148 * 16), kThreads, 0, st>>>(d_q, d_s, R, C, d_bin);
+    k_expand_bin<<<grid_for(R * C, 16 * current_sm_count()), kThreads, 0, st>>>(d_q, d_s, R, C, d_bin);
     SVDI_LAUNCHED();
     return SVDI_OK;
 }

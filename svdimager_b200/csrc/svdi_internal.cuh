@@ -116,6 +116,10 @@ void set_error(const std::string& msg);
 // a launch that needed less stays valid while another thread raises it. Returns an SVDI status.
 int ensure_dynamic_smem(const void* func, size_t bytes, bool carveout_max = false);
 
+// Streaming-multiprocessor count of the current device, queried once per device (148 on a
+// B200; launch caps are multiples of it). Thread-safe.
+int current_sm_count();
+
 #define SVDI_CUDA(call)                                                                       \
     do {                                                                                      \
         cudaError_t e__ = (call);                                                             \

@@ -51,9 +51,13 @@ def test_noalloc_binning_matches_engine_twice(cuda_device):
     for call in range(2):
         rec.fill_(0xAB)
         off.fill_(-1)
+        torch.cuda.synchronize(dev)
+        free_before = torch.cuda.mem_get_info(dev)[0]
         api.bin_samples_noalloc(tb.data_ptr(), tr.data_ptr(), ti.data_ptr(), n, N, cell, tile, inv_det,
                                 rec.data_ptr(), off.data_ptr(), n_keys + 1, stream)
         torch.cuda.synchronize(dev)
+        if call == 1:  # the first call may load the module; later calls take no device memory
+            assert torch.cuda.mem_get_info(dev)[0] == free_before, "the call allocated device memory"
         o = off.cpu().numpy().view(np.uint32)
         assert np.array_equal(o, off_ref), f"call {call}: offsets differ"
         total = int(o[-1])
