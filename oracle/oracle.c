@@ -294,33 +294,50 @@ void orc_tile_keys(long n, const double* r, double scale, int coord_mode, long G
 /* planes: complex128 [nslab*K][G][G], plane = slab*K + term; cell (g1, g2) -> index           */
 /* (g1 + G/2) * G + (g2 + G/2). Weight = V * T_term(s) / det * psi1 * psi2 * (-1)^(g1+g2).     */
 /* The reference divides by det in the gridder (SII:1285) or beforehand (FIPK:377-381).        */
-/* Accumulation in FP64; parallel over bands of grid rows (each thread owns its rows).         */
+/* Accumulation in FP64. Threads own 8-row bands of grid rows in turn (band b -> thread b mod  */
+/* threads, which spreads a dense uv core over all threads); each cell's contributions add in  */
+/* sample order, whatever the thread count.                                                    */
 /* ------------------------------------------------------------------------------------------ */
+#define ORC_BAND 8
 void orc_grid(long n, const double* r, const float* vr, const float* vi, double scale, int coord_mode,
               long G, int W, double beta, int K, int nslab, double r3_min, double slab_width,
               double inv_half, double inv_det, int edge_mode, double* planes /* interleaved re,im */) {
     const long GG = G * G;
     const double half_w_inv = 2.0 / (double)W;
+    const long gmin = -(G / 2);
+    /* first footprint row of every sample (or -1 when the sample is not gridded) */
+    long* row0 = (long*)malloc((size_t)(n > 0 ? n : 1) * sizeof(long));
+#pragma omp parallel for schedule(static)
+    for (long k = 0; k < n; ++k) {
+        long a1, b1, a2, b2;
+        double q1, q2;
+        const double p1 = orc_pos(r[k * 3 + 0], scale, coord_mode);
+        const double p2 = orc_pos(r[k * 3 + 1], scale, coord_mode);
+        row0[k] = (orc_footprint(p1, W, G, edge_mode, &a1, &b1, &q1) &&
+                   orc_footprint(p2, W, G, edge_mode, &a2, &b2, &q2)) ? a1 - gmin : -1;
+    }
 #pragma omp parallel
     {
-        int nt = 1, tid = 0;
+        long nt = 1, tid = 0;
 #ifdef _OPENMP
         nt = omp_get_num_threads();
         tid = omp_get_thread_num();
 #endif
-        const long gmin = -(G / 2);
-        const long band = (G + nt - 1) / nt;
-        const long row_lo = gmin + tid * band, row_hi = row_lo + band - 1;
         double w1[64], w2[64], cheb[64];
         for (long k = 0; k < n; ++k) {
+            const long r0 = row0[k];
+            if (r0 < 0) continue;
+            /* the footprint's W + 1 rows touch at most three bands */
+            const long bfirst = r0 / ORC_BAND, blast = (r0 + W) / ORC_BAND;
+            int mine = 0;
+            for (long b = bfirst; b <= blast; ++b) mine |= (b % nt) == tid;
+            if (!mine) continue;
             const double p1 = orc_pos(r[k * 3 + 0], scale, coord_mode);
             const double p2 = orc_pos(r[k * 3 + 1], scale, coord_mode);
             long a1, b1, a2, b2;
             double q1, q2;
-            if (!orc_footprint(p1, W, G, edge_mode, &a1, &b1, &q1) ||
-                !orc_footprint(p2, W, G, edge_mode, &a2, &b2, &q2))
-                continue;
-            if (b1 < row_lo || a1 > row_hi) continue;
+            orc_footprint(p1, W, G, edge_mode, &a1, &b1, &q1);
+            orc_footprint(p2, W, G, edge_mode, &a2, &b2, &q2);
             int slab;
             double s;
             orc_slab(r[k * 3 + 2], nslab, r3_min, slab_width, inv_half, &slab, &s);
@@ -331,7 +348,7 @@ void orc_grid(long n, const double* r, const float* vr, const float* vi, double 
             for (long g = a2; g <= b2; ++g) w2[g - a2] = orc_es(beta, ((double)g - q2) * half_w_inv);
             const double vre = (double)vr[k] * inv_det, vim = (double)vi[k] * inv_det;
             for (long g1 = a1; g1 <= b1; ++g1) {
-                if (g1 < row_lo || g1 > row_hi) continue;
+                if (((g1 - gmin) / ORC_BAND) % nt != tid) continue;
                 for (long g2 = a2; g2 <= b2; ++g2) {
                     double kv = w1[g1 - a1] * w2[g2 - a2];
                     if ((g1 + g2) & 1) kv = -kv;
@@ -346,6 +363,7 @@ void orc_grid(long n, const double* r, const float* vr, const float* vi, double 
             }
         }
     }
+    free(row0);
 }
 
 /* ------------------------------------------------------------------------------------------ */
@@ -418,14 +436,15 @@ static int orc_t3(const double* vin, long N, double cell, long x, long y, double
 /* SII:1392-1445 (fused_interpolation up to fabs); FIPK:463-549 (accumulation + scaling).      */
 /* moments: complex128 [nslab*K][G][G] AFTER the unnormalised inverse FFT.                     */
 /* phi: ES transform per |pixel offset| (orc_es_correction). Invalid pixels -> NaN.            */
+/* Image rows [y0, y1) only (the whole image: 0, N).                                           */
 /* R = |Re sum_j sum_n c_jn M_jn| / (Phi(|x|) Phi(|y|)) / n_total.                             */
 /* ------------------------------------------------------------------------------------------ */
 void orc_recombine(const double* moments, long G, long N, double cell, const double* vin, int K,
                    int nslab, double r3_min, double slab_width, double slab_half, const double* phi,
-                   double n_total, double* R) {
+                   double n_total, long y0, long y1, double* R) {
     const long GG = G * G;
 #pragma omp parallel for schedule(static)
-    for (long y = 0; y < N; ++y) {
+    for (long y = y0; y < y1; ++y) {
         double jv[64];
         for (long x = 0; x < N; ++x) {
             double t1, t2, t3;
@@ -547,16 +566,19 @@ static void orc_splat4(double* out, long N, double LL, double MM, double value) 
     d[(long)Mc * N + (long)Lc] += (0 + LL - Lf) * (0 + MM - Mf) * value;
 }
 
-void orc_reproject_sii(const double* R, long N, double cell, const double* vin, double* out) {
+/* Pixel rows [y0, y1) of R only (the whole image: 0, N).                                      */
+void orc_reproject_sii(const double* R, long N, double cell, const double* vin, long y0, long y1,
+                       double* out) {
     const double r0 = 180.0 / ORC_PI;
     const double dc = cell / ORC_PI * 180.0;
     const double di2 = (double)N * 0.5;
     const long half = N / 2;
     const double xi = vin[6] / vin[8], eta = vin[7] / vin[8];
-    for (long idy = 0; idy < N; ++idy)
+    for (long idy = y0; idy < y1; ++idy)
         for (long idx = 0; idx < N; ++idx) {
             const double v = R[idy * N + idx];
-            if (isnan(v)) continue;
+            double t1, t2, t3; /* invalid pixels (no t3) are skipped; NaN values are splatted */
+            if (!orc_t3(vin, N, cell, idx, idy, &t1, &t2, &t3)) continue;
             const double idxf = (double)idx - di2, idyf = (double)idy - di2;
             const double p1 = (-vin[0] * idxf + vin[3] * idyf) / fabs(vin[8]) + di2;
             const double p2 = (-vin[1] * idxf + vin[4] * idyf) / fabs(vin[8]) + di2;
@@ -585,15 +607,17 @@ void orc_reproject_sii(const double* R, long N, double cell, const double* vin, 
 
 /* Archive path FIPK:552-677: coordschange (integer half size), p2p (Calabretta & Greisen SIN */
 /* with trig; pixels with r^2 > 1 are dropped), finalinterp.                                  */
-void orc_reproject_fipk(const double* R, long N, double cell, const double* vin, double* out) {
+void orc_reproject_fipk(const double* R, long N, double cell, const double* vin, long y0, long y1,
+                        double* out) {
     const long half = N / 2;
     const double dc = cell / ORC_PI * 180.0;
     const double r0 = 180.0 / ORC_PI;
     const double xi = vin[6] / vin[8], eta = vin[7] / vin[8];
     for (long idx = 0; idx < N; ++idx)
-        for (long idy = 0; idy < N; ++idy) {
+        for (long idy = y0; idy < y1; ++idy) {
             const double v = R[idy * N + idx];
-            if (isnan(v)) continue;
+            double t1, t2, t3; /* invalid pixels (no t3) are skipped; NaN values are splatted */
+            if (!orc_t3(vin, N, cell, idx, idy, &t1, &t2, &t3)) continue;
             const double p1 = (-vin[0] * ((double)idx - (double)half) + vin[3] * ((double)idy - (double)half)) / fabs(vin[8]) + (double)half;
             const double p2 = (-vin[1] * ((double)idx - (double)half) + vin[4] * ((double)idy - (double)half)) / fabs(vin[8]) + (double)half;
             double x = -dc * (p1 - ((double)N / 2.0 + 1.0));

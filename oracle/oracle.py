@@ -57,11 +57,11 @@ def lib():
         L.orc_grid.argtypes = [l, P, P, P, d, i, l, i, d, i, i, d, d, d, d, i, P]
         L.orc_bessel_j.argtypes = [d, i, P]
         L.orc_bessel_series_f32.argtypes = [f, i, P]
-        L.orc_recombine.argtypes = [P, l, l, d, P, i, i, d, d, d, P, d, P]
+        L.orc_recombine.argtypes = [P, l, l, d, P, i, i, d, d, d, P, d, l, l, P]
         L.orc_dft_pixels.argtypes = [l, P, P, P, P, d, d, P, l, d, l, P, P, P]
         L.orc_dft_pixels_sep.argtypes = [l, l, P, P, P, P, P, d, d, P, l, d, l, P, P, P]
-        L.orc_reproject_sii.argtypes = [P, l, d, P, P]
-        L.orc_reproject_fipk.argtypes = [P, l, d, P, P]
+        L.orc_reproject_sii.argtypes = [P, l, d, P, l, l, P]
+        L.orc_reproject_fipk.argtypes = [P, l, d, P, l, l, P]
         L.orc_t3_stats.argtypes = [P, l, d, P, P]
         L.orc_cheb_errors.argtypes = [d, i, i, i, P]
         L.orc_num_threads.restype = i
@@ -167,6 +167,53 @@ def slab_config_sii(r3, vin, N, cell, target_alpha=CHEB_TARGET_ALPHA, k_rule="bu
                       slab_alpha, K)
 
 
+def bessel_j(x, nmax):
+    """J_0(x) .. J_nmax(x) in FP64 (orc_bessel_j, Miller's recurrence)."""
+    j = np.zeros(nmax + 1)
+    lib().orc_bessel_j(float(x), int(nmax), _p(j))
+    return j
+
+
+def truncation_bound(a, K):
+    """Jacobi-Anger truncation error bound on |s| <= 1 with K terms kept: 2 sum_{n>=K} |J_n(a)|."""
+    j = bessel_j(a, min(199, K + 60 + int(abs(a))))
+    return 2.0 * float(np.sum(np.abs(j[K:])))
+
+
+def k_for_target(a, target, kmax=64):
+    for K in range(1, kmax + 1):
+        if truncation_bound(a, K) <= target:
+            return K
+    return -1
+
+
+def slab_config_target(r3, vin, N, cell, target_error=1e-6):
+    """Error-target rule of the B200 engine (not in the reference): the slab count n in 1..64 that
+    minimises the moment planes n * K, K the smallest order whose truncation bound at the slab's
+    alpha is <= target_error; slab geometry as SII:973-991."""
+    r3_min, r3_max = float(np.min(r3)), float(np.max(r3))
+    mt3, _ = t3_stats(vin, N, cell)
+    half_range = max(0.5 * (r3_max - r3_min), 1.0e-6)
+    alpha_max = 2.0 * math.pi * mt3 * half_range
+    r3_range = max(r3_max - r3_min, 2.0e-6)
+    best_n, best_p = 1, 1 << 30
+    for n in range(1, 65):
+        h = max(0.5 * r3_range / n, 1.0e-6)
+        K = k_for_target(2.0 * math.pi * mt3 * h, target_error)
+        if K < 0:
+            continue
+        if n * K < best_p:
+            best_p, best_n = n * K, n
+        if K == 1:
+            break
+    width = r3_range / best_n
+    slab_half = max(0.5 * width, 1.0e-6)
+    slab_alpha = 2.0 * math.pi * mt3 * slab_half
+    K = k_for_target(slab_alpha, target_error)
+    return SlabConfig(r3_min, r3_max, mt3, alpha_max, best_n, width, slab_half, 1.0 / slab_half,
+                      slab_alpha, K)
+
+
 def slab_config_fipk(r3, vin, N, cell):
     """FIPK:320-366 compute_host_chebyshev_selection: one slab centred on the r3 range, K = the
     smallest kept-term count in 1..32 whose sampled error (513 x 2048, FP64) is <= 1e-2."""
@@ -228,25 +275,32 @@ def grid(r, vr, vi, scale, G, sc: SlabConfig, inv_det, W=REF_SUPPORT, beta=REF_B
 
 
 def inverse_fft(planes):
-    """Unnormalised inverse 2-D DFT of every plane, as cufftExecC2C(CUFFT_INVERSE) (SII:1713)."""
+    """Unnormalised inverse 2-D DFT of every plane, as cufftExecC2C(CUFFT_INVERSE) (SII:1713).
+    FP64, on all host cores (scipy's pocketfft with workers=-1)."""
+    import scipy.fft
     G = planes.shape[-1]
-    return np.fft.ifft2(planes, axes=(-2, -1)) * (G * G)
+    return scipy.fft.ifft2(planes, axes=(-2, -1), workers=-1) * (G * G)
 
 
-def recombine(moments, N, cell, vin, sc: SlabConfig, phi, n_total):
+def recombine(moments, N, cell, vin, sc: SlabConfig, phi, n_total, rows=None):
+    """Pre-splat image R [N][N]; rows = (y0, y1) computes those image rows only (others 0)."""
     G = moments.shape[-1]
     R = np.zeros((N, N))
+    y0, y1 = rows or (0, N)
     lib().orc_recombine(_p(_c(moments, np.complex128)), G, N, float(cell),
                         _p(_c(vin, np.float64).reshape(-1)), sc.K, sc.num_slabs, sc.r3_min,
                         sc.slab_width, sc.slab_half, _p(_c(phi, np.float64)), float(n_total),
-                        _p(R))
+                        int(y0), int(y1), _p(R))
     return R
 
 
-def reproject(R, N, cell, vin, variant="sii"):
+def reproject(R, N, cell, vin, variant="sii", rows=None):
+    """Bilinear splat of the valid pixels of R (rows = (y0, y1): those pixel rows only)."""
     out = np.zeros((N, N))
+    y0, y1 = rows or (0, N)
     fn = lib().orc_reproject_sii if variant == "sii" else lib().orc_reproject_fipk
-    fn(_p(_c(R, np.float64)), N, float(cell), _p(_c(vin, np.float64).reshape(-1)), _p(out))
+    fn(_p(_c(R, np.float64)), N, float(cell), _p(_c(vin, np.float64).reshape(-1)), int(y0), int(y1),
+       _p(out))
     return out
 
 

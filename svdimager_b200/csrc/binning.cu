@@ -144,6 +144,18 @@ __global__ void __launch_bounds__(1024) k_scan(const unsigned int* __restrict__ 
     }
 }
 
+// NaN or +-Inf: all exponent bits set
+__device__ __forceinline__ unsigned int nonfinite2(float a, float b) {
+    return ((__float_as_uint(a) & 0x7f800000u) == 0x7f800000u) | ((__float_as_uint(b) & 0x7f800000u) == 0x7f800000u);
+}
+
+// Adds the warp's non-finite record count to *counter (one atomic per warp that saw any).
+__device__ __forceinline__ void flush_nonfinite(unsigned long long* counter, unsigned int nbad) {
+    if (!counter || !__any_sync(0xffffffffu, nbad != 0)) return;
+    for (int o = 16; o > 0; o >>= 1) nbad += __shfl_xor_sync(0xffffffffu, nbad, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(counter, (unsigned long long)nbad);
+}
+
 // Scatter: block-aggregated reservation of output ranges per key, then 16-byte record writes.
 __global__ void __launch_bounds__(kThreads) k_scatter(SampleSource src, GridGeom g, SlabParams sp,
                                                      unsigned int* __restrict__ cursor, int n_keys,
@@ -162,6 +174,7 @@ __global__ void __launch_bounds__(kThreads) k_scatter(SampleSource src, GridGeom
     const int lane = threadIdx.x & 31;
     const long long n = src.n;
     float vm = 0.0f;  // max |record value| written by this thread
+    unsigned int nbad = 0;  // non-finite records written by this thread
     for (long long c0 = (long long)blockIdx.x * kChunk; c0 < n; c0 += (long long)gridDim.x * kChunk) {
         KeyRec kr[kPerThread];
         unsigned int rank[kPerThread];
@@ -205,12 +218,14 @@ __global__ void __launch_bounds__(kThreads) k_scatter(SampleSource src, GridGeom
             r.vim = __fmul_rn(src.vi[idx], src.inv_det);
             rec[pos] = r;
             if (rec_s) rec_s[pos] = kr[i].s;
+            nbad += nonfinite2(r.vre, r.vim);
             const float m = fmaxf(fabsf(r.vre), fabsf(r.vim));
             vm = fmaxf(vm, m);
             if (keymax && m > 0.0f) atomicMax(&keymax[key], __float_as_uint(m));
         }
         if (use_smem) __syncthreads();
     }
+    flush_nonfinite(src.nonfinite, nbad);
     if (vmax) {  // non-negative floats order like their bit patterns
         const unsigned int mb = __reduce_max_sync(0xffffffffu, __float_as_uint(vm));
         if (lane == 0 && mb) atomicMax(vmax, mb);
@@ -306,6 +321,7 @@ __global__ void __launch_bounds__(kThreads) k_scatter_sep(SampleSource src, SepM
     const long long nwarps = (long long)gridDim.x * (kThreads / 32);
     const long long R = src.R;
     float vm = 0.0f;
+    unsigned int nbad = 0;
     for (long long u = (long long)blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5); u < nunits; u += nwarps) {
         int rt, ch;
         unit_of(u, m, rt, ch);
@@ -351,6 +367,7 @@ __global__ void __launch_bounds__(kThreads) k_scatter_sep(SampleSource src, SepM
                 r.vim = __fmul_rn(v.y, src.inv_det);
                 rec[pos] = r;
                 if (rec_s) rec_s[pos] = kr.s;
+                nbad += nonfinite2(r.vre, r.vim);
                 const float m = fmaxf(fabsf(r.vre), fabsf(r.vim));
                 vm = fmaxf(vm, m);
                 if (keymax) {  // the group's maximum, one atomic per group
@@ -360,6 +377,7 @@ __global__ void __launch_bounds__(kThreads) k_scatter_sep(SampleSource src, SepM
             }
         }
     }
+    flush_nonfinite(src.nonfinite, nbad);
     if (vmax) {  // non-negative floats order like their bit patterns
         const unsigned int mb = __reduce_max_sync(0xffffffffu, __float_as_uint(vm));
         if (lane == 0 && mb) atomicMax(vmax, mb);

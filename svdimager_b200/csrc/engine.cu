@@ -602,12 +602,15 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     SVDI_TRY(e->counts.ensure((size_t)n_keys * 4));
     SVDI_TRY(e->offsets.ensure((size_t)(n_keys + 1) * 4));
     SVDI_TRY(e->cursor.ensure((size_t)n_keys * 4));
-    SVDI_TRY(e->dropped.ensure(8));
+    SVDI_TRY(e->dropped.ensure(16));  // [0] dropped samples, [1] non-finite gridded values
     SVDI_TRY(e->rec.ensure((size_t)std::max<long long>(n, 1) * sizeof(SampleRec)));
     const bool need_s = sp.K > 1;
     if (need_s) SVDI_TRY(e->rec_s.ensure((size_t)std::max<long long>(n, 1) * sizeof(float)));
     SVDI_CUDA(cudaMemsetAsync(e->counts.p, 0, (size_t)n_keys * 4, st));
-    SVDI_CUDA(cudaMemsetAsync(e->dropped.p, 0, 8, st));
+    SVDI_CUDA(cudaMemsetAsync(e->dropped.p, 0, 16, st));
+    // a NaN or Inf among the gridded values makes the image NaN, as the reference's float atomics
+    // and FFT do (SVDIntegratedImager.cu:606-612 keeps NaN under a zero weight)
+    src.nonfinite = e->dropped.as<unsigned long long>() + 1;
     SVDI_TRY(launch_histogram(src, g, sp, e->counts.as<unsigned int>(), n_keys,
                               e->dropped.as<unsigned long long>(), st, dplan));
     if (use_tc) {
@@ -694,7 +697,8 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
         bp.r3_min = sp.r3_min + (double)s0 * sp.slab_width;
         SVDI_TRY(launch_recombine(e->planes.as<float2>(), g, N, cell, e->vin64.as<double>(), bp,
                                   e->corr.as<float>(), 1.0 / (double)n, o.reprojection, o.presplat, d_out,
-                                  st, multi_batch ? e->acc.as<double>() : nullptr, s1 == sp.nslab, dplan));
+                                  st, multi_batch ? e->acc.as<double>() : nullptr, s1 == sp.nslab, dplan,
+                                  src.nonfinite));
         if (!timed) continue;
         SVDI_CUDA(cudaEventRecord(e->ev[6], st));
         if (!multi_batch) continue;  // one batch: its stage times are read when the call completes

@@ -130,7 +130,8 @@ __global__ void __launch_bounds__(256) k_recombine(const float2* __restrict__ mo
                                                   SlabParams sp, const float* __restrict__ corr,
                                                   double inv_n, int reprojection, int presplat,
                                                   float* __restrict__ out, double* __restrict__ acc,
-                                                  int final_batch, const DevPlan* __restrict__ plan) {
+                                                  int final_batch, const DevPlan* __restrict__ plan,
+                                                  const unsigned long long* __restrict__ nonfinite) {
     if (plan) {  // one batch of all slabs: the device plan's slab geometry
         sp.r3_min = plan->sp.r3_min;
         sp.slab_width = plan->sp.slab_width;
@@ -190,7 +191,10 @@ __global__ void __launch_bounds__(256) k_recombine(const float2* __restrict__ mo
             return;
         }
     }
-    const double value = fabs(signed_sum) * inv_n;
+    double value = fabs(signed_sum) * inv_n;
+    // a NaN or Inf among the gridded values: every moment cell would be NaN after the FFT, so every
+    // valid pixel is NaN (the reference's float atomics, SVDIntegratedImager.cu:1276-1290, carry it)
+    if (nonfinite && *nonfinite) value = __longlong_as_double(0x7ff8000000000000LL);
     if (presplat) {
         out[y * N + x] = (float)value;
         return;
@@ -214,14 +218,15 @@ __global__ void __launch_bounds__(256) k_recombine(const float2* __restrict__ mo
 int launch_recombine(const float2* d_moments, const GridGeom& g, long long N, double cell,
                      const double* d_vin64, const SlabParams& sp, const float* d_corr,
                      double inv_n_total, int reprojection, int presplat, float* d_out,
-                     cudaStream_t st, double* d_acc, bool final_batch, const DevPlan* d_plan) {
+                     cudaStream_t st, double* d_acc, bool final_batch, const DevPlan* d_plan,
+                     const unsigned long long* d_nonfinite) {
     const dim3 block(32, 8);
     const dim3 grid((unsigned)((N + 31) / 32), (unsigned)((N + 7) / 8));
-    if (sp.K <= 1) k_recombine<1><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out, d_acc, final_batch ? 1 : 0, d_plan);
-    else if (sp.K <= 8) k_recombine<8><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out, d_acc, final_batch ? 1 : 0, d_plan);
-    else if (sp.K <= 16) k_recombine<16><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out, d_acc, final_batch ? 1 : 0, d_plan);
-    else if (sp.K <= 32) k_recombine<32><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out, d_acc, final_batch ? 1 : 0, d_plan);
-    else if (sp.K <= kMaxTerms) k_recombine<kMaxTerms><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out, d_acc, final_batch ? 1 : 0, d_plan);
+    if (sp.K <= 1) k_recombine<1><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out, d_acc, final_batch ? 1 : 0, d_plan, d_nonfinite);
+    else if (sp.K <= 8) k_recombine<8><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out, d_acc, final_batch ? 1 : 0, d_plan, d_nonfinite);
+    else if (sp.K <= 16) k_recombine<16><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out, d_acc, final_batch ? 1 : 0, d_plan, d_nonfinite);
+    else if (sp.K <= 32) k_recombine<32><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out, d_acc, final_batch ? 1 : 0, d_plan, d_nonfinite);
+    else if (sp.K <= kMaxTerms) k_recombine<kMaxTerms><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out, d_acc, final_batch ? 1 : 0, d_plan, d_nonfinite);
     else {
         set_error("recombine: too many Chebyshev terms");
         return SVDI_ERR_UNSUPPORTED;

@@ -181,6 +181,8 @@ struct SampleSource {
     const float* vi;
     long long n;
     float inv_det;
+    // optional: the scatter adds the number of records it writes whose value is NaN or +-Inf
+    unsigned long long* nonfinite;
 };
 // d_plan (optional): slab parameters and 1 / |det| read on the device instead of sp and src.inv_det
 int launch_histogram(const SampleSource& src, const GridGeom& g, const SlabParams& sp,
@@ -237,6 +239,6 @@ int launch_recombine(const float2* d_moments, const GridGeom& g, long long N, do
                      const double* d_vin64, const SlabParams& sp, const float* d_corr,
                      double inv_n_total, int reprojection, int presplat, float* d_out,
                      cudaStream_t st, double* d_acc = nullptr, bool final_batch = true,
-                     const DevPlan* d_plan = nullptr);
+                     const DevPlan* d_plan = nullptr, const unsigned long long* d_nonfinite = nullptr);
 
 }  // namespace svdi

@@ -495,3 +495,30 @@ def test_fixed_order_tile32_matches_oracle(cuda_device, small_snapshot, K):
     assert st["num_terms"] == K and st["tile"] == 32
     o = O.image_sii(s, k_rule=K)
     assert O.rel_rms(img, o.image) < IMG_TOL
+
+
+@pytest.mark.parametrize("bad", ["nan_under_flag", "inf"])
+def test_non_finite_visibility_makes_a_nan_image(cuda_device, bad):
+    """A NaN under a flag (the reference multiplies it by the flag's zero weight,
+    SVDIntegratedImager.cu:606-612, and NaN * 0 is NaN) or an Inf in one gridded sample: the
+    reference's float atomics carry it into the grid and its FFT into every moment cell, so every
+    pixel the reprojection reaches is non-finite. The oracle does the same arithmetic in FP64;
+    the non-finite pixels of this path's image are exactly the oracle's, and the rest are 0."""
+    import dataclasses
+    s0 = snapshot("small", n_rows_limit=3000, nchan=8)
+    s = dataclasses.replace(s0, vis0_real=s0.vis0_real.copy(), flag0=s0.flag0.copy(),
+                            flag3=s0.flag3.copy())
+    k = int(np.argmin(np.abs(s.uvw[:, :2]).sum(axis=1)))   # shortest baseline, channel 0: gridded
+    s.flag3[k] = 0
+    if bad == "nan_under_flag":
+        s.vis0_real[k], s.flag0[k] = np.float32(np.nan), 1
+    else:
+        s.vis0_real[k], s.flag0[k] = np.float32(np.inf), 0
+    with api.Engine() as e:
+        img = e.image(s)
+    with np.errstate(invalid="ignore", over="ignore"):
+        o = O.image_sii(s)
+    bad_gpu, bad_orc = ~np.isfinite(img), ~np.isfinite(o.image)
+    assert bad_orc.sum() > img.size // 4
+    assert np.array_equal(bad_gpu, bad_orc)
+    assert np.all(img[~bad_gpu] == 0) and np.all(o.image[~bad_orc] == 0)
