@@ -29,14 +29,14 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
            "--expt-relaxed-constexpr", "-I", INCLUDE] + ARCH
 CU_SOURCES = ["preprocess.cu", "binning.cu", "gridder.cu", "gridder_tc.cu", "image.cu", "engine.cu", "server.cu",
-              "noalloc.cu", "accuracy.cu"]
+              "noalloc.cu", "accuracy.cu", "sii_entry.cpp"]
 CLI_SOURCES = {"sharedlibrary_gpu": ["fits.cpp", "cli_sharedlibrary_gpu.cpp"],
                "svd_integrated_imager_gpu": ["fits.cpp", "bundle.cpp", "cli_svd_integrated_imager_gpu.cpp"]}
 
 
 def _deps(src):
     headers = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".cuh", ".h"))]
-    return [src] + headers + [os.path.join(INCLUDE, "svdimager_b200.h")]
+    return [src] + headers + [os.path.join(INCLUDE, h) for h in os.listdir(INCLUDE)]
 
 
 def _stale(out, deps):
