@@ -3,12 +3,16 @@
 // The reference images one snapshot per process invocation (SVDIntegratedImager.cu:1773-1854). A
 // server keeps `num_slots` imaging engines resident (each with its own CUDA stream, grids, cuFFT
 // plans and tile bins) and a worker thread per slot. Requests queue in arrival order; a request is
-// admitted when a slot is free and its device-memory estimate fits in the HBM budget next to the
-// requests already running; admitted requests run concurrently, so their kernels overlap on the
+// admitted when a slot is free and its device-memory estimate fits in the HBM budget next to what
+// the other slots hold. A slot's engine keeps its buffers (they only grow), so a slot is charged
+// the largest estimate it has served (its resident buffers) and, while it runs a request, the
+// larger of that and the request's estimate: the charges of all slots never exceed the budget, so
+// the engines' resident buffers stay inside it too. Admitted requests run concurrently, so their kernels overlap on the
 // GPU, and a new request starts the moment a slot frees up. Each request records its queueing,
 // running and total latency (host wall clock, submit to completion).
 #include "svdi_internal.cuh"
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -50,7 +54,8 @@ struct svdi_server {
     svdi_options opt{};
     int num_slots = 0;
     size_t budget = 0;
-    size_t in_use = 0;
+    size_t in_use = 0;                // sum of the slots' charges
+    std::vector<size_t> resident;     // per slot: the largest estimate it has served
     int fault_every = 0;
     uint64_t next_ticket = 1;
     uint64_t admitted = 0;
@@ -75,7 +80,6 @@ size_t request_bytes(const svdi_host_ms& ms, size_t N, double sigma, int planes)
 }
 
 void worker_loop(svdi_server* s, int slot) {
-    svdi_engine* e = s->engines[slot];
     for (;;) {
         std::shared_ptr<Request> r;
         {
@@ -83,15 +87,36 @@ void worker_loop(svdi_server* s, int slot) {
             for (;;) {
                 if (s->stop && s->queue.empty()) return;
                 // continuous batching: take the oldest queued request that fits the HBM budget
+                // (this slot's charge grows from its resident buffers to the request's estimate)
+                const size_t res = s->resident[slot];
                 auto it = s->queue.begin();
                 for (; it != s->queue.end(); ++it)
-                    if (s->in_use + (*it)->est_bytes <= s->budget) break;
+                    if (s->in_use - res + std::max(res, (*it)->est_bytes) <= s->budget) break;
                 if (it != s->queue.end()) {
                     r = *it;
                     s->queue.erase(it);
-                    s->in_use += r->est_bytes;
+                    s->in_use += std::max(res, r->est_bytes) - res;
+                    s->resident[slot] = std::max(res, r->est_bytes);
                     ++s->admitted;
                     break;
+                }
+                if (!s->queue.empty() && res > 0) {
+                    // nothing queued fits next to the other slots' buffers: give this idle slot's
+                    // buffers back (a fresh engine) so that the queue cannot stall on resident memory
+                    lk.unlock();
+                    svdi_engine* fresh = nullptr;
+                    const bool ok = svdi_engine_create(&s->opt, &fresh) == SVDI_OK;
+                    if (ok) {
+                        svdi_engine_destroy(s->engines[slot]);
+                        s->engines[slot] = fresh;
+                    }
+                    lk.lock();
+                    if (ok) {
+                        s->in_use -= res;
+                        s->resident[slot] = 0;
+                        s->cv_work.notify_all();
+                        continue;
+                    }
                 }
                 s->cv_work.wait(lk);
             }
@@ -105,7 +130,7 @@ void worker_loop(svdi_server* s, int slot) {
             st = SVDI_ERR_INTERNAL;
             err = "injected host fault";
         } else {
-            st = svdi_engine_image_host(e, &r->ms, r->N, r->cell, r->out);
+            st = svdi_engine_image_host(s->engines[slot], &r->ms, r->N, r->cell, r->out);
             if (st != SVDI_OK) err = svdi_last_error();
         }
         {
@@ -113,8 +138,7 @@ void worker_loop(svdi_server* s, int slot) {
             r->status = st;
             r->error = err;
             r->t_end = Clock::now();
-            r->done = true;
-            s->in_use -= r->est_bytes;
+            r->done = true;  // the slot stays charged its resident buffers
         }
         s->cv_done.notify_all();
         s->cv_work.notify_all();
@@ -147,6 +171,7 @@ int svdi_server_create(const svdi_options* opt, int num_slots, size_t hbm_budget
         hbm_budget_bytes = free_b / 10 * 8;  // 80 % of the free HBM
     }
     s->budget = hbm_budget_bytes;
+    s->resident.assign((size_t)num_slots, 0);
     for (int i = 0; i < num_slots; ++i) {
         svdi_engine* e = nullptr;
         const int st = svdi_engine_create(&s->opt, &e);

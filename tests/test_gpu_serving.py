@@ -79,6 +79,30 @@ def test_admission_refuses_requests_beyond_the_budget(cuda_device, mix):
         assert ei.value.status == 5 and "budget" in ei.value.message
 
 
+def _estimate(s, N, planes=8):
+    """The server's device-memory estimate of a request (server.cu request_bytes)."""
+    G = int(np.ceil(1.5 * N)) + 8
+    return s.num_samples * 54 + s.num_rows * 36 + planes * G * G * 8 + N * N * 4 + (64 << 20)
+
+
+def test_tight_budget_counts_resident_buffers_and_drains(alone, mix):
+    """Engines keep their buffers between requests, so a slot stays charged the largest request it
+    has served. With a budget that holds the largest request once and a half, three slots can never
+    hold two large requests' buffers at once: the charge never exceeds the budget, idle slots give
+    their buffers back when nothing fits, and every request still completes with the same image."""
+    big = max(_estimate(s, N) for s, N, _ in mix)
+    budget = big * 3 // 2
+    with api.Server(num_slots=3, hbm_budget=budget) as srv:
+        tickets = [(i, srv.submit(s, N, cell)) for rep in range(2) for i, (s, N, cell) in enumerate(mix)]
+        peak = 0
+        for i, t in tickets:
+            img, info = srv.wait(t, timeout_s=120)
+            peak = max(peak, srv.stats()["hbm_in_use"])
+            assert info["status"] == 0
+            assert O.rel_rms(img, alone[i]) < MIX_TOL
+        assert 0 < peak <= budget
+
+
 def test_malformed_requests_are_refused(cuda_device, mix):
     s, N, cell = mix[0]
     with api.Server(num_slots=1) as srv:
