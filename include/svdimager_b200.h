@@ -130,7 +130,8 @@ typedef struct svdi_engine svdi_engine;
 #define SVDI_REPROJ_FIPK 1       /* trigonometric SIN deprojection (archive/FIPkernels.cu)      */
 
 #define SVDI_GRIDDER_FP32 0      /* tile-local FP32 gridder (CUDA cores, shared memory)         */
-#define SVDI_GRIDDER_TC 1        /* split-precision tcgen05 tensor-core gridder                */
+#define SVDI_GRIDDER_TC 1        /* split-precision tcgen05 tensor-core gridder, FP16 hi + lo   */
+#define SVDI_GRIDDER_TC_BF16 2   /* the same with BF16 hi + lo operands (16-bit significand)    */
 
 typedef struct svdi_options {
     int device;                  /* CUDA device ordinal                                        */

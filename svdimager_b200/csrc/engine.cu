@@ -567,7 +567,7 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     g.W = o.support;
     // the tensor-core gridder accumulates one moment plane per CTA in TMEM (K == 1) and bins
     // into 56 x 8 tiles, four of which share a 64-row accumulator (gridder_tc.cu)
-    const bool use_tc = o.gridder == SVDI_GRIDDER_TC && sp.K == 1 && g.W <= 8;
+    const bool use_tc = (o.gridder == SVDI_GRIDDER_TC || o.gridder == SVDI_GRIDDER_TC_BF16) && sp.K == 1 && g.W <= 8;
     if (use_tc) {
         g.T = kTcTileRows;
         g.ntile = (int)((g.G + g.T - 1) / g.T);
@@ -674,7 +674,7 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
                                     e->kb_offsets.as<unsigned int>(), n_keys, s0 * tiles2,
                                     s1 * tiles2, s0, g, e->poly, e->planes.as<float2>(),
                                     e->tc_status.as<unsigned int>() + 1, e->tc_status.as<unsigned int>(),
-                                    e->sm_count, st));
+                                    e->sm_count, st, o.gridder == SVDI_GRIDDER_TC_BF16));
         } else {
             SVDI_TRY(launch_grid_fp32(e->rec.as<SampleRec>(), need_s ? e->rec_s.as<float>() : nullptr,
                                       e->offsets.as<unsigned int>(), e->chunk_key.as<unsigned int>(),
@@ -855,7 +855,7 @@ int check_options(const svdi_options& o) {
         set_error("tile must be 0, 32 or 64");
         return SVDI_ERR_UNSUPPORTED;
     }
-    if (o.gridder != SVDI_GRIDDER_FP32 && o.gridder != SVDI_GRIDDER_TC) {
+    if (o.gridder != SVDI_GRIDDER_FP32 && o.gridder != SVDI_GRIDDER_TC && o.gridder != SVDI_GRIDDER_TC_BF16) {
         set_error("unknown gridder");
         return SVDI_ERR_INVALID_ARGUMENT;
     }

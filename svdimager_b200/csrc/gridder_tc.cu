@@ -13,12 +13,21 @@
 // (six tcgen05.mma kind::f16, M = 64, N = 32, K = 16; the lo*lo term is below 2^-22 relative).
 //
 // Cost model (measured on B200): a tcgen05.mma of this skinny shape costs about its operand bytes
-// read from shared memory at ~117 B/clk (M = 128, N = 32: 43 clk; M = 64, N = 32: 26 clk), so the
-// accumulator is 64 rows and the operands are built with as few shared-memory wavefronts as
-// possible: both operands are MN-major (8 consecutive rows / columns of one sample form one
-// 16-byte row of a core matrix), and the eight threads of a sample hold the eight footprint
-// positions of its two 8-row chunks after a warp-shuffle rotation, so the stores are contiguous
-// 4-byte pairs and a sample's B column is rewritten in full (no clearing).
+// read from shared memory at ~117 B/clk per SM (M = 64, N = 32: 26 clk), one issuing thread issues
+// at most one every ~46 clk and an mbarrier try_wait costs the issuing thread ~200 clk. Hence M = 64
+// accumulators (56-row tiles), two CTAs per SM (two issuing threads) and one wait per pipeline stage
+// of four K-blocks.
+//
+// Operands. Both are MN-major without swizzle: a core matrix is 8 K (samples) x 16 bytes (8
+// consecutive rows of A or columns of B). One thread builds one sample's column of A and of B: its
+// eight row taps land at rows r0 .. r0 + 7 of the 64-row accumulator, that is in the 8-row chunks
+// r0 / 8 and r0 / 8 + 1 at an offset of r0 % 8. The thread evaluates the taps in order (FP32
+// piecewise polynomials whose coefficients are kernel-parameter constants), packs them into FP16
+// hi and lo half pairs and shifts the 16-half window into place with byte permutes and word
+// selects, so each chunk is one 16-byte store (a warp's stores of one chunk fill four whole
+// shared-memory wavefronts, whatever the samples' rows). B's 16 columns (8 real + 8 imaginary taps
+// of the 8-column tile plus halo) are written in full; of A only the chunks the thread's previous
+// sample in this stage slot covered and the new sample does not are cleared.
 //
 // Tiles. Binning uses 56-row x 8-column tiles (footprint origins). Four consecutive tile keys
 // (the same tile row, 32 consecutive columns) form a super-tile whose running sum lives in TMEM
@@ -34,15 +43,19 @@
 // to one of four 32-column "fresh" accumulators (columns 128..255), which the epilogue warps add
 // into the running block with FP32 round-to-nearest adds once those MMAs are done.
 //
-// Roles (two CTAs per SM, 14 warps, 256 TMEM columns each):
-//   warps 0-7   producers, two groups of 128 threads filling alternate K-blocks (a thread owns two
-//               taps and two footprint positions of one sample); stage s is reused once the MMAs of
-//               its previous K-block commit to empty[s]; every thread arrives on full[s].
-//   warp 8      scheduler: walks the CTA's share of the K-blocks (runs of up to 32 records of one
-//               key) and publishes their descriptors to a ring.
-//   warp 9      MMA issuer: issues the MMAs, opens and closes fresh intervals and posts merge /
+// Roles (two CTAs per SM, 10 warps, 256 TMEM columns each):
+//   warps 0-3   producers: warp w fills sub-stage w of the two pipeline stages in turn with K-blocks
+//               j = w, w + 4, w + 8, ... (one thread per sample); the four warps arrive on
+//               full[stage]; a stage is reused once the MMAs of its previous round commit to
+//               empty[stage].
+//   warp 4      scheduler: walks the CTA's share of the K-blocks (runs of up to 32 records of one
+//               key), publishes their descriptors to a ring and stages each K-block's records
+//               (one contiguous run of 16-byte records) into shared memory with a bulk copy
+//               (cp.async.bulk, this GPU's own memory, no multicast) that completes on the record
+//               slot's mbarrier.
+//   warp 5      MMA issuer: issues the MMAs, opens and closes fresh intervals and posts merge /
 //               flush / exit events.
-//   warps 10-13 epilogue: TMEM lane quarter (warp % 4); merge fresh intervals into the running sum
+//   warps 6-9   epilogue: TMEM lane quarter (warp % 4); merge fresh intervals into the running sum
 //               and flush super-tiles to the moment plane, in event order.
 // The scheduler warps take chunks of 32 K-blocks from a global counter (a chunk can start and end
 // inside a tile; each CTA flushes the super-tiles it touched).
@@ -52,15 +65,16 @@
 // low halves of all but negligible contributions stay normal.
 //
 // Rare samples (exact-integer positions, whose footprint is W + 1 cells wide, and footprints
-// clipped at the low grid edge) skip the matrices: the eight threads of the sample add their
-// exact ES weights to the moment plane directly.
+// clipped at the low grid edge) skip the matrices: their thread adds the exact ES weights to the
+// moment plane directly.
 //
 // Every wait is bounded (about one second of global time); a wait that runs out sets *status and
 // a CTA-wide abort flag that every other wait also watches, so all roles leave their loops, the
-// MMA warp waits (bounded) for its last commit, the tensor memory is freed and the host reports
-// the grid as incomplete.
+// MMA warp waits (bounded) for its last commit, the scheduler for its last record copies, the
+// tensor memory is freed and the host reports the grid as incomplete.
 #include "svdi_internal.cuh"
 
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 namespace svdi {
@@ -70,45 +84,43 @@ namespace {
 constexpr int kKB = kTcKBlock;          // samples per K-block
 constexpr int kM = 64;                  // accumulator rows: tile rows + footprint halo
 constexpr int kN = 32;                  // columns per block: 16 real + 16 imaginary
-constexpr int kLanesPerSample = 4;      // a thread owns two taps / two footprint positions
-constexpr int kGroupThreads = kKB * kLanesPerSample;       // one K-block: 128 threads
-constexpr int kGroups = 2;              // producer groups fill alternate K-blocks
-constexpr int kProdWarps = kGroups * kGroupThreads / 32;  // 8
-constexpr int kSchedWarp = kProdWarps;                     // 8
-constexpr int kMmaWarp = kProdWarps + 1;                   // 9
-constexpr int kEpiWarp0 = kProdWarps + 2;                  // 10..13
+constexpr int kSubStages = 4;           // K-blocks per pipeline stage (one per producer warp)
+constexpr int kPipe = 2;                // pipeline stages
+constexpr int kProdWarps = kSubStages;                     // 4: warp w fills sub-stage w of both stages
+constexpr int kSchedWarp = kProdWarps;                     // 4
+constexpr int kMmaWarp = kProdWarps + 1;                   // 5
+constexpr int kEpiWarp0 = kProdWarps + 2;                  // 6..9
 constexpr int kWarps = kProdWarps + 2 + 4;
-constexpr int kThreads = kWarps * 32;                      // 448
-constexpr int kStages = 8;              // operand sub-stages: one K-block each
-constexpr int kPairs = kStages / 2;     // pipeline stages: two consecutive K-blocks (one per group)
+constexpr int kThreads = kWarps * 32;                      // 320
 constexpr int kFreshBufs = 4;
 constexpr int kFreshKB = 8;             // K-blocks (48 MMAs) per fresh interval at most
 constexpr int kFreshCol0 = kTcBlocks * kN;  // running blocks first, then the fresh buffers
 constexpr int kTmemCols = 256;
-constexpr int kMetaRing = 128;          // published K-block descriptors
+constexpr int kMetaRing = 64;           // published K-block descriptors
+constexpr int kRecSlots = 16;           // record slots: K-blocks staged ahead of the producers
 constexpr int kChunkKB = 32;            // K-blocks per chunk of dynamically distributed work
 constexpr int kEventRing = 64;
 
 constexpr int kABytes = kM * kKB * 2;                    // 4 KB per FP16 A operand
 constexpr int kBBytes = kN * kKB * 2;                    // 2 KB per FP16 B operand
-constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;   // 12 KB
-constexpr int kOldBytes = kStages * kGroupThreads;       // last A chunk written, per stage and thread
-constexpr int kSmemUsed = kStages * kStageBytes + kOldBytes;
+constexpr int kSubBytes = 2 * kABytes + 2 * kBBytes;     // 12 KB: one K-block
+constexpr int kStageBytes = kSubStages * kSubBytes;      // 48 KB
+constexpr int kRecOff = kPipe * kStageBytes;             // record slots after the stages
+constexpr int kRecBytes = kRecSlots * kKB * 16;          // 8 KB
+constexpr int kSmemUsed = kRecOff + kRecBytes;
 // Requested dynamic shared memory: more than a third of the SM's 228 KB, so at most two CTAs share
 // an SM and their 2 x 256 TMEM columns always fit in its 512.
-constexpr int kSmemBytes = 100 * 1024;
-static_assert(kSmemUsed <= kSmemBytes, "shared-memory plan exceeds the request");
+constexpr int kSmemBytes = kSmemUsed;
+static_assert(kSmemBytes > 228 * 1024 / 3 && 2 * (kSmemBytes + 4096) <= 228 * 1024, "two CTAs per SM");
 static_assert(kFreshCol0 + kFreshBufs * kN <= kTmemCols, "TMEM plan exceeds the allocation");
 static_assert(kTcTileRows + 8 <= kM && kTcTileCols + 8 <= 16, "tile + footprint must fit the accumulator");
-static_assert(kGroups == 2 && kStages % 2 == 0, "a pipeline stage holds one K-block of each producer group");
 static_assert(kEpiWarp0 + 4 == kWarps, "four epilogue warps (one per TMEM lane quarter) come last");
+static_assert(kRecSlots <= kMetaRing && kKB == 32, "one record slot per published K-block, one lane per record");
 
 // MN-major, no-swizzle canonical layout of an FP16 operand with kKB K-columns: a core matrix is
 // 8 K-rows x 16 bytes (8 consecutive M or N elements); the next 8 K at +128 bytes (LBO), the next
-// 8 M / N elements at +512 bytes (SBO).
-__device__ __forceinline__ int op_off(int mn, int k) {
-    return (mn & 7) * 2 + (k & 7) * 16 + (k >> 3) * 128 + (mn >> 3) * 512;
-}
+// 8 M / N elements at +512 bytes (SBO). Element (mn, k) sits at byte
+// (mn % 8) * 2 + (k % 8) * 16 + (k / 8) * 128 + (mn / 8) * 512.
 constexpr unsigned long long kDescFixed = ((128ull >> 4) << 16) | ((512ull >> 4) << 32) | (1ull << 46);
 __device__ __forceinline__ unsigned long long smem_desc(uint32_t addr) {
     return (unsigned long long)((addr >> 4) & 0x3FFFu) | kDescFixed;
@@ -116,6 +128,8 @@ __device__ __forceinline__ unsigned long long smem_desc(uint32_t addr) {
 // Instruction descriptor: FP32 accumulator, FP16 A and B, both MN-major, N = 32, M = 64.
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 15) | (1u << 16) | ((uint32_t)(kN >> 3) << 17) |
                             ((uint32_t)(kM >> 4) << 24);
+// The same with BF16 A and B (both operands always have the same type).
+constexpr uint32_t kIdescBf16 = kIdesc | (1u << 7) | (1u << 10);
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -142,6 +156,16 @@ __device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count) {
 }
 __device__ __forceinline__ void mbar_arrive(uint32_t addr) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(addr) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t addr, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(addr), "r"(bytes) : "memory");
+}
+// Bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from this GPU's global
+// memory into this CTA's shared memory, completing on the mbarrier at `mbar` (no multicast).
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(mbar)
+                 : "memory");
 }
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
@@ -178,13 +202,14 @@ __device__ bool wait_at_least(const unsigned int* p, unsigned int target, const 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void mma_f16(uint32_t d_tmem, unsigned long long a, unsigned long long b, uint32_t accum) {
+__device__ __forceinline__ void mma_f16(uint32_t d_tmem, unsigned long long a, unsigned long long b, uint32_t accum,
+                                        uint32_t idesc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
         :
-        : "r"(d_tmem), "l"(a), "l"(b), "r"(kIdesc), "r"(accum)
+        : "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accum)
         : "memory");
 }
 __device__ __forceinline__ void mma_commit(uint32_t mbar) {
@@ -193,41 +218,19 @@ __device__ __forceinline__ void mma_commit(uint32_t mbar) {
 }
 
 // 32 consecutive TMEM columns of this thread's lane.
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
-    uint32_t r[32];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+// 8 consecutive TMEM columns of this thread's lane (the wait is separate: issue several, then wait).
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
 }
-
-__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float (&v)[32]) {
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
-        "{%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, "
-        "%17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(taddr),
-        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
-        "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
-        "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
-        "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
-        "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
-        "r"(__float_as_uint(v[15])), "r"(__float_as_uint(v[16])), "r"(__float_as_uint(v[17])),
-        "r"(__float_as_uint(v[18])), "r"(__float_as_uint(v[19])), "r"(__float_as_uint(v[20])),
-        "r"(__float_as_uint(v[21])), "r"(__float_as_uint(v[22])), "r"(__float_as_uint(v[23])),
-        "r"(__float_as_uint(v[24])), "r"(__float_as_uint(v[25])), "r"(__float_as_uint(v[26])),
-        "r"(__float_as_uint(v[27])), "r"(__float_as_uint(v[28])), "r"(__float_as_uint(v[29])),
-        "r"(__float_as_uint(v[30])), "r"(__float_as_uint(v[31]))
-        : "memory");
-    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&r)[8]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+                 "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+                 : "memory");
 }
+__device__ __forceinline__ void tmem_st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void red_add_v2(float2* addr, float a, float b) {
     asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(addr), "f"(a), "f"(b) : "memory");
@@ -239,13 +242,68 @@ __device__ __forceinline__ float es_exact(float beta, float x) {
     return expf(-beta * x * x / (1.0f + sqrtf((1.0f - x) * (1.0f + x))));
 }
 
-// x0, x1 as FP16 hi + lo pairs packed into two 32-bit words (x0 in the low halves).
-__device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_t& lo) {
-    const __half2 h = __floats2half2_rn(x0, x1);
-    const float2 f = __half22float2(h);
-    const __half2 l = __floats2half2_rn(x0 - f.x, x1 - f.y);
-    hi = *reinterpret_cast<const uint32_t*>(&h);
-    lo = *reinterpret_cast<const uint32_t*>(&l);
+
+// Eight values (taps 0..7) as FP16 (or BF16) hi or lo pairs (x = hi + lo + O(2^-22 x) in FP16,
+// O(2^-17 x) in BF16): word w holds taps 2w (low half) and 2w + 1.
+template <bool kBf16>
+__device__ __forceinline__ uint32_t pack_rn(float a, float b) {
+    if constexpr (kBf16) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+        return *reinterpret_cast<const uint32_t*>(&h);
+    } else {
+        const __half2 h = __floats2half2_rn(a, b);
+        return *reinterpret_cast<const uint32_t*>(&h);
+    }
+}
+template <bool kBf16>
+__device__ __forceinline__ float2 unpack(uint32_t w) {
+    if constexpr (kBf16) {
+        return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w));
+    } else {
+        return __half22float2(*reinterpret_cast<const __half2*>(&w));
+    }
+}
+template <bool kBf16>
+__device__ __forceinline__ void hi8(const float (&x)[8], uint32_t (&hi)[4]) {
+#pragma unroll
+    for (int w = 0; w < 4; ++w) hi[w] = pack_rn<kBf16>(x[2 * w], x[2 * w + 1]);
+}
+template <bool kBf16>
+__device__ __forceinline__ void lo8(const float (&x)[8], uint32_t (&lo)[4]) {
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+        const float2 f = unpack<kBf16>(pack_rn<kBf16>(x[2 * w], x[2 * w + 1]));
+        lo[w] = pack_rn<kBf16>(x[2 * w] - f.x, x[2 * w + 1] - f.y);
+    }
+}
+
+// The 16-half window of two 8-element chunks with taps 0..7 at positions sh .. sh + 7 (0 <= sh < 8)
+// and zeros elsewhere: o[0..3] is the first chunk, o[4..7] the second. A half shift by the low bit
+// of sh (byte permutes), then word shifts by 1 and 2 (selects).
+__device__ __forceinline__ void window16(const uint32_t (&h)[4], int sh, uint32_t (&o)[8]) {
+    const uint32_t sel = (sh & 1) ? 0x5432u : 0x7654u;
+    uint32_t g[5];
+    g[0] = __byte_perm(0u, h[0], sel);
+    g[1] = __byte_perm(h[0], h[1], sel);
+    g[2] = __byte_perm(h[1], h[2], sel);
+    g[3] = __byte_perm(h[2], h[3], sel);
+    g[4] = __byte_perm(h[3], 0u, sel);
+    const bool s1 = (sh & 2) != 0, s2 = (sh & 4) != 0;
+    uint32_t u[6];
+    u[0] = s1 ? 0u : g[0];
+#pragma unroll
+    for (int w = 1; w < 5; ++w) u[w] = s1 ? g[w - 1] : g[w];
+    u[5] = s1 ? g[4] : 0u;
+    o[0] = s2 ? 0u : u[0];
+    o[1] = s2 ? 0u : u[1];
+#pragma unroll
+    for (int w = 2; w < 6; ++w) o[w] = s2 ? u[w - 2] : u[w];
+    o[6] = s2 ? u[4] : 0u;
+    o[7] = s2 ? u[5] : 0u;
+}
+
+__device__ __forceinline__ void st_chunk(unsigned char* p, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+    *reinterpret_cast<uint4*>(p) = make_uint4(a, b, c, d);
 }
 
 struct KBMeta {
@@ -275,14 +333,15 @@ struct TcParams {
 };
 
 struct __align__(8) TcShared {
-    unsigned long long full[kPairs];      // producers -> MMA: both K-blocks of the stage written
-    unsigned long long empty[kPairs];     // MMA -> producers: stage read (tcgen05.commit)
+    unsigned long long full[kPipe];       // producers -> MMA: the stage's K-blocks written (4 warp arrivals)
+    unsigned long long empty[kPipe];      // MMA -> producers: stage read (tcgen05.commit)
+    unsigned long long rec_full[kRecSlots];  // scheduler's bulk copy -> producers: records staged
     unsigned long long fdone[kFreshBufs]; // MMA -> epilogue: fresh interval's MMAs done (commit)
     unsigned long long ffree[kFreshBufs]; // epilogue -> MMA: fresh buffer merged (4 warp arrivals)
     KBMeta meta[kMetaRing];
     Event events[kEventRing];
     unsigned int published;               // K-block descriptors published
-    unsigned int consumed;                // K-blocks whose descriptor the MMA warp and producers are done with
+    unsigned int consumed;                // K-blocks whose descriptor and records everyone is done with
     unsigned int sched_done;              // 1 + total K-blocks once the schedule is complete
     unsigned int ev_published;
     unsigned int ev_consumed[4];
@@ -290,16 +349,19 @@ struct __align__(8) TcShared {
     uint32_t tmem_base;
 };
 
+
+template <bool kBf16>
 __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g, EsPoly poly) {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ TcShared S;
-    signed char* oldchunk = reinterpret_cast<signed char*>(smem + kStages * kStageBytes);
+    const SampleRec* recs = reinterpret_cast<const SampleRec*>(smem + kRecOff);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int W = g.W, HW = W / 2;
     const int tiles2 = g.ntile * g.ntile2;
     const long long GG = g.G * g.G;
     volatile int* abort_flag = &S.abort;
+    const uint32_t idesc = kBf16 ? kIdescBf16 : kIdesc;
 
     // ---- set-up: tensor memory, barriers, the CTA's record range
     if (warp == kMmaWarp) {
@@ -311,10 +373,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
     // the K-blocks of keys [key_lo, key_hi), handed out in chunks by the scheduler warps
     const unsigned int kb_lo = P.kb_offsets[P.key_lo], kb_hi = P.kb_offsets[P.key_hi];
     if (tid == 0) {
-        for (int s = 0; s < kPairs; ++s) {
-            mbar_init(smem_u32(&S.full[s]), kGroups * kGroupThreads);
+        for (int s = 0; s < kPipe; ++s) {
+            mbar_init(smem_u32(&S.full[s]), kSubStages);
             mbar_init(smem_u32(&S.empty[s]), 1);
         }
+        for (int s = 0; s < kRecSlots; ++s) mbar_init(smem_u32(&S.rec_full[s]), 1);
         for (int b = 0; b < kFreshBufs; ++b) {
             mbar_init(smem_u32(&S.fdone[b]), 1);
             mbar_init(smem_u32(&S.ffree[b]), 4);
@@ -327,9 +390,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
         for (int q = 0; q < 4; ++q) S.ev_consumed[q] = 0;
         S.abort = 0;
     }
-    for (int i = tid; i < kStages * kStageBytes / 16; i += kThreads)
+    for (int i = tid; i < kPipe * kStageBytes / 16; i += kThreads)
         reinterpret_cast<uint4*>(smem)[i] = make_uint4(0, 0, 0, 0);
-    for (int i = tid; i < kOldBytes; i += kThreads) oldchunk[i] = -1;
     // FP16 operand scale from max |v| over all records
     float vscale = 0.0f;
     {
@@ -349,35 +411,29 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
 
     if (warp < kProdWarps) {
         // =========================== producers ===========================
-        const int grp = warp / (kGroupThreads / 32);
-        const int gtid = tid % kGroupThreads;
-        const int slot = gtid / kLanesPerSample, t = gtid % kLanesPerSample;
-        const int lane0 = lane & ~(kLanesPerSample - 1);  // first lane of this sample's four
-        const int q0 = 2 * t, q1 = 2 * t + 1;             // this thread's taps and positions
-        float cf0[kPolyDeg + 1], cf1[kPolyDeg + 1];
-#pragma unroll
-        for (int d = 0; d <= kPolyDeg; ++d) {
-            cf0[d] = poly.c[q0][d];
-            cf1[d] = poly.c[q1][d];
-        }
-        // operand byte offset of positions (q0, q1) of chunk 0 in K-slot `slot`; chunk c adds 512 c
-        const int pbase = op_off(q0, slot);
-        // record prefetch queue: the records of this group's next two K-blocks (tag = K-block)
-        SampleRec preA = {0, 0, 0.0f, 0.0f}, preB = {0, 0, 0.0f, 0.0f};
-        int tagA = -1, tagB = -1;
+        // warp -> sub-stage; lane -> sample (K-slot) of the K-block; round `it` uses stage it % 2
+        const int kofs = (lane & 7) * 16 + (lane >> 3) * 128;  // byte offset of this K-slot's 16-byte row
+        int oldj0 = -1, oldj1 = -1;  // first A chunk of this lane's previous sample per stage (-1: none)
         int pub_seen = 0;  // lane 0: published count last read (acquire)
+        bool failed = false;
         for (int it = 0;; ++it) {
-            const int j = it * kGroups + grp;
+            const int j = it * kProdWarps + warp;
+            const int stg = it & 1;
+            const int use = it >> 1;  // earlier rounds of this stage
+            unsigned char* const A_hi = smem + stg * kStageBytes + warp * kSubBytes;
+            unsigned char* const A_lo = A_hi + kABytes;
+            unsigned char* const B_hi = A_lo + kABytes;
+            unsigned char* const B_lo = B_hi + kBBytes;
             // wait until K-block j is published or the schedule ends before it (warp-uniform)
-            int state = 0, pub = 0;  // state 1: produce, 0: done, -1: abort
+            int state = 0;  // 1: produce, 0: done, -1: give up
+            unsigned int sdv = 0;
             if (lane == 0) {
                 const unsigned long long t0 = global_ns();
                 for (unsigned int n = 0;; ++n) {
-                    if (pub_seen <= j + 2 * kGroups) pub_seen = (int)ld_acquire(&S.published);
-                    pub = pub_seen;
-                    if (pub > j) { state = 1; break; }
-                    const unsigned int sd = ld_acquire(&S.sched_done);
-                    if (sd && (unsigned int)j >= sd - 1) { state = 0; break; }
+                    if (pub_seen <= j) pub_seen = (int)ld_acquire(&S.published);
+                    if (pub_seen > j) { state = 1; break; }
+                    sdv = ld_acquire(&S.sched_done);
+                    if (sdv && (unsigned int)j >= sdv - 1) { state = 0; break; }
                     if ((n & 63u) == 0 && (*abort_flag || global_ns() - t0 > 1000000000ull)) {
                         state = -1;
                         break;
@@ -386,140 +442,44 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
                 }
             }
             state = __shfl_sync(0xffffffffu, state, 0);
-            pub = __shfl_sync(0xffffffffu, pub, 0);
-            // pipeline stage of K-block j: pair j / 2 (the other group fills the other half)
-            const int pr = (j >> 1) % kPairs, u = (j >> 1) / kPairs;
-            const int s = 2 * pr + grp;  // this K-block's sub-stage
-            if (state == 0 && (j & 1)) {
-                // the schedule ends at K-block j - 1, the first half of this stage: complete the
-                // stage's arrival count (after the stage is free, so the arrivals count for this use)
-                unsigned int sd = 0;
-                if (lane == 0) sd = ld_acquire(&S.sched_done);
-                sd = __shfl_sync(0xffffffffu, sd, 0);
-                if (sd && (unsigned int)j == sd - 1) {
+            if (state == 0) {
+                // the schedule holds T = sdv - 1 K-blocks: when a stage-mate has one in this round, this
+                // warp still arrives (after the stage is free, so the arrival counts for this use)
+                const unsigned int T = __shfl_sync(0xffffffffu, sdv, 0) - 1;
+                if ((unsigned int)(it * kProdWarps) < T) {
                     bool ok = true;
-                    if (u > 0) ok = mbar_wait(smem_u32(&S.empty[pr]), (uint32_t)((u - 1) & 1), abort_flag);
-                    if (__all_sync(0xffffffffu, ok)) mbar_arrive(smem_u32(&S.full[pr]));
-                }
-            }
-            if (state <= 0) {
-                if (state < 0 && lane == 0 && !*abort_flag) {
-                    atomicOr(P.status, 1u);
-                    *abort_flag = 1;
+                    if (use > 0) ok = mbar_wait(smem_u32(&S.empty[stg]), (uint32_t)((use - 1) & 1), abort_flag);
+                    if (__all_sync(0xffffffffu, ok)) {
+                        if (lane == 0) mbar_arrive(smem_u32(&S.full[stg]));
+                    } else {
+                        failed = true;
+                    }
                 }
                 break;
             }
-            const KBMeta m = S.meta[j % kMetaRing];
-            // record of this thread's sample (the four threads of a sample load the same 16 bytes)
-            const bool valid = slot < m.cnt;
-            SampleRec r = {0, 0, 0.0f, 0.0f};
-            if (valid) r = (tagA == j) ? preA : P.rec[m.pos + slot];
-            {  // advance the queue; load the records of K-block j + 2 kGroups if it is published
-                preA = preB;
-                tagA = tagB;
-                const int jn = j + 2 * kGroups;
-                tagB = -1;
-                if (pub > jn) {
-                    const KBMeta mn = S.meta[jn % kMetaRing];
-                    if (slot < mn.cnt) preB = P.rec[mn.pos + slot];
-                    tagB = jn;
-                }
+            if (state < 0) {
+                failed = true;
+                break;
             }
+            const KBMeta m = S.meta[j % kMetaRing];
+            // this K-block's records, staged by the scheduler's bulk copy
+            const int slot = j % kRecSlots;
+            bool ok = mbar_wait(smem_u32(&S.rec_full[slot]), (uint32_t)((j / kRecSlots) & 1), abort_flag);
+            // the stage slot: the MMAs of its previous round must be done with it
+            if (ok && use > 0) ok = mbar_wait(smem_u32(&S.empty[stg]), (uint32_t)((use - 1) & 1), abort_flag);
+            if (!__all_sync(0xffffffffu, ok)) {
+                failed = true;
+                break;
+            }
+            const bool valid = lane < m.cnt;
+            SampleRec r = {0, 0, 0.0f, 0.0f};
+            if (valid) r = recs[slot * kKB + lane];
             const int cx = r.xq >> 24, cy = r.yq >> 24;
             const int fxq = r.xq & 0xFFFFFF, fyq = r.yq & 0xFFFFFF;
             const int r0 = cx - (HW - 1), c0 = cy - (HW - 1);
             const bool rare = valid && (fxq == 0 || fyq == 0 || r0 < 0 || c0 < 0 || r0 >= g.T || c0 >= g.T2);
             const bool fast = valid && !rare;
-            float wx0, wx1, wy0, wy1;
-            {
-                const float ux = fmaf(2.0f, (float)fxq * (1.0f / 16777216.0f), -1.0f);
-                const float uy = fmaf(2.0f, (float)fyq * (1.0f / 16777216.0f), -1.0f);
-                wx0 = cf0[kPolyDeg]; wx1 = cf1[kPolyDeg];
-                wy0 = cf0[kPolyDeg]; wy1 = cf1[kPolyDeg];
-#pragma unroll
-                for (int d = kPolyDeg - 1; d >= 0; --d) {
-                    wx0 = fmaf(wx0, ux, cf0[d]);
-                    wx1 = fmaf(wx1, ux, cf1[d]);
-                    wy0 = fmaf(wy0, uy, cf0[d]);
-                    wy1 = fmaf(wy1, uy, cf1[d]);
-                }
-            }
-            // rotation: footprint position q of the 16 rows (columns) from the 8-aligned chunk below
-            // r0 (c0) holds tap (q - shift) & 7, in chunk 0 if q >= shift, else in chunk 1
-            const int sr = fast ? (r0 & 7) : 0, sc = fast ? c0 : 0;
-            float vx0, vx1, vy0, vy1;
-            {
-                auto rot = [&](float w0, float w1, int sh, float& v0, float& v1) {
-                    const int tau = (q0 - sh) & 7;  // tap at position q0; q1 holds tau + 1
-                    const bool odd = tau & 1;
-                    const int srcA = lane0 + (tau >> 1), srcB = lane0 + (((tau >> 1) + 1) & 3);
-                    const float p = __shfl_sync(0xffffffffu, w0, odd ? srcB : srcA);
-                    const float q = __shfl_sync(0xffffffffu, w1, srcA);
-                    v0 = odd ? q : p;
-                    v1 = odd ? p : q;
-                };
-                rot(wx0, wx1, sr, vx0, vx1);
-                rot(wy0, wy1, sc, vy0, vy1);
-            }
-            // stage reuse: the MMAs of K-block j - kStages must be done with it (warp-uniform)
-            bool ok = true;
-            if (u > 0) ok = mbar_wait(smem_u32(&S.empty[pr]), (uint32_t)((u - 1) & 1), abort_flag);
-            ok = __all_sync(0xffffffffu, ok);
-            if (!ok) {
-                if (lane == 0 && !*abort_flag) {
-                    atomicOr(P.status, 1u);
-                    *abort_flag = 1;
-                }
-                break;
-            }
-            unsigned char* A_hi = smem + s * kStageBytes;
-            unsigned char* A_lo = A_hi + kABytes;
-            unsigned char* B_hi = A_lo + kABytes;
-            unsigned char* B_lo = B_hi + kBBytes;
-            // A: clear this thread's pair in the previous sample's chunks the new one does not cover
-            const int j0 = fast ? (r0 >> 3) : -8;
-            const int oj = oldchunk[s * kGroupThreads + gtid];
-            if (oj >= 0) {
-#pragma unroll
-                for (int d = 0; d < 2; ++d) {
-                    const int cj = oj + d;
-                    if (cj != j0 && cj != j0 + 1) {
-                        *reinterpret_cast<uint32_t*>(A_hi + pbase + cj * 512) = 0u;
-                        *reinterpret_cast<uint32_t*>(A_lo + pbase + cj * 512) = 0u;
-                    }
-                }
-            }
-            oldchunk[s * kGroupThreads + gtid] = (signed char)(fast ? j0 : -1);
-            const bool up0 = q0 < sr, up1 = q1 < sr;  // position in chunk j0 + 1
-            if (fast) {
-                const float a0 = 256.0f * vx0, a1 = 256.0f * vx1;
-                uint32_t h, l;
-                split2(up0 ? 0.0f : a0, up1 ? 0.0f : a1, h, l);
-                *reinterpret_cast<uint32_t*>(A_hi + pbase + j0 * 512) = h;
-                *reinterpret_cast<uint32_t*>(A_lo + pbase + j0 * 512) = l;
-                split2(up0 ? a0 : 0.0f, up1 ? a1 : 0.0f, h, l);
-                *reinterpret_cast<uint32_t*>(A_hi + pbase + (j0 + 1) * 512) = h;
-                *reinterpret_cast<uint32_t*>(A_lo + pbase + (j0 + 1) * 512) = l;
-            }
-            {  // B: all four 8-column chunks of this sample's column, every time
-                const float wv0 = fast ? vy0 * vscale : 0.0f, wv1 = fast ? vy1 * vscale : 0.0f;
-                const bool cu0 = q0 < sc, cu1 = q1 < sc;  // column position in chunk 1
-                const float re0 = wv0 * r.vre, re1 = wv1 * r.vre, im0 = wv0 * r.vim, im1 = wv1 * r.vim;
-                uint32_t h, l;
-                split2(cu0 ? 0.0f : re0, cu1 ? 0.0f : re1, h, l);
-                *reinterpret_cast<uint32_t*>(B_hi + pbase) = h;
-                *reinterpret_cast<uint32_t*>(B_lo + pbase) = l;
-                split2(cu0 ? re0 : 0.0f, cu1 ? re1 : 0.0f, h, l);
-                *reinterpret_cast<uint32_t*>(B_hi + pbase + 512) = h;
-                *reinterpret_cast<uint32_t*>(B_lo + pbase + 512) = l;
-                split2(cu0 ? 0.0f : im0, cu1 ? 0.0f : im1, h, l);
-                *reinterpret_cast<uint32_t*>(B_hi + pbase + 1024) = h;
-                *reinterpret_cast<uint32_t*>(B_lo + pbase + 1024) = l;
-                split2(cu0 ? im0 : 0.0f, cu1 ? im1 : 0.0f, h, l);
-                *reinterpret_cast<uint32_t*>(B_hi + pbase + 1536) = h;
-                *reinterpret_cast<uint32_t*>(B_lo + pbase + 1536) = l;
-            }
-            if (rare) {  // exact ES weights straight to the moment plane; the 4 threads over cells
+            if (rare) {  // exact ES weights straight to the moment plane
                 const int slab = m.key / tiles2;
                 const int t1 = (m.key / g.ntile2) % g.ntile, t2 = m.key % g.ntile2;
                 const long long o1 = g.gmin + (long long)t1 * g.T, o2 = g.gmin + (long long)t2 * g.T2;
@@ -527,7 +487,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
                 const int lo_c = fyq ? c0 : cy - HW, nc = fyq ? W : W + 1;
                 const float px = (float)fxq * (1.0f / 16777216.0f), py = (float)fyq * (1.0f / 16777216.0f);
                 float2* plane = P.planes + (long long)(slab - P.slab_lo) * GG;
-                for (int cidx = t; cidx < nr * nc; cidx += kLanesPerSample) {
+                for (int cidx = 0; cidx < nr * nc; ++cidx) {
                     const int rr = lo_r + cidx / nc, cc = lo_c + cidx % nc;
                     const long long g1 = o1 + rr, g2 = o2 + cc;
                     if (g1 < g.gmin || g2 < g.gmin || g1 > g.gmax || g2 > g.gmax) continue;
@@ -538,8 +498,81 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
                     red_add_v2(plane + (g1 - g.gmin) * g.G + (g2 - g.gmin), sg * r.vre, sg * r.vim);
                 }
             }
+            // ---- A: row taps (256 wx), chunks j0 and j0 + 1 at offset r0 % 8
+            {
+                const float ux = fmaf(2.0f, (float)fxq * (1.0f / 16777216.0f), -1.0f);
+                float a[8];
+#pragma unroll
+                for (int t = 0; t < 8; ++t) {
+                    float w = poly.c[t][kPolyDeg];
+#pragma unroll
+                    for (int d = kPolyDeg - 1; d >= 0; --d) w = fmaf(w, ux, poly.c[t][d]);
+                    a[t] = 256.0f * w;
+                }
+                const int j0 = fast ? (r0 >> 3) : -8;
+                const int oldj = stg ? oldj1 : oldj0;
+                if (oldj >= 0) {  // clear the previous sample's chunks the new one does not cover
+#pragma unroll
+                    for (int d = 0; d < 2; ++d) {
+                        const int cj = oldj + d;
+                        if (cj != j0 && cj != j0 + 1) {
+                            st_chunk(A_hi + kofs + cj * 512, 0u, 0u, 0u, 0u);
+                            st_chunk(A_lo + kofs + cj * 512, 0u, 0u, 0u, 0u);
+                        }
+                    }
+                }
+                if (fast) {
+                    uint32_t h[4], o[8];
+                    hi8<kBf16>(a, h);
+                    window16(h, r0 & 7, o);
+                    st_chunk(A_hi + kofs + j0 * 512, o[0], o[1], o[2], o[3]);
+                    st_chunk(A_hi + kofs + j0 * 512 + 512, o[4], o[5], o[6], o[7]);
+                    lo8<kBf16>(a, h);
+                    window16(h, r0 & 7, o);
+                    st_chunk(A_lo + kofs + j0 * 512, o[0], o[1], o[2], o[3]);
+                    st_chunk(A_lo + kofs + j0 * 512 + 512, o[4], o[5], o[6], o[7]);
+                }
+                if (stg) oldj1 = fast ? j0 : -1;
+                else oldj0 = fast ? j0 : -1;
+            }
+            // ---- B: column taps times the visibility (real: chunks 0-1, imaginary: chunks 2-3)
+            {
+                const float uy = fmaf(2.0f, (float)fyq * (1.0f / 16777216.0f), -1.0f);
+                float wy[8];
+#pragma unroll
+                for (int t = 0; t < 8; ++t) {
+                    float w = poly.c[t][kPolyDeg];
+#pragma unroll
+                    for (int d = kPolyDeg - 1; d >= 0; --d) w = fmaf(w, uy, poly.c[t][d]);
+                    wy[t] = fast ? w * vscale : 0.0f;
+                }
+                const int sc = fast ? c0 : 0;
+#pragma unroll
+                for (int part = 0; part < 2; ++part) {
+                    const float v = part ? r.vim : r.vre;
+                    float b[8];
+#pragma unroll
+                    for (int t = 0; t < 8; ++t) b[t] = wy[t] * v;
+                    uint32_t h[4], o[8];
+                    unsigned char* bh = B_hi + kofs + part * 1024;
+                    unsigned char* bl = B_lo + kofs + part * 1024;
+                    hi8<kBf16>(b, h);
+                    window16(h, sc, o);
+                    st_chunk(bh, o[0], o[1], o[2], o[3]);
+                    st_chunk(bh + 512, o[4], o[5], o[6], o[7]);
+                    lo8<kBf16>(b, h);
+                    window16(h, sc, o);
+                    st_chunk(bl, o[0], o[1], o[2], o[3]);
+                    st_chunk(bl + 512, o[4], o[5], o[6], o[7]);
+                }
+            }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            mbar_arrive(smem_u32(&S.full[pr]));
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&S.full[stg]));
+        }
+        if (failed && lane == 0 && !*abort_flag) {
+            atomicOr(P.status, 1u);
+            *abort_flag = 1;
         }
     } else if (warp == kSchedWarp) {
         // ============================ scheduler ============================
@@ -601,7 +634,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
                 const int key = kc + ci;
                 while (remaining && published < target && m_in_key < nkb) {
                     const unsigned int pos = ka + (unsigned int)kKB * m_in_key;
-                    if (lane == 0) S.meta[published % kMetaRing] = KBMeta{key, pos, (int)min((unsigned int)kKB, kend - pos)};
+                    const unsigned int cnt = min((unsigned int)kKB, kend - pos);
+                    if (lane == 0) {
+                        S.meta[published % kMetaRing] = KBMeta{key, pos, (int)cnt};
+                        // stage the K-block's records: one contiguous run of 16-byte records
+                        const uint32_t bar = smem_u32(&S.rec_full[published % kRecSlots]);
+                        mbar_arrive_expect_tx(bar, cnt * 16u);
+                        bulk_g2s(smem_u32(smem + kRecOff + (published % kRecSlots) * kKB * 16), P.rec + pos,
+                                 cnt * 16u, bar);
+                    }
                     ++published;
                     ++m_in_key;
                     --remaining;
@@ -640,11 +681,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
             have_key = false;
             fetch(kc, off_l, kbo_l, off_e, kbo_e);
             fetch(kc + 32, noff_l, nkbo_l, noff_e, nkbo_e);
-            while (remaining) {  // keep the ring full: up to kMetaRing descriptors ahead of the MMA warp
+            while (remaining) {  // keep the record slots full: up to kRecSlots K-blocks ahead of consumption
                 int cons = 0;
                 if (lane == 0) cons = (int)ld_acquire(&S.consumed);
                 cons = __shfl_sync(0xffffffffu, cons, 0);
-                schedule_to((unsigned int)cons + kMetaRing);
+                schedule_to((unsigned int)cons + kRecSlots);
                 if (!remaining) break;
                 if (lane == 0) ok = wait_at_least(&S.consumed, (unsigned int)cons + 1, abort_flag);
                 ok = __shfl_sync(0xffffffffu, (int)ok, 0);
@@ -653,6 +694,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
             if (!ok) break;
         }
         if (ok && lane == 0) st_release(&S.sched_done, published + 1);
+        // no record copy of this CTA may still be in flight when it exits: wait for the last copy of
+        // every slot (the producers normally consumed them all already)
+        if (lane == 0) {
+            const volatile int never = 0;
+            for (unsigned int s = 0; s < (unsigned int)kRecSlots && s < published; ++s) {
+                const unsigned int uses = (published - s + kRecSlots - 1) / kRecSlots;
+                if (!mbar_wait(smem_u32(&S.rec_full[s]), (uint32_t)((uses - 1) & 1u), &never)) atomicOr(P.status, 16u);
+            }
+        }
     } else if (warp == kMmaWarp) {
         // ============================ MMA issuer ============================
         // MMA / interval / event state (lane 0)
@@ -664,8 +714,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
         unsigned int ev_n = 0;
         int last_commit_stage = -1;
         unsigned int last_commit_parity = 0;
-        int open_pair = -1;  // stage whose second K-block never came (end of the schedule)
-        unsigned int open_pair_parity = 0;
+        int open_stage = -1;  // stage whose last K-blocks never came (end of the schedule)
+        unsigned int open_stage_parity = 0;
         bool failed = false;
         unsigned int ev_free_seen = 0;  // events consumed by every epilogue warp, last read
         auto push_event = [&](Event ev) {  // lane 0
@@ -739,35 +789,35 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
                     ob = b;
                     oc = c;
                 }
-                const int pr = (int)((i >> 1) % kPairs);
-                const unsigned int u = (i >> 1) / kPairs;
-                const int s = 2 * pr + (int)(i & 1u);  // sub-stage of K-block i
-                // one wait per stage (two K-blocks): a try_wait costs the issuing thread ~200 clk
-                if (!failed && (i & 1u) == 0 && !mbar_wait(smem_u32(&S.full[pr]), u & 1u, abort_flag)) failed = true;
-                // producers and this warp are done with meta[<= i]; tell the scheduler every 8 K-blocks
-                if (!failed && (i & 7u) == 7u) st_release(&S.consumed, i + 1);
+                const int stg = (int)((i / kSubStages) % kPipe);
+                const unsigned int u = i / (kSubStages * kPipe);
+                const int sub = (int)(i % kSubStages);  // sub-stage of K-block i
+                // one wait per stage (four K-blocks): a try_wait costs the issuing thread ~200 clk
+                if (!failed && sub == 0 && !mbar_wait(smem_u32(&S.full[stg]), u & 1u, abort_flag)) failed = true;
+                // producers and this warp are done with the descriptors and records of K-blocks <= i
+                if (!failed && sub == kSubStages - 1) st_release(&S.consumed, i + 1);
                 if (!failed) {
                     tc_fence_after();
                     const uint32_t d = tmem + (uint32_t)(kFreshCol0 + kN * ob);
-                    const uint32_t ah = smem_u32(smem + s * kStageBytes), al = ah + kABytes;
+                    const uint32_t ah = smem_u32(smem + stg * kStageBytes + sub * kSubBytes), al = ah + kABytes;
                     const uint32_t bh = al + kABytes, bl = bh + kBBytes;
                     uint32_t acc = on > 0 ? 1u : 0u;
 #pragma unroll
                     for (int k = 0; k < kKB / 16; ++k) {  // 16-element K steps: 2 K-groups = +256 bytes
                         const uint32_t ko = (uint32_t)k * 256u;
-                        mma_f16(d, smem_desc(ah + ko), smem_desc(bh + ko), acc);
+                        mma_f16(d, smem_desc(ah + ko), smem_desc(bh + ko), acc, idesc);
                         acc = 1u;
-                        mma_f16(d, smem_desc(ah + ko), smem_desc(bl + ko), 1u);
-                        mma_f16(d, smem_desc(al + ko), smem_desc(bh + ko), 1u);
+                        mma_f16(d, smem_desc(ah + ko), smem_desc(bl + ko), 1u, idesc);
+                        mma_f16(d, smem_desc(al + ko), smem_desc(bh + ko), 1u, idesc);
                     }
-                    if (i & 1u) {  // both K-blocks of the stage issued
-                        mma_commit(smem_u32(&S.empty[pr]));
-                        last_commit_stage = pr;
+                    if (sub == kSubStages - 1) {  // all K-blocks of the stage issued
+                        mma_commit(smem_u32(&S.empty[stg]));
+                        last_commit_stage = stg;
                         last_commit_parity = u & 1u;
-                        open_pair = -1;
+                        open_stage = -1;
                     } else {
-                        open_pair = pr;
-                        open_pair_parity = u & 1u;
+                        open_stage = stg;
+                        open_stage_parity = u & 1u;
                     }
                     ++on;
                 }
@@ -779,10 +829,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
             if (__shfl_sync(0xffffffffu, (int)failed, 0) || *abort_flag) break;
         }
         if (lane == 0) {
-            if (open_pair >= 0) {
-                mma_commit(smem_u32(&S.empty[open_pair]));
-                last_commit_stage = open_pair;
-                last_commit_parity = open_pair_parity;
+            if (open_stage >= 0) {
+                mma_commit(smem_u32(&S.empty[open_stage]));
+                last_commit_stage = open_stage;
+                last_commit_parity = open_stage_parity;
             }
             if (!failed && !*abort_flag && cur_st >= 0) {
                 close_interval();
@@ -829,16 +879,23 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
                     break;
                 }
                 tc_fence_after();
-                float f[32];
-                tmem_ld32(tmem + lane_addr + (uint32_t)(kFreshCol0 + kN * ev.buf), f);
+                const uint32_t fa = tmem + lane_addr + (uint32_t)(kFreshCol0 + kN * ev.buf);
                 const uint32_t ra = tmem + lane_addr + (uint32_t)(kN * ev.blk);
-                if ((run_valid >> ev.blk) & 1u) {
-                    float rv[32];
-                    tmem_ld32(ra, rv);
+                const bool have_run = (run_valid >> ev.blk) & 1u;
+#pragma unroll 1
+                for (int c8 = 0; c8 < kN; c8 += 8) {  // eight columns at a time
+                    uint32_t f[8], rv[8];
+                    tmem_ld8(fa + (uint32_t)c8, f);
+                    if (have_run) tmem_ld8(ra + (uint32_t)c8, rv);
+                    tmem_ld_wait();
+                    if (have_run) {
 #pragma unroll
-                    for (int jj = 0; jj < 32; ++jj) f[jj] += rv[jj];  // FP32 round-to-nearest
+                        for (int jj = 0; jj < 8; ++jj)  // FP32 round-to-nearest
+                            f[jj] = __float_as_uint(__uint_as_float(f[jj]) + __uint_as_float(rv[jj]));
+                    }
+                    tmem_st8(ra + (uint32_t)c8, f);
                 }
-                tmem_st32(ra, f);
+                tmem_st_wait();
                 run_valid |= 1u << ev.blk;
                 tc_fence_before();
                 __syncwarp();
@@ -864,18 +921,29 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
                 };
 #pragma unroll 1
                 for (int c = 0; c < kTcBlocks; ++c) {
-                    float v[32];
-                    if ((run_valid >> c) & 1u) {
-                        tmem_ld32(tmem + lane_addr + (uint32_t)(kN * c), v);
-                    } else {
+                    // block c: columns 0..7 real / 16..23 imaginary overlap the carry of block c - 1;
+                    // columns 8..15 / 24..31 become the carry
+                    uint32_t re[8], im[8];
+                    const bool have = (run_valid >> c) & 1u;
+                    const uint32_t ba = tmem + lane_addr + (uint32_t)(kN * c);
+                    if (have) {
+                        tmem_ld8(ba, re);
+                        tmem_ld8(ba + 16u, im);
+                        tmem_ld_wait();
+                    }
 #pragma unroll
-                        for (int jj = 0; jj < 32; ++jj) v[jj] = 0.0f;
+                    for (int jj = 0; jj < 8; ++jj)
+                        emit(o2 + 8 * c + jj, cre[jj] + (have ? __uint_as_float(re[jj]) : 0.0f),
+                             cim[jj] + (have ? __uint_as_float(im[jj]) : 0.0f));
+                    if (have) {
+                        tmem_ld8(ba + 8u, re);
+                        tmem_ld8(ba + 24u, im);
+                        tmem_ld_wait();
                     }
 #pragma unroll
                     for (int jj = 0; jj < 8; ++jj) {
-                        emit(o2 + 8 * c + jj, cre[jj] + v[jj], cim[jj] + v[16 + jj]);
-                        cre[jj] = v[8 + jj];
-                        cim[jj] = v[24 + jj];
+                        cre[jj] = have ? __uint_as_float(re[jj]) : 0.0f;
+                        cim[jj] = have ? __uint_as_float(im[jj]) : 0.0f;
                     }
                 }
 #pragma unroll
@@ -903,7 +971,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
 int launch_grid_tc(const SampleRec* d_rec, const unsigned int* d_offsets, const unsigned int* d_kb_offsets,
                    int n_keys, int key_lo, int key_hi, int slab_lo, const GridGeom& g, const EsPoly& poly,
                    float2* d_planes, const unsigned int* d_vmax, unsigned int* d_status, int sm_count,
-                   cudaStream_t st) {
+                   cudaStream_t st, bool bf16) {
     if (key_lo < 0 || key_hi > n_keys || key_lo >= key_hi) {
         set_error("tensor-core gridder: bad key range");
         return SVDI_ERR_INTERNAL;
@@ -913,9 +981,14 @@ int launch_grid_tc(const SampleRec* d_rec, const unsigned int* d_offsets, const 
         set_error("tensor-core gridder: needs even support <= 8 and 56 x 8 tiles in groups of 4");
         return SVDI_ERR_UNSUPPORTED;
     }
-    SVDI_TRY(ensure_dynamic_smem((const void*)k_grid_tc, kSmemBytes, true));
+    if (reinterpret_cast<uintptr_t>(d_rec) % 16 != 0) {
+        set_error("tensor-core gridder: records must be 16-byte aligned");
+        return SVDI_ERR_INTERNAL;
+    }
+    auto kern = bf16 ? k_grid_tc<true> : k_grid_tc<false>;
+    SVDI_TRY(ensure_dynamic_smem((const void*)kern, kSmemBytes, true));
     int per_sm = 0;
-    SVDI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grid_tc, kThreads, kSmemBytes));
+    SVDI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, kSmemBytes));
     if (per_sm < 1) {
         set_error("tensor-core gridder: kernel does not fit on an SM");
         return SVDI_ERR_UNSUPPORTED;
@@ -924,8 +997,9 @@ int launch_grid_tc(const SampleRec* d_rec, const unsigned int* d_offsets, const 
     SVDI_CUDA(cudaMemsetAsync(d_status + 2, 0, sizeof(unsigned int), st));
     TcParams P{d_rec, d_offsets, d_kb_offsets, d_vmax, d_planes, d_status, d_status + 2, key_lo, key_hi, slab_lo};
     // two CTAs per SM (two MMA-issuing threads: one thread issues a skinny MMA every ~46 clk, the
-    // tensor pipe takes one every ~26), each with 256 of the SM's 512 TMEM columns
-    k_grid_tc<<<2 * sm_count, kThreads, kSmemBytes, st>>>(P, g, poly);
+    // tensor pipe takes one every ~26), each with 256 of the SM's 512 TMEM columns; the records must
+    // start 16-byte aligned for the bulk copies
+    kern<<<2 * sm_count, kThreads, kSmemBytes, st>>>(P, g, poly);
     SVDI_LAUNCHED();
     return SVDI_OK;
 }

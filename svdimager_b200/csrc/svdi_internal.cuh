@@ -215,7 +215,7 @@ constexpr int kTcKBlock = 32;      // records per K-block (one MMA pair of K ste
 int launch_grid_tc(const SampleRec* d_rec, const unsigned int* d_offsets, const unsigned int* d_kb_offsets,
                    int n_keys, int key_lo, int key_hi, int slab_lo, const GridGeom& g, const EsPoly& poly,
                    float2* d_planes, const unsigned int* d_vmax, unsigned int* d_status, int sm_count,
-                   cudaStream_t st);
+                   cudaStream_t st, bool bf16 = false);
 
 // gridder.cu
 // d_chunk_key, d_keymax: the scan's chunk table (chunks of kGridChunk records) and the scatter's

@@ -157,3 +157,43 @@ def test_tc_precision_config_accuracy(cuda_device):
     peak = np.max(np.abs(R[py, px] - d)) / np.max(np.abs(d))
     print("precision (tensor core): rel RMS vs FP64 DFT", err, "peak", peak, "vs FP32 path", O.rel_rms(R, R32))
     assert err < IMG_TOL
+
+
+# BF16 hi + lo keeps 16 significant bits per operand (FP16 hi + lo: 22), so each product carries up
+# to ~2^-16 relative error; the images are held to this tolerance, and the precision configuration's
+# error against the FP64 DFT is printed for the record.
+BF16_IMG_TOL = 1e-4
+
+
+def test_tc_bf16_small_image_against_oracle(cuda_device, small_snapshot):
+    s = small_snapshot
+    with api.Engine(**_tc(gridder=api.GRIDDER_TC_BF16)) as e:
+        img = e.image(s)
+        assert e.stats()["used_tc"] == 1
+    err = O.rel_rms(img, O.image_sii(s, k_rule=1).image)
+    print("small (tensor core, BF16 hi+lo): rel RMS vs oracle", err)
+    assert err < BF16_IMG_TOL
+
+
+def test_tc_bf16_precision_config_accuracy(cuda_device):
+    s = snapshot("precision")
+    kw = dict(edge_mode=api.EDGE_STRICT, presplat=1, k_rule=api.KRULE_TARGET, target_error=1e-6)
+    with api.Engine(gridder=api.GRIDDER_TC_BF16, **kw) as e:
+        R = e.image(s)
+        st = e.stats()
+        vr, vi = e.buffer(api.BUF_VIS_REAL), e.buffer(api.BUF_VIS_IMAG)
+        q, sv = e.buffer(api.BUF_Q).reshape(-1, 3), e.buffer(api.BUF_S)
+    assert st["used_tc"] == 1
+    vin = np.array(st["vin"]).reshape(3, 3)
+    r = O.expand_coords(q, sv)
+    G = st["grid_size"]
+    inc = O.inclusion_mask(r, _scale(s.cell_size, G), G, edge_mode=1)
+    rng = np.random.default_rng(7)
+    N = s.image_size
+    px, py = rng.integers(0, N, 256), rng.integers(0, N, 256)
+    inv_det = 1 / abs(vin[0, 0] * vin[1, 1] - vin[0, 1] * vin[1, 0])
+    d = O.dft_pixels_sep(q, sv, vr, vi, inv_det, s.num_samples, vin, N, float(np.float32(s.cell_size)), px, py, inc)
+    err = O.rel_rms(R[py, px], d)
+    peak = np.max(np.abs(R[py, px] - d)) / np.max(np.abs(d))
+    print("precision (tensor core, BF16 hi+lo): rel RMS vs FP64 DFT", err, "peak", peak)
+    assert err < BF16_IMG_TOL
