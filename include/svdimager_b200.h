@@ -215,6 +215,13 @@ int svdi_engine_dft_pixels(svdi_engine* e, const int64_t* px, const int64_t* py,
  * engine (recording each snapshot's host decisions: rotation, w range, slab and Chebyshev
  * configuration, and sizing the engine's buffers for the largest), then captures the device work
  * of all snapshots into one CUDA graph. svdi_batch_launch replays it with one cudaGraphLaunch.
+ * The graph runs every stage over all snapshots at once where it can ("wide" batch, the batch's
+ * own buffers): the small per-snapshot kernels (collapse, rotation, histogram, scatter) side by
+ * side on several streams, one scan over the tile keys of all snapshots, one persistent gridder
+ * launch per Chebyshev order that walks the records of all its snapshots from a device work
+ * counter, one batched cuFFT over all moment planes, and the recombinations. A batch whose
+ * snapshots split their w-slabs over several FFT batches, or whose moment planes do not fit in
+ * half of the free device memory, is captured snapshot after snapshot instead.
  *   snapshots: device-resident descriptors as for svdi_engine_image_device; their arrays must
  *              stay allocated at the same addresses (refill them in place to image new data of
  *              the same layout, sizes and w range: the recorded plans are reused as they are);
@@ -228,6 +235,7 @@ int svdi_batch_launch(svdi_batch* b, void* cuda_stream);  /* asynchronous; NULL:
 int svdi_batch_check(svdi_batch* b);   /* waits for the last launch; SVDI_ERR_INTERNAL if a tensor-core
                                           gridder wait gave up in any snapshot                        */
 int svdi_batch_plan(const svdi_batch* b, size_t index, int* num_slabs, int* num_terms);
+int svdi_batch_mode(const svdi_batch* b);  /* 1: wide batch, 0: snapshot after snapshot         */
 void svdi_batch_destroy(svdi_batch* b);
 
 /* Intermediate buffers of the last call, for inspection and tests (device-to-host copy). */

@@ -37,7 +37,7 @@ EXPORTED_SYMBOLS = (
     "svdi_kernel_launch_count", "svdi_bin_samples_noalloc", "svdi_server_create",
     "svdi_server_submit", "svdi_server_wait", "svdi_server_poll", "svdi_server_stats",
     "svdi_server_destroy", "svdi_engine_dft_pixels", "svdi_batch_create", "svdi_batch_launch",
-    "svdi_batch_check", "svdi_batch_plan", "svdi_batch_destroy", "svdi_copy_to_host", "_Z6FIpipePfS_S_S_S_mmf",
+    "svdi_batch_check", "svdi_batch_plan", "svdi_batch_mode", "svdi_batch_destroy", "svdi_copy_to_host", "_Z6FIpipePfS_S_S_S_mmf",
     "svdi_create", "svdi_submit", "svdi_poll", "svdi_wait", "svdi_destroy",
 )
 NOALLOC_MAX_KEYS = 16384
@@ -167,6 +167,7 @@ def lib():
         L.svdi_batch_check.argtypes = [P]
         L.svdi_batch_plan.argtypes = [P, sz, ctypes.POINTER(i), ctypes.POINTER(i)]
         L.svdi_batch_destroy.argtypes = [P]
+        L.svdi_batch_mode.argtypes = [P]
         L.svdi_batch_destroy.restype = None
         _lib = L
     return _lib
@@ -341,6 +342,11 @@ class Batch:
         ns, nt = ctypes.c_int(), ctypes.c_int()
         _check(lib().svdi_batch_plan(self._h, int(index), ctypes.byref(ns), ctypes.byref(nt)))
         return {"num_slabs": ns.value, "num_terms": nt.value}
+
+    @property
+    def wide(self) -> bool:
+        """True when every stage runs over all snapshots at once (one gridder launch per order)."""
+        return lib().svdi_batch_mode(self._h) == 1
 
     def close(self):
         if getattr(self, "_h", None):

@@ -1321,17 +1321,313 @@ struct svdi_batch {
     size_t N = 0;
     float cell = 0.0f;
     float* d_images = nullptr;
-    svdi::DevBuf status;  // per snapshot: the tensor-core gridder's status word
+    svdi::DevBuf status;  // per snapshot (chained graph) or per gridder launch (wide): give-up status
+    int num_status = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaStream_t last_stream = nullptr;
+    // Wide batch: every stage over all snapshots at once (batch-owned buffers, one gridder launch
+    // per Chebyshev order over the keys of all snapshots, one FFT over all moment planes).
+    bool wide = false;
+    svdi::DevBuf vr, vi, q, s, vin64, vin32, stats, partial, counts, offsets, cursor, keymax, chunk_key,
+        kb_offsets, rec, rec_s, planes, dropped, work, corr;
+    cufftHandle fft = 0;
+    bool have_fft = false;
+    std::vector<cudaStream_t> lanes;
+    std::vector<cudaEvent_t> lane_ev;
+    cudaEvent_t ev_fork = nullptr;
     ~svdi_batch() {
         if (e) cudaSetDevice(e->device);
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
+        if (have_fft) cufftDestroy(fft);
+        for (auto ev : lane_ev) cudaEventDestroy(ev);
+        for (auto st : lanes) cudaStreamDestroy(st);
+        if (ev_fork) cudaEventDestroy(ev_fork);
         if (e) e->batch_bound = false;
     }
 };
+
+namespace svdi {
+namespace {
+
+// Grid geometry of an imaging call (the same rules as image_core).
+GridGeom geom_for(const svdi_options& o, long long N, float cell_f, int K, bool use_tc) {
+    GridGeom g{};
+    g.G = grid_size(N, o.sigma);
+    g.gmin = -(g.G / 2);
+    g.gmax = (g.G - 1) / 2;
+    g.W = o.support;
+    if (use_tc) {
+        g.T = kTcTileRows;
+        g.ntile = (int)((g.G + g.T - 1) / g.T);
+        g.T2 = kTcTileCols;
+        g.ntile2 = (int)((g.G + g.T2 - 1) / g.T2);
+        g.ntile2 = (g.ntile2 + kTcBlocks - 1) / kTcBlocks * kTcBlocks;
+    } else {
+        g.T = o.tile ? o.tile : (K == 1 ? 64 : 32);
+        g.ntile = (int)((g.G + g.T - 1) / g.T);
+        g.T2 = g.T;
+        g.ntile2 = g.ntile;
+    }
+    g.edge_mode = o.edge_mode;
+    g.coord_mode = o.coord_mode;
+    g.scale = (double)cell_f * (double)g.G;
+    g.scale32 = cell_f * (float)g.G;
+    return g;
+}
+
+// The wide batch's device work, captured into b->graph from the engine's stream. Snapshots are
+// grouped by Chebyshev order; group g owns a contiguous range of tile keys (its snapshots' keys in
+// turn, slabs first), of global slabs and of moment planes. Per snapshot: collapse, rotation and
+// histogram (into its key range of one counts array), on kLanes side streams so that the small
+// per-snapshot kernels overlap; then one scan over all keys; the scatters (side streams); one
+// gridder launch per group walking the chunks of all its snapshots' records from a device counter;
+// one cuFFT execution over all planes; the recombination of every snapshot into its image.
+// Returns SVDI_ERR_UNSUPPORTED (nothing captured) when a snapshot's plan splits its slabs over
+// several FFT batches or all planes do not fit in half of the free device memory.
+int wide_capture(svdi_batch* b) {
+    svdi_engine* e = b->e;
+    const svdi_options& o = e->opt;
+    const size_t B = b->snaps.size();
+    const long long N = (long long)b->N;
+    const float cell_f = b->cell;
+    for (const auto& p : b->plans)
+        if ((int)p.bslabs < p.sp.nslab) return SVDI_ERR_UNSUPPORTED;
+    const bool tc_opt = o.gridder == SVDI_GRIDDER_TC || o.gridder == SVDI_GRIDDER_TC_BF16;
+    // groups of equal Chebyshev order, in order of first appearance
+    std::vector<int> group_k;
+    std::vector<int> group_of(B);
+    for (size_t s = 0; s < B; ++s) {
+        const int K = b->plans[s].sp.K;
+        auto it = std::find(group_k.begin(), group_k.end(), K);
+        group_of[s] = (int)(it - group_k.begin());
+        if (it == group_k.end()) group_k.push_back(K);
+    }
+    const int NG = (int)group_k.size();
+    struct Group {
+        int K = 1;
+        bool tc = false;
+        GridGeom g{};
+        long long key_lo = 0, key_hi = 0, slab_lo = 0, plane_lo = 0;
+    };
+    std::vector<Group> groups(NG);
+    std::vector<long long> key_base(B), plane_base(B), samp_off(B), row_off(B), chan_off(B);
+    long long nkeys = 0, nplanes = 0, ntot = 0, rtot = 0, ctot = 0;
+    bool need_s = false, any_tc = false;
+    for (int gi = 0; gi < NG; ++gi) {
+        Group& G = groups[gi];
+        G.K = group_k[gi];
+        G.tc = tc_opt && G.K == 1 && o.support <= 8;
+        G.g = geom_for(o, N, cell_f, G.K, G.tc);
+        // the gridders take a key's slab as key / (tiles per slab): start the group on a multiple of
+        // its tiles per slab (the keys skipped stay empty)
+        const long long tiles2 = (long long)G.g.ntile * G.g.ntile2;
+        nkeys = (nkeys + tiles2 - 1) / tiles2 * tiles2;
+        G.key_lo = nkeys;
+        G.slab_lo = nkeys / tiles2;
+        G.plane_lo = nplanes;
+        for (size_t s = 0; s < B; ++s) {
+            if (group_of[s] != gi) continue;
+            const SlabParams& sp = b->plans[s].sp;
+            key_base[s] = nkeys;
+            plane_base[s] = nplanes;
+            nkeys += (long long)sp.nslab * G.g.ntile * G.g.ntile2;
+            nplanes += (long long)sp.nslab * sp.K;
+        }
+        G.key_hi = nkeys;
+        need_s = need_s || G.K > 1;
+        any_tc = any_tc || G.tc;
+    }
+    for (size_t s = 0; s < B; ++s) {
+        samp_off[s] = ntot;
+        row_off[s] = rtot;
+        chan_off[s] = ctot;
+        ntot += (long long)b->snaps[s].num_samples;
+        rtot += (long long)b->snaps[s].num_rows;
+        ctot += (long long)b->snaps[s].num_channels;
+    }
+    if (nkeys > (1LL << 28) || ntot >= (1LL << 32) - 1) return SVDI_ERR_UNSUPPORTED;
+    const long long Gs = groups[0].g.G, GG = Gs * Gs;
+    size_t free_b = 0, total_b = 0;
+    SVDI_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t plane_bytes = (size_t)nplanes * (size_t)GG * sizeof(float2);
+    if (plane_bytes > free_b / 2) return SVDI_ERR_UNSUPPORTED;
+
+    const size_t NN = (size_t)N * (size_t)N;
+    SVDI_TRY(b->vr.ensure((size_t)ntot * 4));
+    SVDI_TRY(b->vi.ensure((size_t)ntot * 4));
+    SVDI_TRY(b->q.ensure((size_t)rtot * 24));
+    SVDI_TRY(b->s.ensure((size_t)ctot * 8));
+    SVDI_TRY(b->vin64.ensure(B * 9 * 8));
+    SVDI_TRY(b->vin32.ensure(B * 9 * 4));
+    SVDI_TRY(b->stats.ensure(B * ST_COUNT * 8));
+    const int L = (int)std::min<size_t>(8, B);
+    SVDI_TRY(b->partial.ensure((size_t)L * kPartialCap * 9 * 8));
+    SVDI_TRY(b->counts.ensure((size_t)nkeys * 4));
+    SVDI_TRY(b->offsets.ensure((size_t)(nkeys + 1) * 4));
+    SVDI_TRY(b->cursor.ensure((size_t)nkeys * 4));
+    SVDI_TRY(b->keymax.ensure((size_t)nkeys * 4));
+    SVDI_TRY(b->chunk_key.ensure(((size_t)std::max<long long>(ntot, 1) / kGridChunk + 2) * 4));
+    if (any_tc) SVDI_TRY(b->kb_offsets.ensure((size_t)(nkeys + 1) * 4));
+    SVDI_TRY(b->rec.ensure((size_t)std::max<long long>(ntot, 1) * sizeof(SampleRec)));
+    if (need_s) SVDI_TRY(b->rec_s.ensure((size_t)std::max<long long>(ntot, 1) * 4));
+    SVDI_TRY(b->planes.ensure(plane_bytes));
+    SVDI_TRY(b->dropped.ensure(B * 2 * 8));
+    SVDI_TRY(b->work.ensure(4 * sizeof(unsigned int) * (size_t)(NG + 1)));
+    SVDI_TRY(b->status.ensure((size_t)NG * 4 * sizeof(unsigned int)));
+    b->num_status = NG;
+    // correction table and ES polynomial of this geometry (the table copied: the batch owns it)
+    SVDI_TRY(ensure_corr(e, N, Gs, o.support, o.beta));
+    SVDI_TRY(b->corr.ensure((size_t)(N / 2 + 1) * 4));
+    SVDI_CUDA(cudaMemcpyAsync(b->corr.p, e->corr.p, (size_t)(N / 2 + 1) * 4, cudaMemcpyDeviceToDevice, e->stream));
+    if (e->poly_W != o.support || e->poly_beta != o.beta) {
+        build_es_poly(o.support, o.beta, &e->poly);
+        e->poly_W = o.support;
+        e->poly_beta = o.beta;
+    }
+    int dims[2] = {(int)Gs, (int)Gs};
+    SVDI_CUFFT(cufftPlanMany(&b->fft, 2, dims, nullptr, 1, (int)GG, nullptr, 1, (int)GG, CUFFT_C2C, (int)nplanes));
+    b->have_fft = true;
+    SVDI_CUFFT(cufftSetStream(b->fft, e->stream));
+    int prio_low = 0, prio_high = 0;
+    SVDI_CUDA(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+    for (int l = 0; l < L; ++l) {
+        cudaStream_t st = nullptr;
+        cudaEvent_t ev = nullptr;
+        SVDI_CUDA(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio_low));
+        b->lanes.push_back(st);
+        SVDI_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        b->lane_ev.push_back(ev);
+    }
+    SVDI_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+    SVDI_CUDA(cudaStreamSynchronize(e->stream));
+
+    cudaStream_t st = e->stream;
+    auto fork = [&]() -> int {
+        SVDI_CUDA(cudaEventRecord(b->ev_fork, st));
+        for (int l = 0; l < L; ++l) SVDI_CUDA(cudaStreamWaitEvent(b->lanes[l], b->ev_fork, 0));
+        return SVDI_OK;
+    };
+    auto join = [&]() -> int {
+        for (int l = 0; l < L; ++l) {
+            SVDI_CUDA(cudaEventRecord(b->lane_ev[l], b->lanes[l]));
+            SVDI_CUDA(cudaStreamWaitEvent(st, b->lane_ev[l], 0));
+        }
+        return SVDI_OK;
+    };
+    auto source = [&](size_t s) {
+        SampleSource src{};
+        src.q = b->q.as<double>() + 3 * row_off[s];
+        src.s = b->s.as<double>() + chan_off[s];
+        src.R = (long long)b->snaps[s].num_rows;
+        src.vr = b->vr.as<float>() + samp_off[s];
+        src.vi = b->vi.as<float>() + samp_off[s];
+        src.n = (long long)b->snaps[s].num_samples;
+        src.inv_det = b->plans[s].inv_det;
+        src.nonfinite = b->dropped.as<unsigned long long>() + 2 * s + 1;
+        return src;
+    };
+    unsigned int* vmax = b->work.as<unsigned int>() + 4 * NG + 1;  // max |record value| for the TC gridder
+
+    SVDI_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = [&]() -> int {
+        SVDI_CUDA(cudaMemsetAsync(b->counts.p, 0, (size_t)nkeys * 4, st));
+        SVDI_CUDA(cudaMemsetAsync(b->keymax.p, 0, (size_t)nkeys * 4, st));
+        SVDI_CUDA(cudaMemsetAsync(b->dropped.p, 0, B * 2 * 8, st));
+        SVDI_CUDA(cudaMemsetAsync(b->status.p, 0, (size_t)NG * 4 * sizeof(unsigned int), st));
+        SVDI_CUDA(cudaMemsetAsync(vmax, 0, sizeof(unsigned int), st));
+        SVDI_CUDA(cudaMemsetAsync(b->d_images, 0, B * NN * 4, st));
+        // per snapshot: collapse, rotation, histogram
+        SVDI_TRY(fork());
+        for (size_t s = 0; s < B; ++s) {
+            cudaStream_t ls = b->lanes[s % L];
+            const svdi_host_ms& d = b->snaps[s];
+            const Group& G = groups[group_of[s]];
+            SVDI_TRY(launch_collapse(d.vis0_real, d.vis0_imag, d.vis3_real, d.vis3_imag, d.flag0, d.flag3, d.weight0,
+                                     d.weight3, b->vr.as<float>() + samp_off[s], b->vi.as<float>() + samp_off[s],
+                                     (long long)d.num_samples, ls));
+            SVDI_TRY(launch_preprocess(d.uvw, d.frequencies_hz, (long long)d.num_rows, (long long)d.num_channels,
+                                       d.array_center_x, b->partial.as<double>() + (size_t)(s % L) * kPartialCap * 9,
+                                       kPartialCap, b->vin64.as<double>() + 9 * s, b->vin32.as<float>() + 9 * s,
+                                       b->q.as<double>() + 3 * row_off[s], b->s.as<double>() + chan_off[s],
+                                       b->stats.as<double>() + ST_COUNT * s, ls));
+            const SlabParams& sp = b->plans[s].sp;
+            const int nk = (int)((long long)sp.nslab * G.g.ntile * G.g.ntile2);
+            SVDI_TRY(launch_histogram(source(s), G.g, sp, b->counts.as<unsigned int>() + key_base[s], nk,
+                                      b->dropped.as<unsigned long long>() + 2 * s, ls));
+        }
+        SVDI_TRY(join());
+        SVDI_TRY(launch_scan(b->counts.as<unsigned int>(), (int)nkeys, b->offsets.as<unsigned int>(),
+                             b->cursor.as<unsigned int>(), st, any_tc ? b->kb_offsets.as<unsigned int>() : nullptr,
+                             kTcKBlock, b->chunk_key.as<unsigned int>(), kGridChunk));
+        // per snapshot: scatter into the global record order
+        SVDI_TRY(fork());
+        for (size_t s = 0; s < B; ++s) {
+            cudaStream_t ls = b->lanes[s % L];
+            const Group& G = groups[group_of[s]];
+            const SlabParams& sp = b->plans[s].sp;
+            const int nk = (int)((long long)sp.nslab * G.g.ntile * G.g.ntile2);
+            SVDI_TRY(launch_scatter(source(s), G.g, sp, b->cursor.as<unsigned int>() + key_base[s], nk,
+                                    b->rec.as<SampleRec>(), need_s ? b->rec_s.as<float>() : nullptr,
+                                    G.tc ? vmax : nullptr, ls, b->keymax.as<unsigned int>() + key_base[s]));
+        }
+        SVDI_TRY(join());
+        // one gridder launch per Chebyshev order over the records of all its snapshots
+        SVDI_CUDA(cudaMemsetAsync(b->planes.p, 0, plane_bytes, st));
+        for (int gi = 0; gi < NG; ++gi) {
+            const Group& G = groups[gi];
+            if (G.key_hi == G.key_lo) continue;
+            SlabParams sg{};
+            sg.K = G.K;
+            sg.nslab = (int)((G.key_hi - G.key_lo) / ((long long)G.g.ntile * G.g.ntile2));
+            float2* pl = b->planes.as<float2>() + G.plane_lo * GG;
+            unsigned int* stw = b->status.as<unsigned int>() + 4 * gi;
+            if (G.tc) {
+                // the TC gridder keeps its status in [0], reads max |v| from the pointer and counts work in [2]
+                SVDI_TRY(launch_grid_tc(b->rec.as<SampleRec>(), b->offsets.as<unsigned int>(),
+                                        b->kb_offsets.as<unsigned int>(), (int)nkeys, (int)G.key_lo, (int)G.key_hi,
+                                        (int)G.slab_lo, G.g, e->poly, pl, vmax, stw, e->sm_count, st,
+                                        o.gridder == SVDI_GRIDDER_TC_BF16));
+            } else {
+                SVDI_TRY(launch_grid_fp32(b->rec.as<SampleRec>(), need_s ? b->rec_s.as<float>() : nullptr,
+                                          b->offsets.as<unsigned int>(), b->chunk_key.as<unsigned int>(),
+                                          b->keymax.as<unsigned int>(), b->work.as<unsigned int>() + gi, (int)nkeys,
+                                          (int)G.key_lo, (int)G.key_hi, (int)G.slab_lo, G.g, sg, e->poly, pl,
+                                          e->sm_count, st));
+            }
+        }
+        SVDI_CUFFT(cufftExecC2C(b->fft, b->planes.as<cufftComplex>(), b->planes.as<cufftComplex>(), CUFFT_INVERSE));
+        for (size_t s = 0; s < B; ++s) {
+            const Group& G = groups[group_of[s]];
+            SVDI_TRY(launch_recombine(b->planes.as<float2>() + plane_base[s] * GG, G.g, N, (double)cell_f,
+                                      b->vin64.as<double>() + 9 * s, b->plans[s].sp, b->corr.as<float>(),
+                                      1.0 / (double)b->snaps[s].num_samples, o.reprojection, o.presplat,
+                                      b->d_images + s * NN, st, nullptr, true, nullptr,
+                                      b->dropped.as<unsigned long long>() + 2 * s + 1));
+        }
+        return SVDI_OK;
+    }();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+    if (rc != SVDI_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return rc == SVDI_ERR_UNSUPPORTED ? SVDI_ERR_INTERNAL : rc;
+    }
+    if (ce != cudaSuccess || !graph) {
+        set_error(std::string("graph capture failed: ") + cudaGetErrorString(ce));
+        cudaGetLastError();
+        return SVDI_ERR_CUDA;
+    }
+    b->graph = graph;
+    SVDI_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    b->wide = true;
+    return SVDI_OK;
+}
+
+}  // namespace
+}  // namespace svdi
 
 extern "C" {
 
@@ -1373,6 +1669,21 @@ int svdi_batch_create(svdi_engine* e, const svdi_host_ms* snapshots, size_t num_
         SVDI_TRY(main_path_device(e, &b->snaps[s], image_size, cell_size, d_images + s * NN, nullptr, &b->plans[s]));
     SVDI_CUDA(cudaStreamSynchronize(e->stream));
     SVDI_TRY(finish_pending(e));
+    b->e = e;
+    // every stage over all snapshots at once; when that is not possible (a snapshot's slabs span
+    // several FFT batches, or the planes of all snapshots do not fit), the chained graph below
+    const int wrc = wide_capture(b.get());
+    if (wrc == SVDI_OK) {
+        e->batch_bound = true;
+        *out = b.release();
+        return SVDI_OK;
+    }
+    if (wrc != SVDI_ERR_UNSUPPORTED) {
+        b->e = nullptr;
+        return wrc;
+    }
+    b->e = nullptr;
+    b->num_status = (int)num_snapshots;
     // capture the device work of every snapshot with its plan
     SVDI_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
     int rc = SVDI_OK;
@@ -1421,6 +1732,17 @@ int svdi_batch_check(svdi_batch* b) {
     }
     SVDI_CUDA(cudaSetDevice(b->e->device));
     if (b->last_stream) SVDI_CUDA(cudaStreamSynchronize(b->last_stream));
+    if (b->wide) {  // one status block of 4 words per gridder launch
+        std::vector<unsigned int> st((size_t)b->num_status * 4);
+        SVDI_CUDA(cudaMemcpy(st.data(), b->status.p, st.size() * sizeof(unsigned int), cudaMemcpyDeviceToHost));
+        for (int gi = 0; gi < b->num_status; ++gi)
+            if (st[4 * gi]) {
+                set_error("gridder launch " + std::to_string(gi) + ": the tensor-core gridder gave up waiting (status " +
+                          std::to_string(st[4 * gi]) + "); the batch's images are incomplete");
+                return SVDI_ERR_INTERNAL;
+            }
+        return SVDI_OK;
+    }
     std::vector<unsigned int> st(b->snaps.size());
     SVDI_CUDA(cudaMemcpy(st.data(), b->status.p, st.size() * sizeof(unsigned int), cudaMemcpyDeviceToHost));
     for (size_t s = 0; s < st.size(); ++s)
@@ -1441,6 +1763,14 @@ int svdi_batch_plan(const svdi_batch* b, size_t index, int* num_slabs, int* num_
     if (num_slabs) *num_slabs = b->plans[index].sp.nslab;
     if (num_terms) *num_terms = b->plans[index].sp.K;
     return SVDI_OK;
+}
+
+int svdi_batch_mode(const svdi_batch* b) {
+    if (!b) {
+        svdi::set_error("null batch");
+        return -SVDI_ERR_INVALID_ARGUMENT;
+    }
+    return b->wide ? 1 : 0;
 }
 
 void svdi_batch_destroy(svdi_batch* b) { delete b; }

@@ -91,9 +91,32 @@ def test_batch_matches_single_images(cuda_device, stream5):
     e.close()
 
 
+def test_batch_is_wide(cuda_device, stream5):
+    keep, descs, imgs, b, e, out1 = _batch_vs_single(stream5)
+    assert b.wide
+    b.close()
+    e.close()
+
+
+def test_wide_batch_with_mixed_chebyshev_orders(cuda_device, stream5):
+    """A snapshot with a large w range (elevated stations) beside two of the batching stream: the
+    error-target rule gives them different Chebyshev orders and slab counts, so the batch grids two
+    groups of tile keys (32 x 32 tiles, Chebyshev arguments per record) with one launch each; every
+    image equals the engine's."""
+    wf = synth.make_snapshot("widefield", n_rows_limit=3000, nchan=8)
+    snaps = [stream5[0], wf, stream5[1]]
+    keep, descs, imgs, b, e, out1 = _batch_vs_single(snaps, k_rule=api.KRULE_TARGET, target_error=1e-6)
+    assert b.wide
+    plans = [b.plan(i) for i in range(len(descs))]
+    assert len({p["num_terms"] for p in plans}) > 1, plans
+    b.close()
+    e.close()
+
+
 def test_batch_tensor_core_gridder(cuda_device, stream5):
     keep, descs, imgs, b, e, out1 = _batch_vs_single(stream5, gridder=api.GRIDDER_TC, k_rule=api.KRULE_FIXED,
                                                      fixed_k=1)
+    assert b.wide
     b.close()
     e.close()
 
