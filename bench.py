@@ -198,7 +198,7 @@ def batching_phase(api, local, n_snapshots=256, launches=3, seed_offset=0):
     reps = [descs[i] for i in (order[0], order[len(order) // 2], order[-1])]
     scratch = torch.zeros((N, N), dtype=torch.float32, device=dev)
     t_tune = time.perf_counter()
-    best, trials = autotune.tune(reps, N, cell, scratch, device=local, repeats=2)
+    best, trials = autotune.tune(reps, N, cell, scratch, device=local, repeats=3)
     t_tune = time.perf_counter() - t_tune
     chosen = [t for t in trials if all(t.options[k] == best[k] for k in ("support", "sigma", "gridder", "tile"))][0]
     imgs = torch.zeros((n_snapshots, N, N), dtype=torch.float32, device=dev)

@@ -139,9 +139,12 @@ def test_autotune_picks_an_accurate_fast_option(cuda_device, stream5):
     keep, descs = _upload(stream5[:2], torch)
     out = torch.zeros((N, N), dtype=torch.float32, device="cuda")
     cands = autotune.candidates(supports=(6, 8), sigmas=(1.5, 2.0), tiles=(64,))
-    best, trials = autotune.tune(descs, N, CELL, out, cands=cands, repeats=1)
-    assert len(trials) == len(cands)
+    best, trials = autotune.tune(descs, N, CELL, out, cands=cands, repeats=3)
+    assert len(trials) == len(cands) + 1   # the default options are always tried
     chosen = [t for t in trials if t.options["support"] == best["support"] and t.options["sigma"] == best["sigma"]
               and t.options["gridder"] == best["gridder"] and t.options["tile"] == best["tile"]][0]
     assert chosen.error <= 1e-5
-    assert all(t.ms >= chosen.ms for t in trials if t.error <= 1e-5 and np.isfinite(t.ms))
+    fastest = min(t.ms for t in trials if t.error <= 1e-5 and np.isfinite(t.ms))
+    is_default = all(chosen.options.get(k) == v for k, v in autotune.DEFAULT_CANDIDATE.items())
+    # the fastest accurate candidate, or the default options when nothing beats them by the margin
+    assert chosen.ms == fastest or (is_default and fastest > 0.97 * chosen.ms)
