@@ -390,6 +390,8 @@ def run_ours(args):
     rank, ws, local, dist = dist_init()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    from svdimager_b200 import replicas
+    host_cpus = replicas.bind_host_to_gpu(local)  # pinned buffers on the GPU's NUMA node
     snap = make_workload(args.config, rank)
     N, cell = snap.image_size, snap.cell_size
     gridder = api.GRIDDER_TC if args.gridder == "tc" else api.GRIDDER_FP32
@@ -553,6 +555,8 @@ def run_ours(args):
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "e2e": {"value": round(e2e_value, 3), "unit": "snapshots/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
+                "h2d_gbs": round(h2d * e2e_value / ws / 1e9, 2),
+                "host_cpus": f"{len(host_cpus)} CPUs of the GPU's NUMA node" if host_cpus else "unbound",
                 "api": f"svdi_server submit/wait, {stream_out['slots']} slots, {stream_out['window']} requests "
                        "in flight, pinned host inputs and output images",
                 "latency_ms": stream_out["latency_ms"],

@@ -66,3 +66,27 @@ def test_rank_leaving_is_detected_by_the_survivor():
     res = dict(q.get(timeout=10) for _ in range(2))
     assert res[1] == "left"
     assert res[0] != "no error"
+
+
+def test_bind_host_to_gpu_with_a_fake_nvml(monkeypatch):
+    """The host-side NUMA binding reads the GPU's CPU mask from NVML and restricts this process's
+    affinity to it (nothing of the GPU changes); without NVML it leaves the affinity alone."""
+    import os
+    import sys
+    import types
+    from svdimager_b200 import replicas
+    before = os.sched_getaffinity(0)
+    cpu0 = min(before)
+    fake = types.SimpleNamespace(
+        nvmlInit=lambda: None, nvmlShutdown=lambda: None,
+        nvmlDeviceGetHandleByIndex=lambda i: i,
+        nvmlDeviceGetCpuAffinity=lambda h, n: [1 << cpu0] + [0] * (n - 1))
+    monkeypatch.setitem(sys.modules, "pynvml", fake)
+    try:
+        assert replicas.bind_host_to_gpu(0) == [cpu0]
+        assert os.sched_getaffinity(0) == {cpu0}
+    finally:
+        os.sched_setaffinity(0, before)
+    monkeypatch.setitem(sys.modules, "pynvml", None)  # import fails: nothing changes
+    assert replicas.bind_host_to_gpu(0) == []
+    assert os.sched_getaffinity(0) == before
