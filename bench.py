@@ -394,7 +394,7 @@ def run_ours(args):
     host_cpus = replicas.bind_host_to_gpu(local)  # pinned buffers on the GPU's NUMA node
     snap = make_workload(args.config, rank)
     N, cell = snap.image_size, snap.cell_size
-    gridder = api.GRIDDER_TC if args.gridder == "tc" else api.GRIDDER_FP32
+    gridder = {"tc": api.GRIDDER_TC, "tc_bf16": api.GRIDDER_TC_BF16}.get(args.gridder, api.GRIDDER_FP32)
     opts = dict(device=local, edge_mode=api.EDGE_STRICT, k_rule=api.KRULE_TARGET, target_error=1e-6,
                 gridder=gridder)
     eng = api.Engine(**opts)
@@ -537,12 +537,14 @@ def run_ours(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f16 hi+lo operands, f32 accumulation" if st["used_tc"] else "f32",
+        "dtype": ("bf16 hi+lo operands, f32 accumulation" if args.gridder == "tc_bf16" else
+                  "f16 hi+lo operands, f32 accumulation") if st["used_tc"] else "f32",
         "data": "synthetic (seeded; 512-station layout, 220-source sky, noise, flags, weights)",
         "config": {
             "workload": f"{args.config}: {snap.num_rows} baselines x {snap.num_channels} channels = "
                         f"{snap.num_samples} vis, one snapshot, {N}^2 image, cell {cell} rad",
-            "gridder": "tcgen05 split-precision" if st["used_tc"] else "fp32 fixed-point",
+            "gridder": ("tcgen05 split-precision (" + ("BF16" if args.gridder == "tc_bf16" else "FP16") + " hi+lo)")
+                       if st["used_tc"] else "fp32 fixed-point",
             "grid": G, "planes": planes, "num_slabs": st["num_slabs"], "chebyshev_terms": st["num_terms"],
             "support": 8, "beta": 15.3704324328, "oversampling": 1.5, "tile": st["tile"],
             "k_rule": "target 1e-6", "edges": "strict (samples whose footprint leaves the grid are dropped)",
@@ -826,8 +828,9 @@ def main():
     ap.add_argument("--no-fipipe", action="store_true", help="skip the archive-entry (FIpipe) timing")
     ap.add_argument("--no-ref-binary", action="store_true",
                     help="reference arm: skip timing the reference's own GPU imager")
-    ap.add_argument("--gridder", default="fp32", choices=["tc", "fp32"],
-                    help="tc: split-precision tcgen05 gridder; fp32: CUDA-core fixed-point gridder")
+    ap.add_argument("--gridder", default="fp32", choices=["tc", "tc_bf16", "fp32"],
+                    help="tc: split-precision tcgen05 gridder (FP16 hi+lo); tc_bf16: the same with BF16 hi+lo; "
+                         "fp32: CUDA-core fixed-point gridder")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

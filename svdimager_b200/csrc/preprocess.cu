@@ -290,60 +290,77 @@ __global__ void k_vin_from_float(const float* __restrict__ v32, double* __restri
 
 // max |t3| and the valid-pixel count over the N x N rotated-frame pixels
 // (SVDIntegratedImager.cu:1029-1077), FP64, pixel offsets from the integer image centre.
+// max |t3| and the valid-pixel count over the image. t3 = -v33 + sgn(v33) sqrt(ra) is monotone in
+// the radicand ra (FP64 square root and subtraction of a constant preserve order), so the largest
+// |t3| sits at the smallest or the largest valid radicand: the pixel loop keeps only those two and
+// the final reduction takes the square roots (the same values the per-pixel form would produce).
+// Rows are spread over blocks and columns over threads (no 64-bit division per pixel).
 __global__ void __launch_bounds__(kThreads) k_t3_stats(const double* __restrict__ vin, long long N, double cell,
                                                       double* __restrict__ partial) {
-    __shared__ double sm[2 * kThreads];
-    const double v13 = vin[2], v23 = vin[5], v33 = vin[8];
-    const long long half = N / 2, total = N * N;
-    double mx = 0.0, cnt = 0.0;
-    for (long long p = blockIdx.x * (long long)kThreads + threadIdx.x; p < total;
-         p += (long long)gridDim.x * kThreads) {
-        const long long y = p / N, x = p - y * N;
-        const double t1 = cell * (double)(y - half), t2 = cell * (double)(x - half);
-        const double ra = 1.0 - (t1 + v13) * (t1 + v13) - (t2 + v23) * (t2 + v23);
-        if (ra >= 0.0) {
-            const double t3 = -v33 + (v33 >= 0.0 ? 1.0 : -1.0) * sqrt(ra);
-            mx = fmax(mx, fabs(t3));
-            cnt += 1.0;
+    __shared__ double sm[3 * kThreads];
+    const double v13 = vin[2], v23 = vin[5];
+    const long long half = N / 2;
+    double lo = 2.0, hi = -1.0, cnt = 0.0;  // radicands lie in [0, 1]
+    for (long long y = blockIdx.x; y < N; y += gridDim.x) {
+        const double t1 = cell * (double)(y - half) + v13;
+        const double r1 = 1.0 - t1 * t1;
+        for (long long x = threadIdx.x; x < N; x += kThreads) {
+            const double t2 = cell * (double)(x - half) + v23;
+            const double ra = r1 - t2 * t2;
+            if (ra >= 0.0) {
+                lo = fmin(lo, ra);
+                hi = fmax(hi, ra);
+                cnt += 1.0;
+            }
         }
     }
-    sm[threadIdx.x] = mx;
-    sm[kThreads + threadIdx.x] = cnt;
+    sm[threadIdx.x] = lo;
+    sm[kThreads + threadIdx.x] = hi;
+    sm[2 * kThreads + threadIdx.x] = cnt;
     __syncthreads();
     for (int stride = kThreads / 2; stride > 0; stride >>= 1) {
         if (threadIdx.x < stride) {
-            sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + stride]);
-            sm[kThreads + threadIdx.x] += sm[kThreads + threadIdx.x + stride];
+            sm[threadIdx.x] = fmin(sm[threadIdx.x], sm[threadIdx.x + stride]);
+            sm[kThreads + threadIdx.x] = fmax(sm[kThreads + threadIdx.x], sm[kThreads + threadIdx.x + stride]);
+            sm[2 * kThreads + threadIdx.x] += sm[2 * kThreads + threadIdx.x + stride];
         }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        partial[blockIdx.x * 2 + 0] = sm[0];
-        partial[blockIdx.x * 2 + 1] = sm[kThreads];
+        partial[blockIdx.x * 3 + 0] = sm[0];
+        partial[blockIdx.x * 3 + 1] = sm[kThreads];
+        partial[blockIdx.x * 3 + 2] = sm[2 * kThreads];
     }
 }
 
 __global__ void __launch_bounds__(kThreads) k_t3_final(const double* __restrict__ partial, int nblocks,
-                                                      double* __restrict__ stats) {
-    __shared__ double sm[2 * kThreads];
-    double mx = 0.0, cnt = 0.0;
+                                                      const double* __restrict__ vin, double* __restrict__ stats) {
+    __shared__ double sm[3 * kThreads];
+    double lo = 2.0, hi = -1.0, cnt = 0.0;
     for (int b = threadIdx.x; b < nblocks; b += kThreads) {
-        mx = fmax(mx, partial[b * 2 + 0]);
-        cnt += partial[b * 2 + 1];
+        lo = fmin(lo, partial[b * 3 + 0]);
+        hi = fmax(hi, partial[b * 3 + 1]);
+        cnt += partial[b * 3 + 2];
     }
-    sm[threadIdx.x] = mx;
-    sm[kThreads + threadIdx.x] = cnt;
+    sm[threadIdx.x] = lo;
+    sm[kThreads + threadIdx.x] = hi;
+    sm[2 * kThreads + threadIdx.x] = cnt;
     __syncthreads();
     for (int stride = kThreads / 2; stride > 0; stride >>= 1) {
         if (threadIdx.x < stride) {
-            sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + stride]);
-            sm[kThreads + threadIdx.x] += sm[kThreads + threadIdx.x + stride];
+            sm[threadIdx.x] = fmin(sm[threadIdx.x], sm[threadIdx.x + stride]);
+            sm[kThreads + threadIdx.x] = fmax(sm[kThreads + threadIdx.x], sm[kThreads + threadIdx.x + stride]);
+            sm[2 * kThreads + threadIdx.x] += sm[2 * kThreads + threadIdx.x + stride];
         }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        stats[ST_MAX_T3] = sm[0];
-        stats[ST_VALID_PIX] = sm[kThreads];
+        const double v33 = vin[8], sg = v33 >= 0.0 ? 1.0 : -1.0;
+        double mx = 0.0;
+        if (sm[2 * kThreads] > 0.0)
+            mx = fmax(fabs(-v33 + sg * sqrt(sm[0])), fabs(-v33 + sg * sqrt(sm[kThreads])));
+        stats[ST_MAX_T3] = mx;
+        stats[ST_VALID_PIX] = sm[2 * kThreads];
     }
 }
 
@@ -477,10 +494,10 @@ int launch_vin_from_float(const float* d_vin32, double* d_vin64, cudaStream_t st
 
 int launch_t3_stats(const double* d_vin64, long long N, double cell, double* d_partial,
                     int partial_cap, double* d_stats, cudaStream_t st) {
-    const int nb = grid_for(N * N, partial_cap);
+    const int nb = (int)std::max<long long>(1, std::min<long long>(N, partial_cap));  // one row per block and step
     k_t3_stats<<<nb, kThreads, 0, st>>>(d_vin64, N, cell, d_partial);
     SVDI_LAUNCHED();
-    k_t3_final<<<1, kThreads, 0, st>>>(d_partial, nb, d_stats);
+    k_t3_final<<<1, kThreads, 0, st>>>(d_partial, nb, d_vin64, d_stats);
     SVDI_LAUNCHED();
     return SVDI_OK;
 }
