@@ -5,8 +5,9 @@ SVDIntegratedImager.cu:884-888, 1510) and picks only the Chebyshev order. Here t
 CUDA-core or tensor-core), its tile size, the ES support W, the oversampling sigma (with the ES
 beta that goes with W and sigma) and the Chebyshev error target are chosen per family: every
 candidate images the representative snapshots once with presplat = 1 and is checked against the
-library's FP64 direct DFT at random pixels (`Engine.dft_pixels`), then timed; the fastest
-candidate whose relative RMS error stays within the target wins. The Chebyshev order K and the
+library's FP64 direct DFT at random pixels (`Engine.dft_pixels`), then timed as one batch of those
+snapshots (median of several graph launches); the fastest candidate whose relative RMS error stays
+within the target wins. The Chebyshev order K and the
 w-slab count follow from the error target per snapshot (k_rule TARGET: the fewest moment planes
 that meet it)."""
 from __future__ import annotations
@@ -51,7 +52,7 @@ def candidates(supports: Sequence[int] = SUPPORTS, sigmas: Sequence[float] = SIG
 class Trial:
     options: Dict
     error: float = math.inf          # worst relative RMS over the representative snapshots
-    ms: float = math.inf             # mean device time per snapshot
+    ms: float = math.inf             # device time per snapshot in a batch of the snapshots
     num_terms: List[int] = field(default_factory=list)
     num_slabs: List[int] = field(default_factory=list)
     used_tc: bool = False
@@ -65,6 +66,30 @@ def _rel_rms(a: np.ndarray, b: np.ndarray) -> float:
 
 # The library's default options (the reference's kernel): the candidate a tuned choice must beat.
 DEFAULT_CANDIDATE = dict(support=8, sigma=1.5, beta=REF_BETA, gridder=api.GRIDDER_FP32, tile=0)
+
+
+def _batch_ms(snapshots, N: int, cell_size: float, out, options: Dict, repeats: int) -> float:
+    """Device time per snapshot of `snapshots` imaged as one batch (the way batches run: every
+    stage over all snapshots at once), median over `repeats` graph launches."""
+    import torch
+    imgs = out.new_zeros((len(snapshots), N, N))
+    stream = torch.cuda.Stream(out.device)
+    with api.Engine(**options) as e:
+        b = api.Batch(e, snapshots, N, cell_size, imgs.data_ptr())
+        try:
+            b.launch(stream.cuda_stream)  # warm
+            b.check()
+            ms = []
+            for _ in range(max(1, repeats)):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                b.launch(stream.cuda_stream)
+                e1.record(stream)
+                b.check()
+                ms.append(e0.elapsed_time(e1) / len(snapshots))
+        finally:
+            b.close()
+    return float(np.median(ms))
 
 
 def tune(snapshots, image_size: int, cell_size: float, out, *, target: float = 1e-5,
@@ -103,15 +128,7 @@ def tune(snapshots, image_size: int, cell_size: float, out, *, target: float = 1
                     t.error = max(t.error if math.isfinite(t.error) else 0.0,
                                   _rel_rms(host[py, px].astype(np.float64), ref))
             if t.error <= target:
-                with api.Engine(**common, **opt) as e:
-                    for d in snapshots:  # warm plans and buffers
-                        e.image_device(d, N, cell_size, out_ptr, stream_ptr)
-                    ms = []
-                    for _ in range(repeats):
-                        for d in snapshots:
-                            e.image_device(d, N, cell_size, out_ptr, stream_ptr)
-                            ms.append(e.stats()["ms_total"])
-                    t.ms = float(np.median(ms))
+                t.ms = _batch_ms(snapshots, N, cell_size, out, dict(common, **opt), repeats)
         except api.SvdiError as ex:
             t.failure = ex.message
         trials.append(t)

@@ -305,8 +305,19 @@ def _piled_quartet():
     b[:, 2] = rng.uniform(-1e-3, 1e-3, n_pile + n_rest)
     visr = np.concatenate([3.0e4 + rng.normal(0, 30.0, n_pile), rng.normal(size=n_rest)]).astype(np.float32)
     visi = np.concatenate([rng.normal(0, 30.0, n_pile), rng.normal(size=n_rest)]).astype(np.float32)
-    v = np.eye(3, dtype=np.float32)
-    return visr, visi, b.astype(np.float32), v, N, cell, G, scale
+    return visr, visi, b.astype(np.float32), _tilted_basis(), N, cell, G, scale
+
+
+def _tilted_basis():
+    """A rotation about w by 0.3 rad, then a tilt of 0.05 rad (V31, V32 != 0). With an identity
+    basis the archive SIN deprojection maps every pixel onto an exact integer position, and whether
+    a pixel landing exactly on the splat bound |L| = N/2 - 1 is kept then depends on the last bit
+    of its FP64 arithmetic (glibc and CUDA's math differ there); this basis keeps every target at
+    least 5e-3 pixel away from that bound."""
+    a, t = 0.3, 0.05
+    rz = np.array([[np.cos(a), np.sin(a), 0.0], [-np.sin(a), np.cos(a), 0.0], [0.0, 0.0, 1.0]])
+    rx = np.array([[1.0, 0.0, 0.0], [0.0, np.cos(t), np.sin(t)], [0.0, -np.sin(t), np.cos(t)]])
+    return (rx @ rz).astype(np.float32)
 
 
 def test_samples_piled_on_one_position(cuda_device):
@@ -320,7 +331,9 @@ def test_samples_piled_on_one_position(cuda_device):
         _check_binning(e, st, b.astype(np.float64), visr, visi, cell, coord_mode=1)
         grid = e.buffer(api.BUF_GRID).reshape(-1, G, G)
     o = O.image_fipk(visr, visi, b, v, N, cell, coord_mode=1)
-    og = O.grid(b.astype(np.float64), visr, visi, scale, G, o.sc, 1.0, coord_mode=1)
+    V = v.astype(np.float64)
+    inv_det = 1.0 / abs(V[0, 0] * V[1, 1] - V[0, 1] * V[1, 0])
+    og = O.grid(b.astype(np.float64), visr, visi, scale, G, o.sc, inv_det, coord_mode=1)
     assert np.linalg.norm(grid - og) / np.linalg.norm(og) < GRID_TOL
     assert O.rel_rms(img, o.image) < IMG_TOL
 
