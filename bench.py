@@ -516,14 +516,13 @@ def run_ours(args):
         alg = 8 * planes * N * N + 4 * N * N
         name = "k_recombine"
     achieved = alg / (stage_ms[dom] * 1e-3) / 1e9
-    traffic = None  # DRAM bytes per launch of the dominant kernel from an ncu capture, when recorded
-    tr_path = os.path.join(ROOT, "profiles", "traffic.txt")
-    if dom == "ms_grid" and os.path.exists(tr_path):
-        kern = "k_grid_tc" if st["used_tc"] else "k_grid_fp32"
-        for ln in open(tr_path):
-            f = ln.split()
-            if len(f) == 2 and f[0] == kern:
-                traffic = int(f[1])
+    # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of each gridder on
+    # this workload, from the one-launch --set full captures summarised in
+    # profiles/k_grid_fp32_precision.md and profiles/k_grid_tc_precision.md
+    traffic = None
+    if dom == "ms_grid" and args.config == "precision":
+        traffic = {"k_grid_fp32": 223432960, "k_grid_tc": 224904960}.get(
+            "k_grid_tc" if st["used_tc"] else "k_grid_fp32")
 
     cpu = cpu_baseline(snap, eng, api, st, args) if not args.no_cpu else None
     line = {
