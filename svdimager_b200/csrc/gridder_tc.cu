@@ -6,42 +6,42 @@
 // Gridding with a separable kernel is a sum of outer products. For the samples k of one tile,
 //   G[m][n] = sum_k  wx_k[m] * (wy_k[n] v_k)   =   (A B^T)[m][n],
 // where column k of A holds the ES weights of sample k on its footprint rows and column k of B its
-// ES weights on its footprint columns times the visibility (re and im as separate B rows). Each
-// K-block of 32 samples of one tile is written to shared memory as FP16 hi + lo pairs
-// (x = hi + lo + O(2^-22 x)) and accumulated in FP32 in tensor memory by
-//   D += A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T
-// (six tcgen05.mma kind::f16, M = 64, N = 32, K = 16; the lo*lo term is below 2^-22 relative).
+// ES weights on its footprint columns times the visibility (re and im as separate B columns).
+// Each K-block of 32 samples of one tile is written to shared memory with both factors split into
+// FP16 (or BF16) hi + lo parts (x = hi + lo + O(2^-22 x) in FP16), stacked as
+//   A' = [A_hi; A_lo] (128 rows),  B' = [B_hi | B_lo] (64 columns),
+// so that ONE tcgen05.mma kind::f16 (M = 128, N = 64, K = 16) per 16 samples computes all four
+// products A_hi B_hi, A_hi B_lo, A_lo B_hi, A_lo B_lo into the quarters of a 128 x 64 FP32
+// accumulator in tensor memory; the epilogue adds the quarters. Two MMAs per K-block.
 //
-// Cost model (measured on B200): a tcgen05.mma of this skinny shape costs about its operand bytes
-// read from shared memory at ~117 B/clk per SM (M = 64, N = 32: 26 clk), one issuing thread issues
-// at most one every ~46 clk and an mbarrier try_wait costs the issuing thread ~200 clk. Hence M = 64
-// accumulators (56-row tiles), two CTAs per SM (two issuing threads) and one wait per pipeline stage
-// of four K-blocks.
+// Cost model (measured on B200): a skinny tcgen05.mma costs about its operand bytes read from
+// shared memory at ~117 B/clk per SM, and in this kernel one issuing thread spent ~110 clk per
+// MMA; an mbarrier try_wait costs the issuing thread ~200 clk. Hence few, wide MMAs (6 KB of
+// operands each, 2 per K-block instead of 6 skinny ones), two CTAs per SM (two issuing threads)
+// and one wait per pipeline stage of four K-blocks.
 //
 // Operands. Both are MN-major without swizzle: a core matrix is 8 K (samples) x 16 bytes (8
-// consecutive rows of A or columns of B). One thread builds one sample's column of A and of B: its
+// consecutive rows of A or columns of B). One thread builds one sample's column of A' and of B': its
 // eight row taps land at rows r0 .. r0 + 7 of the 64-row accumulator, that is in the 8-row chunks
 // r0 / 8 and r0 / 8 + 1 at an offset of r0 % 8. The thread evaluates the taps in order (FP32
-// piecewise polynomials whose coefficients are kernel-parameter constants), packs them into FP16
-// hi and lo half pairs and shifts the 16-half window into place with byte permutes and word
-// selects, so each chunk is one 16-byte store (a warp's stores of one chunk fill four whole
-// shared-memory wavefronts, whatever the samples' rows). B's 16 columns (8 real + 8 imaginary taps
-// of the 8-column tile plus halo) are written in full; of A only the chunks the thread's previous
-// sample in this stage slot covered and the new sample does not are cleared.
+// piecewise polynomials whose coefficients are kernel-parameter constants), packs them into hi and
+// lo half pairs and shifts the 16-half window into place with byte permutes and word selects, so
+// each chunk is one 16-byte store (a warp's stores of one chunk fill four whole shared-memory
+// wavefronts, whatever the samples' rows). The A' rows are ordered so that TMEM lane quarter q
+// holds grid rows 16q .. 16q + 15 of the hi part and then of the lo part (a_chunk). B's 16 columns
+// (8 real + 8 imaginary taps of the 8-column tile plus halo) are written in full; of A only the
+// chunks the thread's previous sample in this stage slot covered and the new sample does not are
+// cleared.
 //
-// Tiles. Binning uses 56-row x 8-column tiles (footprint origins). Four consecutive tile keys
-// (the same tile row, 32 consecutive columns) form a super-tile whose running sum lives in TMEM
-// columns [0, 128): block c = key % 4 owns columns [32c, 32c + 32) (0..15 real, 16..31 imaginary
-// part of grid columns origin2 + 8c .. + 15); row r of the 64-row accumulator sits in TMEM lane
-// 32 (r / 16) + r % 16. Neighbouring blocks overlap by 8 grid columns; the epilogue adds the
-// overlap and reduces every non-zero cell once into the moment plane (red.global.add.v2.f32),
-// checkerboard sign and 1 / scale applied.
+// Accumulation. Consecutive K-blocks of one tile key (at most kIntervalKB of them, 32 MMAs) form
+// an interval that accumulates in one of four 64-column TMEM accumulators. The tensor core's FP32
+// accumulation is not round-to-nearest: summing thousands of MMAs into one accumulator shrank
+// dense grid cells by a relative 3.5e-5 on the 8.4M-sample snapshot (measured against the oracle),
+// so intervals stay short and each one is drained by the epilogue into the moment plane with FP32
+// round-to-nearest reductions (red.global.add.v2.f32, checkerboard sign and 1 / scale applied).
 //
-// Two-level accumulation. The tensor core's FP32 accumulation is not round-to-nearest: summing
-// thousands of MMAs into one accumulator shrank dense grid cells by a relative 3.5e-5 on the 8.4M
-// sample snapshot (measured against the oracle). So the MMAs of at most 8 K-blocks of one key go
-// to one of four 32-column "fresh" accumulators (columns 128..255), which the epilogue warps add
-// into the running block with FP32 round-to-nearest adds once those MMAs are done.
+// Tiles. Binning uses 56-row x 8-column tiles (footprint origins); an accumulator covers the tile's
+// 64 rows (56 + halo) and 16 columns (8 + halo).
 //
 // Roles (two CTAs per SM, 10 warps, 256 TMEM columns each):
 //   warps 0-3   producers: warp w fills sub-stage w of the two pipeline stages in turn with K-blocks
@@ -53,12 +53,11 @@
 //               (one contiguous run of 16-byte records) into shared memory with a bulk copy
 //               (cp.async.bulk, this GPU's own memory, no multicast) that completes on the record
 //               slot's mbarrier.
-//   warp 5      MMA issuer: issues the MMAs, opens and closes fresh intervals and posts merge /
-//               flush / exit events.
-//   warps 6-9   epilogue: TMEM lane quarter (warp % 4); merge fresh intervals into the running sum
-//               and flush super-tiles to the moment plane, in event order.
+//   warp 5      MMA issuer: issues the MMAs, opens and closes intervals and posts a drain event
+//               per interval.
+//   warps 6-9   epilogue: TMEM lane quarter (warp % 4); drain the intervals in event order.
 // The scheduler warps take chunks of 32 K-blocks from a global counter (a chunk can start and end
-// inside a tile; each CTA flushes the super-tiles it touched).
+// inside a tile).
 //
 // Scaling. The B values are wy * v * 2^(14 - e) with max|v| < 2^e over all records (the scatter
 // kernel's max reduction) and the A values 256 * wx, so every FP16 operand is below 65504 and the
@@ -82,8 +81,10 @@ namespace svdi {
 namespace {
 
 constexpr int kKB = kTcKBlock;          // samples per K-block
-constexpr int kM = 64;                  // accumulator rows: tile rows + footprint halo
-constexpr int kN = 32;                  // columns per block: 16 real + 16 imaginary
+constexpr int kRows = 64;               // grid rows of an accumulator: tile rows + footprint halo
+constexpr int kCols = 32;               // columns of a split: 16 real + 16 imaginary
+constexpr int kM = 2 * kRows;           // MMA rows: A_hi rows, then A_lo rows
+constexpr int kN = 2 * kCols;           // MMA columns: B_hi columns, then B_lo columns
 constexpr int kSubStages = 4;           // K-blocks per pipeline stage (one per producer warp)
 constexpr int kPipe = 2;                // pipeline stages
 constexpr int kProdWarps = kSubStages;                     // 4: warp w fills sub-stage w of both stages
@@ -92,17 +93,16 @@ constexpr int kMmaWarp = kProdWarps + 1;                   // 5
 constexpr int kEpiWarp0 = kProdWarps + 2;                  // 6..9
 constexpr int kWarps = kProdWarps + 2 + 4;
 constexpr int kThreads = kWarps * 32;                      // 320
-constexpr int kFreshBufs = 4;
-constexpr int kFreshKB = 8;             // K-blocks (48 MMAs) per fresh interval at most
-constexpr int kFreshCol0 = kTcBlocks * kN;  // running blocks first, then the fresh buffers
+constexpr int kAccBufs = 4;             // TMEM accumulators of kN columns
+constexpr int kIntervalKB = 16;         // K-blocks (32 MMAs) per accumulator interval at most
 constexpr int kTmemCols = 256;
 constexpr int kMetaRing = 64;           // published K-block descriptors
 constexpr int kRecSlots = 16;           // record slots: K-blocks staged ahead of the producers
 constexpr int kChunkKB = 32;            // K-blocks per chunk of dynamically distributed work
 constexpr int kEventRing = 64;
 
-constexpr int kABytes = kM * kKB * 2;                    // 4 KB per FP16 A operand
-constexpr int kBBytes = kN * kKB * 2;                    // 2 KB per FP16 B operand
+constexpr int kABytes = kRows * kKB * 2;                 // 4 KB per FP16 A half (hi or lo)
+constexpr int kBBytes = kCols * kKB * 2;                 // 2 KB per FP16 B half
 constexpr int kSubBytes = 2 * kABytes + 2 * kBBytes;     // 12 KB: one K-block
 constexpr int kStageBytes = kSubStages * kSubBytes;      // 48 KB
 constexpr int kRecOff = kPipe * kStageBytes;             // record slots after the stages
@@ -112,8 +112,8 @@ constexpr int kSmemUsed = kRecOff + kRecBytes;
 // an SM and their 2 x 256 TMEM columns always fit in its 512.
 constexpr int kSmemBytes = kSmemUsed;
 static_assert(kSmemBytes > 228 * 1024 / 3 && 2 * (kSmemBytes + 4096) <= 228 * 1024, "two CTAs per SM");
-static_assert(kFreshCol0 + kFreshBufs * kN <= kTmemCols, "TMEM plan exceeds the allocation");
-static_assert(kTcTileRows + 8 <= kM && kTcTileCols + 8 <= 16, "tile + footprint must fit the accumulator");
+static_assert(kAccBufs * kN <= kTmemCols, "TMEM plan exceeds the allocation");
+static_assert(kTcTileRows + 8 <= kRows && kTcTileCols + 8 <= 16, "tile + footprint must fit the accumulator");
 static_assert(kEpiWarp0 + 4 == kWarps, "four epilogue warps (one per TMEM lane quarter) come last");
 static_assert(kRecSlots <= kMetaRing && kKB == 32, "one record slot per published K-block, one lane per record");
 
@@ -125,7 +125,7 @@ constexpr unsigned long long kDescFixed = ((128ull >> 4) << 16) | ((512ull >> 4)
 __device__ __forceinline__ unsigned long long smem_desc(uint32_t addr) {
     return (unsigned long long)((addr >> 4) & 0x3FFFu) | kDescFixed;
 }
-// Instruction descriptor: FP32 accumulator, FP16 A and B, both MN-major, N = 32, M = 64.
+// Instruction descriptor: FP32 accumulator, FP16 A and B, both MN-major, N = 64, M = 128.
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 15) | (1u << 16) | ((uint32_t)(kN >> 3) << 17) |
                             ((uint32_t)(kM >> 4) << 24);
 // The same with BF16 A and B (both operands always have the same type).
@@ -225,12 +225,6 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
                  : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&r)[8]) {
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
-                 "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
-                 : "memory");
-}
-__device__ __forceinline__ void tmem_st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void red_add_v2(float2* addr, float a, float b) {
     asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(addr), "f"(a), "f"(b) : "memory");
@@ -302,6 +296,12 @@ __device__ __forceinline__ void window16(const uint32_t (&h)[4], int sh, uint32_
     o[7] = s2 ? u[5] : 0u;
 }
 
+// A operand row order: the TMEM lane quarter q (accumulator lanes 32q .. 32q + 31) holds grid rows
+// 16q .. 16q + 15 of the hi part in its first 16 lanes and the same rows of the lo part in the
+// last 16, so one warp adds hi and lo with a shuffle. In 8-row chunks: grid-row chunk j of the hi
+// part is A chunk a_chunk(j), of the lo part a_chunk(j) + 2.
+__device__ __forceinline__ int a_chunk(int j) { return ((j >> 1) << 2) | (j & 1); }
+
 __device__ __forceinline__ void st_chunk(unsigned char* p, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
     *reinterpret_cast<uint4*>(p) = make_uint4(a, b, c, d);
 }
@@ -312,13 +312,12 @@ struct KBMeta {
     int cnt;            // records (1..32)
 };
 
-enum EventType : int { kEvMerge = 0, kEvFlush = 1, kEvExit = 2 };
+enum EventType : int { kEvDrain = 0, kEvExit = 1 };
 struct Event {
     int type;
-    int buf;     // merge: fresh buffer
-    int blk;     // merge: running block
-    int key;     // flush: a key of the super-tile
-    int parity;  // merge: phase parity of the fresh buffer's MMAs-done barrier
+    int buf;     // accumulator to drain
+    int key;     // its tile key
+    int parity;  // phase parity of the accumulator's MMAs-done barrier
 };
 
 struct TcParams {
@@ -336,8 +335,8 @@ struct __align__(8) TcShared {
     unsigned long long full[kPipe];       // producers -> MMA: the stage's K-blocks written (4 warp arrivals)
     unsigned long long empty[kPipe];      // MMA -> producers: stage read (tcgen05.commit)
     unsigned long long rec_full[kRecSlots];  // scheduler's bulk copy -> producers: records staged
-    unsigned long long fdone[kFreshBufs]; // MMA -> epilogue: fresh interval's MMAs done (commit)
-    unsigned long long ffree[kFreshBufs]; // epilogue -> MMA: fresh buffer merged (4 warp arrivals)
+    unsigned long long fdone[kAccBufs];   // MMA -> epilogue: the interval's MMAs done (commit)
+    unsigned long long ffree[kAccBufs];   // epilogue -> MMA: accumulator read (4 warp arrivals)
     KBMeta meta[kMetaRing];
     Event events[kEventRing];
     unsigned int published;               // K-block descriptors published
@@ -378,7 +377,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
             mbar_init(smem_u32(&S.empty[s]), 1);
         }
         for (int s = 0; s < kRecSlots; ++s) mbar_init(smem_u32(&S.rec_full[s]), 1);
-        for (int b = 0; b < kFreshBufs; ++b) {
+        for (int b = 0; b < kAccBufs; ++b) {
             mbar_init(smem_u32(&S.fdone[b]), 1);
             mbar_init(smem_u32(&S.ffree[b]), 4);
         }
@@ -420,9 +419,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
             const int j = it * kProdWarps + warp;
             const int stg = it & 1;
             const int use = it >> 1;  // earlier rounds of this stage
-            unsigned char* const A_hi = smem + stg * kStageBytes + warp * kSubBytes;
-            unsigned char* const A_lo = A_hi + kABytes;
-            unsigned char* const B_hi = A_lo + kABytes;
+            unsigned char* const A = smem + stg * kStageBytes + warp * kSubBytes;  // A_hi and A_lo rows
+            unsigned char* const B_hi = A + 2 * kABytes;
             unsigned char* const B_lo = B_hi + kBBytes;
             // wait until K-block j is published or the schedule ends before it (warp-uniform)
             int state = 0;  // 1: produce, 0: done, -1: give up
@@ -516,21 +514,22 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
                     for (int d = 0; d < 2; ++d) {
                         const int cj = oldj + d;
                         if (cj != j0 && cj != j0 + 1) {
-                            st_chunk(A_hi + kofs + cj * 512, 0u, 0u, 0u, 0u);
-                            st_chunk(A_lo + kofs + cj * 512, 0u, 0u, 0u, 0u);
+                            st_chunk(A + kofs + a_chunk(cj) * 512, 0u, 0u, 0u, 0u);
+                            st_chunk(A + kofs + (a_chunk(cj) + 2) * 512, 0u, 0u, 0u, 0u);
                         }
                     }
                 }
                 if (fast) {
                     uint32_t h[4], o[8];
+                    const int c0h = a_chunk(j0), c1h = a_chunk(j0 + 1);
                     hi8<kBf16>(a, h);
                     window16(h, r0 & 7, o);
-                    st_chunk(A_hi + kofs + j0 * 512, o[0], o[1], o[2], o[3]);
-                    st_chunk(A_hi + kofs + j0 * 512 + 512, o[4], o[5], o[6], o[7]);
+                    st_chunk(A + kofs + c0h * 512, o[0], o[1], o[2], o[3]);
+                    st_chunk(A + kofs + c1h * 512, o[4], o[5], o[6], o[7]);
                     lo8<kBf16>(a, h);
                     window16(h, r0 & 7, o);
-                    st_chunk(A_lo + kofs + j0 * 512, o[0], o[1], o[2], o[3]);
-                    st_chunk(A_lo + kofs + j0 * 512 + 512, o[4], o[5], o[6], o[7]);
+                    st_chunk(A + kofs + (c0h + 2) * 512, o[0], o[1], o[2], o[3]);
+                    st_chunk(A + kofs + (c1h + 2) * 512, o[4], o[5], o[6], o[7]);
                 }
                 if (stg) oldj1 = fast ? j0 : -1;
                 else oldj0 = fast ? j0 : -1;
@@ -705,12 +704,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
         }
     } else if (warp == kMmaWarp) {
         // ============================ MMA issuer ============================
-        // MMA / interval / event state (lane 0)
-        int cur_st = -1, cur_key = 0;
-        int ob = 0, oc = 0, on = 0, next_buf = 0;
-        unsigned int fuse[kFreshBufs];
+        // Consecutive K-blocks of one key form an interval (at most kIntervalKB K-blocks) that
+        // accumulates in one of the kAccBufs TMEM accumulators; closing it commits the
+        // accumulator's MMAs to fdone[b] and hands the accumulator to the epilogue.
+        int cur_key = -1;
+        int ob = 0, on = 0, next_buf = 0;
+        unsigned int fuse[kAccBufs];
 #pragma unroll
-        for (int b = 0; b < kFreshBufs; ++b) fuse[b] = 0;
+        for (int b = 0; b < kAccBufs; ++b) fuse[b] = 0;
         unsigned int ev_n = 0;
         int last_commit_stage = -1;
         unsigned int last_commit_parity = 0;
@@ -740,7 +741,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
         auto close_interval = [&]() {  // lane 0
             if (on > 0) {
                 mma_commit(smem_u32(&S.fdone[ob]));
-                push_event(Event{kEvMerge, ob, oc, 0, (int)(fuse[ob] & 1u)});
+                push_event(Event{kEvDrain, ob, cur_key, (int)(fuse[ob] & 1u)});
                 ++fuse[ob];
                 on = 0;
             }
@@ -769,25 +770,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
             state = __shfl_sync(0xffffffffu, state, 0);
             if (state <= 0) break;
             if (lane == 0 && !failed) {
-                const KBMeta m = S.meta[i % kMetaRing];
-                const int st = m.key / kTcBlocks;  // ntile2 is a multiple of kTcBlocks
-                const int c = m.key % kTcBlocks;
-                if (st != cur_st) {
-                    if (cur_st >= 0) {
-                        close_interval();
-                        push_event(Event{kEvFlush, 0, 0, cur_key, 0});
-                    }
-                    cur_st = st;
-                }
-                cur_key = m.key;
-                if (on > 0 && (c != oc || on == kFreshKB)) close_interval();
-                if (on == 0) {  // open a fresh interval on the next buffer, once its last merge is done
+                const int key = S.meta[i % kMetaRing].key;
+                if (on > 0 && (key != cur_key || on == kIntervalKB)) close_interval();
+                cur_key = key;
+                if (on == 0) {  // open an interval on the next accumulator, once the epilogue has read it
                     const int b = next_buf;
-                    next_buf = (next_buf + 1) % kFreshBufs;
+                    next_buf = (next_buf + 1) % kAccBufs;
                     if (fuse[b] > 0 && !mbar_wait(smem_u32(&S.ffree[b]), (fuse[b] - 1) & 1u, abort_flag))
                         failed = true;
                     ob = b;
-                    oc = c;
                 }
                 const int stg = (int)((i / kSubStages) % kPipe);
                 const unsigned int u = i / (kSubStages * kPipe);
@@ -798,18 +789,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
                 if (!failed && sub == kSubStages - 1) st_release(&S.consumed, i + 1);
                 if (!failed) {
                     tc_fence_after();
-                    const uint32_t d = tmem + (uint32_t)(kFreshCol0 + kN * ob);
-                    const uint32_t ah = smem_u32(smem + stg * kStageBytes + sub * kSubBytes), al = ah + kABytes;
-                    const uint32_t bh = al + kABytes, bl = bh + kBBytes;
-                    uint32_t acc = on > 0 ? 1u : 0u;
-#pragma unroll
-                    for (int k = 0; k < kKB / 16; ++k) {  // 16-element K steps: 2 K-groups = +256 bytes
-                        const uint32_t ko = (uint32_t)k * 256u;
-                        mma_f16(d, smem_desc(ah + ko), smem_desc(bh + ko), acc, idesc);
-                        acc = 1u;
-                        mma_f16(d, smem_desc(ah + ko), smem_desc(bl + ko), 1u, idesc);
-                        mma_f16(d, smem_desc(al + ko), smem_desc(bh + ko), 1u, idesc);
-                    }
+                    const uint32_t d = tmem + (uint32_t)(kN * ob);
+                    const uint32_t a = smem_u32(smem + stg * kStageBytes + sub * kSubBytes);
+                    const uint32_t b = a + 2 * kABytes;
+                    // one MMA per 16-sample K step: [A_hi; A_lo] x [B_hi | B_lo] gives all four
+                    // hi/lo products in the accumulator's quarters
+                    mma_f16(d, smem_desc(a), smem_desc(b), on > 0 ? 1u : 0u, idesc);
+                    mma_f16(d, smem_desc(a + 256u), smem_desc(b + 256u), 1u, idesc);
                     if (sub == kSubStages - 1) {  // all K-blocks of the stage issued
                         mma_commit(smem_u32(&S.empty[stg]));
                         last_commit_stage = stg;
@@ -834,11 +820,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
                 last_commit_stage = open_stage;
                 last_commit_parity = open_stage_parity;
             }
-            if (!failed && !*abort_flag && cur_st >= 0) {
-                close_interval();
-                push_event(Event{kEvFlush, 0, 0, cur_key, 0});
-            }
-            push_event(Event{kEvExit, 0, 0, 0, 0});
+            if (!failed && !*abort_flag) close_interval();
+            push_event(Event{kEvExit, 0, 0, 0});
             if (failed && !*abort_flag) {
                 atomicOr(P.status, 2u);
                 *abort_flag = 1;
@@ -853,9 +836,16 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
         __syncwarp();
     } else {
         // ============================ epilogue ============================
-        const int q = warp & 3;  // TMEM lane quarter: accumulator rows 16q .. 16q + 15 in lanes 0..15
+        // Warp q reads TMEM lane quarter q: lanes 0-15 hold accumulator rows 16q .. 16q + 15 of the
+        // A_hi products, lanes 16-31 the same rows of the A_lo products; columns 0-31 come from
+        // B_hi, 32-63 from B_lo (0-15 real, 16-31 imaginary within each). A lane adds its two column
+        // halves, the partner lane (lane ^ 16) supplies the other A half, and the pair emits the
+        // row's 16 complex cells to the moment plane (lanes 0-15 cells 0-7, lanes 16-31 cells 8-15),
+        // checkerboard sign and 1 / scale applied, zero cells skipped.
+        const int q = warp & 3;
         const uint32_t lane_addr = (uint32_t)(32 * q) << 16;
-        unsigned int run_valid = 0;
+        const int row = 16 * q + (lane & 15);
+        const int cell0 = (lane >> 4) * 8;
         for (unsigned int e = 0;; ++e) {
             bool ok = true;
             if (lane == 0) ok = wait_at_least(&S.ev_published, e + 1, abort_flag);
@@ -868,88 +858,55 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
             }
             const Event ev = S.events[e % kEventRing];
             if (ev.type == kEvExit) break;
-            if (ev.type == kEvMerge) {
-                bool dn = mbar_wait(smem_u32(&S.fdone[ev.buf]), (uint32_t)ev.parity, abort_flag);
-                dn = __all_sync(0xffffffffu, dn);
-                if (!dn) {
-                    if (lane == 0 && !*abort_flag) {
-                        atomicOr(P.status, 8u);
-                        *abort_flag = 1;
-                    }
-                    break;
+            bool dn = mbar_wait(smem_u32(&S.fdone[ev.buf]), (uint32_t)ev.parity, abort_flag);
+            dn = __all_sync(0xffffffffu, dn);
+            if (!dn) {
+                if (lane == 0 && !*abort_flag) {
+                    atomicOr(P.status, 8u);
+                    *abort_flag = 1;
                 }
-                tc_fence_after();
-                const uint32_t fa = tmem + lane_addr + (uint32_t)(kFreshCol0 + kN * ev.buf);
-                const uint32_t ra = tmem + lane_addr + (uint32_t)(kN * ev.blk);
-                const bool have_run = (run_valid >> ev.blk) & 1u;
-#pragma unroll 1
-                for (int c8 = 0; c8 < kN; c8 += 8) {  // eight columns at a time
-                    uint32_t f[8], rv[8];
-                    tmem_ld8(fa + (uint32_t)c8, f);
-                    if (have_run) tmem_ld8(ra + (uint32_t)c8, rv);
-                    tmem_ld_wait();
-                    if (have_run) {
+                break;
+            }
+            tc_fence_after();
+            const uint32_t base = tmem + lane_addr + (uint32_t)(kN * ev.buf);
+            float re[8], im[8];  // this lane's 8 cells of its row: real, imaginary
 #pragma unroll
-                        for (int jj = 0; jj < 8; ++jj)  // FP32 round-to-nearest
-                            f[jj] = __float_as_uint(__uint_as_float(f[jj]) + __uint_as_float(rv[jj]));
+            for (int half = 0; half < 2; ++half) {  // cells 0-7, then 8-15
+                uint32_t rh[8], rl[8], ih[8], il[8];
+                tmem_ld8(base + (uint32_t)(8 * half), rh);        // real, B_hi
+                tmem_ld8(base + (uint32_t)(32 + 8 * half), rl);   // real, B_lo
+                tmem_ld8(base + (uint32_t)(16 + 8 * half), ih);   // imaginary, B_hi
+                tmem_ld8(base + (uint32_t)(48 + 8 * half), il);   // imaginary, B_lo
+                tmem_ld_wait();
+#pragma unroll
+                for (int jj = 0; jj < 8; ++jj) {
+                    float xr = __uint_as_float(rh[jj]) + __uint_as_float(rl[jj]);
+                    float xi = __uint_as_float(ih[jj]) + __uint_as_float(il[jj]);
+                    xr += __shfl_xor_sync(0xffffffffu, xr, 16);
+                    xi += __shfl_xor_sync(0xffffffffu, xi, 16);
+                    if ((lane >> 4) == half) {
+                        re[jj] = xr;
+                        im[jj] = xi;
                     }
-                    tmem_st8(ra + (uint32_t)c8, f);
                 }
-                tmem_st_wait();
-                run_valid |= 1u << ev.blk;
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(smem_u32(&S.ffree[ev.buf]));
-            } else {  // flush the super-tile of ev.key
-                tc_fence_after();
-                const int slab = ev.key / tiles2;
-                const int t1 = (ev.key / g.ntile2) % g.ntile;
-                const int t2b = (ev.key % g.ntile2) / kTcBlocks * kTcBlocks;
-                const int row = 16 * q + (lane & 15);
-                const long long g1 = g.gmin + (long long)t1 * g.T + row;
-                const bool row_ok = lane < 16 && g1 <= g.gmax;
-                const long long o2 = g.gmin + (long long)t2b * g.T2;  // grid column of block 0, column 0
-                float2* plane = P.planes + (long long)(slab - P.slab_lo) * GG + (g1 - g.gmin) * g.G;
-                float cre[8], cim[8];
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&S.ffree[ev.buf]));  // the accumulator is read
+            const int slab = ev.key / tiles2;
+            const int t1 = (ev.key / g.ntile2) % g.ntile, t2 = ev.key % g.ntile2;
+            const long long g1 = g.gmin + (long long)t1 * g.T + row;
+            const long long o2 = g.gmin + (long long)t2 * g.T2 + cell0;
+            if (g1 <= g.gmax) {
+                float2* prow = P.planes + (long long)(slab - P.slab_lo) * GG + (g1 - g.gmin) * g.G - g.gmin;
 #pragma unroll
-                for (int jj = 0; jj < 8; ++jj) { cre[jj] = 0.0f; cim[jj] = 0.0f; }
-                auto emit = [&](long long g2, float re, float im) {
-                    if (row_ok && g2 <= g.gmax && (re != 0.0f || im != 0.0f)) {
+                for (int jj = 0; jj < 8; ++jj) {
+                    const long long g2 = o2 + jj;
+                    if (g2 <= g.gmax && (re[jj] != 0.0f || im[jj] != 0.0f)) {
                         const float sg = ((g1 + g2) & 1) ? -inv_scale : inv_scale;
-                        red_add_v2(plane + (g2 - g.gmin), sg * re, sg * im);
-                    }
-                };
-#pragma unroll 1
-                for (int c = 0; c < kTcBlocks; ++c) {
-                    // block c: columns 0..7 real / 16..23 imaginary overlap the carry of block c - 1;
-                    // columns 8..15 / 24..31 become the carry
-                    uint32_t re[8], im[8];
-                    const bool have = (run_valid >> c) & 1u;
-                    const uint32_t ba = tmem + lane_addr + (uint32_t)(kN * c);
-                    if (have) {
-                        tmem_ld8(ba, re);
-                        tmem_ld8(ba + 16u, im);
-                        tmem_ld_wait();
-                    }
-#pragma unroll
-                    for (int jj = 0; jj < 8; ++jj)
-                        emit(o2 + 8 * c + jj, cre[jj] + (have ? __uint_as_float(re[jj]) : 0.0f),
-                             cim[jj] + (have ? __uint_as_float(im[jj]) : 0.0f));
-                    if (have) {
-                        tmem_ld8(ba + 8u, re);
-                        tmem_ld8(ba + 24u, im);
-                        tmem_ld_wait();
-                    }
-#pragma unroll
-                    for (int jj = 0; jj < 8; ++jj) {
-                        cre[jj] = have ? __uint_as_float(re[jj]) : 0.0f;
-                        cim[jj] = have ? __uint_as_float(im[jj]) : 0.0f;
+                        red_add_v2(prow + g2, sg * re[jj], sg * im[jj]);
                     }
                 }
-#pragma unroll
-                for (int jj = 0; jj < 8; ++jj) emit(o2 + 8 * kTcBlocks + jj, cre[jj], cim[jj]);
-                run_valid = 0;
-                tc_fence_before();
             }
             __syncwarp();
             if (lane == 0) st_release(&S.ev_consumed[q], e + 1);
@@ -976,9 +933,8 @@ int launch_grid_tc(const SampleRec* d_rec, const unsigned int* d_offsets, const 
         set_error("tensor-core gridder: bad key range");
         return SVDI_ERR_INTERNAL;
     }
-    if (g.W > 8 || (g.W & 1) || g.T != kTcTileRows || g.T2 != kTcTileCols || (g.ntile2 % kTcBlocks) != 0 ||
-        (key_lo % kTcBlocks) != 0) {
-        set_error("tensor-core gridder: needs even support <= 8 and 56 x 8 tiles in groups of 4");
+    if (g.W > 8 || (g.W & 1) || g.T != kTcTileRows || g.T2 != kTcTileCols) {
+        set_error("tensor-core gridder: needs even support <= 8 and 56 x 8 tiles");
         return SVDI_ERR_UNSUPPORTED;
     }
     if (reinterpret_cast<uintptr_t>(d_rec) % 16 != 0) {
