@@ -124,26 +124,14 @@ __device__ inline SplatTarget reproject_fipk(long long idx, long long idy, long 
     return {oi0 - (double)half, oi1 - (double)half, true};
 }
 
+// One pixel (x, y) of the rotated frame: moments -> |Re sum| -> grid correction -> reprojection.
 template <int KMAX>
-__global__ void __launch_bounds__(256) k_recombine(const float2* __restrict__ moments, GridGeom g, long long N,
-                                                  double cell, const double* __restrict__ vin,
-                                                  SlabParams sp, const float* __restrict__ corr,
-                                                  double inv_n, int reprojection, int presplat,
-                                                  float* __restrict__ out, double* __restrict__ acc,
-                                                  int final_batch, const DevPlan* __restrict__ plan,
-                                                  const unsigned long long* __restrict__ nonfinite) {
-    if (plan) {  // one batch of all slabs: the device plan's slab geometry
-        sp.r3_min = plan->sp.r3_min;
-        sp.slab_width = plan->sp.slab_width;
-        sp.slab_half = plan->sp.slab_half;
-        sp.inv_half = plan->sp.inv_half;
-    }
-    __shared__ ReprojConst kc;
-    if (threadIdx.x == 0 && threadIdx.y == 0) kc = reproj_const(vin, cell);
-    __syncthreads();
-    const long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const long long y = blockIdx.y * (long long)blockDim.y + threadIdx.y;
-    if (x >= N || y >= N) return;
+__device__ __forceinline__ void recombine_pixel(long long x, long long y, const float2* __restrict__ moments,
+                                                const GridGeom& g, long long N, double cell,
+                                                const double* __restrict__ vin, const SlabParams& sp,
+                                                const float* __restrict__ corr, double inv_n, int reprojection,
+                                                int presplat, float* __restrict__ out, double* __restrict__ acc,
+                                                int final_batch, bool bad, const ReprojConst& kc) {
     double V[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) V[k] = vin[k];
@@ -194,7 +182,7 @@ __global__ void __launch_bounds__(256) k_recombine(const float2* __restrict__ mo
     double value = fabs(signed_sum) * inv_n;
     // a NaN or Inf among the gridded values: every moment cell would be NaN after the FFT, so every
     // valid pixel is NaN (the reference's float atomics, SVDIntegratedImager.cu:1276-1290, carry it)
-    if (nonfinite && *nonfinite) value = __longlong_as_double(0x7ff8000000000000LL);
+    if (bad) value = __longlong_as_double(0x7ff8000000000000LL);
     if (presplat) {
         out[y * N + x] = (float)value;
         return;
@@ -213,6 +201,36 @@ __global__ void __launch_bounds__(256) k_recombine(const float2* __restrict__ mo
     atomicAdd(&d[(long long)Mc * N + (long long)Lc], (float)((0 + LL - Lf) * (0 + MM - Mf) * value));
 }
 
+// Persistent over 32 x 8 pixel tiles: the per-launch constants (slab geometry, reprojection
+// constants, the non-finite flag) are set up once per block.
+template <int KMAX>
+__global__ void __launch_bounds__(256, 4) k_recombine(const float2* __restrict__ moments, GridGeom g, long long N,
+                                                  double cell, const double* __restrict__ vin,
+                                                  SlabParams sp, const float* __restrict__ corr,
+                                                  double inv_n, int reprojection, int presplat,
+                                                  float* __restrict__ out, double* __restrict__ acc,
+                                                  int final_batch, const DevPlan* __restrict__ plan,
+                                                  const unsigned long long* __restrict__ nonfinite) {
+    if (plan) {  // one batch of all slabs: the device plan's slab geometry
+        sp.r3_min = plan->sp.r3_min;
+        sp.slab_width = plan->sp.slab_width;
+        sp.slab_half = plan->sp.slab_half;
+        sp.inv_half = plan->sp.inv_half;
+    }
+    __shared__ ReprojConst kc;
+    if (threadIdx.x == 0 && threadIdx.y == 0) kc = reproj_const(vin, cell);
+    __syncthreads();
+    const bool bad = nonfinite && *nonfinite;
+    const long long ntx = (N + 31) / 32, nty = (N + 7) / 8;
+    for (long long t = blockIdx.x; t < ntx * nty; t += gridDim.x) {
+        const long long ty = t / ntx, tx = t - ty * ntx;
+        const long long x = tx * 32 + threadIdx.x, y = ty * 8 + threadIdx.y;
+        if (x < N && y < N)
+            recombine_pixel<KMAX>(x, y, moments, g, N, cell, vin, sp, corr, inv_n, reprojection, presplat, out, acc,
+                                  final_batch, bad, kc);
+    }
+}
+
 }  // namespace
 
 int launch_recombine(const float2* d_moments, const GridGeom& g, long long N, double cell,
@@ -221,7 +239,8 @@ int launch_recombine(const float2* d_moments, const GridGeom& g, long long N, do
                      cudaStream_t st, double* d_acc, bool final_batch, const DevPlan* d_plan,
                      const unsigned long long* d_nonfinite) {
     const dim3 block(32, 8);
-    const dim3 grid((unsigned)((N + 31) / 32), (unsigned)((N + 7) / 8));
+    const long long tiles = ((N + 31) / 32) * ((N + 7) / 8);
+    const dim3 grid((unsigned)std::min<long long>(tiles, 8LL * current_sm_count()));
     if (sp.K <= 1) k_recombine<1><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out, d_acc, final_batch ? 1 : 0, d_plan, d_nonfinite);
     else if (sp.K <= 8) k_recombine<8><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out, d_acc, final_batch ? 1 : 0, d_plan, d_nonfinite);
     else if (sp.K <= 16) k_recombine<16><<<grid, block, 0, st>>>(d_moments, g, N, cell, d_vin64, sp, d_corr, inv_n_total, reprojection, presplat, d_out, d_acc, final_batch ? 1 : 0, d_plan, d_nonfinite);
