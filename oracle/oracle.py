@@ -189,8 +189,9 @@ def k_for_target(a, target, kmax=64):
 
 def slab_config_target(r3, vin, N, cell, target_error=1e-6):
     """Error-target rule of the B200 engine (not in the reference): the slab count n in 1..64 that
-    minimises the moment planes n * K, K the smallest order whose truncation bound at the slab's
-    alpha is <= target_error; slab geometry as SII:973-991."""
+    minimises the moment planes n * K (on ties the larger n, i.e. the smaller K), K the smallest
+    order whose truncation bound at the slab's alpha is <= target_error; slab geometry as
+    SII:973-991."""
     r3_min, r3_max = float(np.min(r3)), float(np.max(r3))
     mt3, _ = t3_stats(vin, N, cell)
     half_range = max(0.5 * (r3_max - r3_min), 1.0e-6)
@@ -202,7 +203,7 @@ def slab_config_target(r3, vin, N, cell, target_error=1e-6):
         K = k_for_target(2.0 * math.pi * mt3 * h, target_error)
         if K < 0:
             continue
-        if n * K < best_p:
+        if n * K <= best_p:  # equal plane counts: the smaller K (more slabs)
             best_p, best_n = n * K, n
         if K == 1:
             break

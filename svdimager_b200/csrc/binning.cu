@@ -70,77 +70,127 @@ __global__ void __launch_bounds__(kThreads) k_histogram(SampleSource src, GridGe
 
 // Exclusive scan of the key counts (one block): offsets[0..n_keys], cursor = offsets. With
 // kb_offsets, also the exclusive scan of ceil(count / kb_size): the K-blocks of kb_size records of
-// one key each that the tensor-core gridder splits evenly over its CTAs.
+// one key each that the tensor-core gridder splits evenly over its CTAs. With chunk_key, for every
+// chunk of chunk_size records the key its first record belongs to.
+// The keys go through shared memory in tiles of kScanTile (coalesced loads and stores), each thread
+// scanning kScanPer consecutive keys of a tile and the block combining the 1024 thread sums with warp
+// shuffles; a running carry links the tiles.
+constexpr int kScanPer = 4;               // keys (or chunks) per thread and tile
+constexpr int kScanTile = kScanPer * 1024;
+
+// Inclusive block-wide scan (sum or max) of one value per thread of a 1024-thread block; `tmp`
+// holds 32 words of shared memory. Returns this thread's inclusive result and the block total.
+template <bool kMax>
+__device__ __forceinline__ unsigned int block_scan(unsigned int v, unsigned int* tmp, unsigned int& total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v = kMax ? max(v, u) : v + u;
+    }
+    if (lane == 31) tmp[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        unsigned int x = tmp[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned int u = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x = kMax ? max(x, u) : x + u;
+        }
+        tmp[lane] = x;
+    }
+    __syncthreads();
+    if (w > 0) v = kMax ? max(v, tmp[w - 1]) : v + tmp[w - 1];
+    total = tmp[31];
+    __syncthreads();
+    return v;
+}
+
 __global__ void __launch_bounds__(1024) k_scan(const unsigned int* __restrict__ counts, int n_keys,
                                               unsigned int* __restrict__ offsets,
                                               unsigned int* __restrict__ cursor,
                                               unsigned int* __restrict__ kb_offsets, int kb_size,
                                               unsigned int* __restrict__ chunk_key, int chunk_size) {
-    __shared__ unsigned int part[1024];
-    __shared__ unsigned int kpart[1024];
+    __shared__ __align__(16) unsigned int tile[kScanTile];
+    __shared__ __align__(16) unsigned int ktile[kScanTile];
+    __shared__ unsigned int tmp[32];
     const int t = threadIdx.x;
-    const int per = (n_keys + 1023) / 1024;
-    const int b = t * per, e = min(n_keys, b + per);
-    unsigned int s = 0, ks = 0;
-    for (int k = b; k < e; ++k) {
-        const unsigned int c = counts[k];
-        s += c;
-        ks += (c + kb_size - 1) / kb_size;
-    }
-    part[t] = s;
-    kpart[t] = ks;
-    __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-        const unsigned int v = (t >= off) ? part[t - off] : 0u;
-        const unsigned int kv = (t >= off) ? kpart[t - off] : 0u;
-        __syncthreads();
-        part[t] += v;
-        kpart[t] += kv;
+    unsigned int carry = 0, kcarry = 0;
+    if (chunk_key) {  // chunks are marked below: clear the table first (needs the record total)
+        unsigned int sum = 0, total = 0;
+        for (int k = t; k < n_keys; k += 1024) sum += counts[k];
+        block_scan<false>(sum, tmp, total);
+        const unsigned int n_chunks = (total + chunk_size - 1) / chunk_size;
+        for (unsigned int ch = t; ch < n_chunks; ch += 1024) chunk_key[ch] = 0u;
         __syncthreads();
     }
-    const unsigned int total = part[1023];
-    const unsigned int n_chunks = chunk_key ? (total + chunk_size - 1) / chunk_size : 0u;
-    for (unsigned int ch = t; ch < n_chunks; ch += 1024) chunk_key[ch] = 0u;
-    __syncthreads();
-    unsigned int run = part[t] - s, krun = kpart[t] - ks;
-    for (int k = b; k < e; ++k) {
-        const unsigned int c = counts[k];
-        offsets[k] = run;
-        cursor[k] = run;
-        if (chunk_key && c) {  // marks the first chunk that starts inside this key's records
-            const unsigned int ch = (run + chunk_size - 1) / chunk_size;
-            if ((unsigned long long)ch * chunk_size < (unsigned long long)run + c) chunk_key[ch] = (unsigned int)k;
+    for (int base = 0; base < n_keys; base += kScanTile) {
+        const int n = min(kScanTile, n_keys - base);
+        for (int i = t; i < kScanTile; i += 1024) tile[i] = i < n ? counts[base + i] : 0u;
+        __syncthreads();
+        unsigned int c[kScanPer], s = 0, ks = 0;
+#pragma unroll
+        for (int k = 0; k < kScanPer; ++k) {
+            c[k] = tile[kScanPer * t + k];
+            s += c[k];
+            ks += (c[k] + kb_size - 1) / kb_size;
         }
-        run += c;
-        if (kb_offsets) {
-            kb_offsets[k] = krun;
-            krun += (c + kb_size - 1) / kb_size;
+        unsigned int tot = 0, ktot = 0;
+        const unsigned int incl = block_scan<false>(s, tmp, tot);
+        const unsigned int kincl = kb_offsets ? block_scan<false>(ks, tmp, ktot) : 0u;
+        unsigned int run = carry + incl - s, krun = kcarry + kincl - ks;
+#pragma unroll
+        for (int k = 0; k < kScanPer; ++k) {
+            const int key = base + kScanPer * t + k;
+            if (chunk_key && c[k] && key < n_keys) {  // the first chunk that starts inside this key's records
+                const unsigned int ch = (run + chunk_size - 1) / chunk_size;
+                if ((unsigned long long)ch * chunk_size < (unsigned long long)run + c[k]) chunk_key[ch] = (unsigned int)key;
+            }
+            tile[kScanPer * t + k] = run;
+            run += c[k];
+            ktile[kScanPer * t + k] = krun;
+            krun += (c[k] + kb_size - 1) / kb_size;
         }
+        __syncthreads();
+        for (int i = t; i < n; i += 1024) {
+            offsets[base + i] = tile[i];
+            cursor[base + i] = tile[i];
+            if (kb_offsets) kb_offsets[base + i] = ktile[i];
+        }
+        carry += tot;
+        kcarry += ktot;
+        __syncthreads();
     }
-    if (t == 1023) {
-        offsets[n_keys] = part[1023];
-        if (kb_offsets) kb_offsets[n_keys] = kpart[1023];
+    if (t == 0) {
+        offsets[n_keys] = carry;
+        if (kb_offsets) kb_offsets[n_keys] = kcarry;
     }
     if (!chunk_key) return;
     // chunks without a mark start inside the key of the last mark before them: a running maximum
-    // (keys increase along the records) over contiguous chunk ranges, then across threads
+    // (keys increase along the records), in tiles with a carry
     __syncthreads();
-    const unsigned int cper = (n_chunks + 1023) / 1024;
-    const unsigned int cb = t * cper, ce = min(n_chunks, cb + cper);
-    unsigned int m = 0;
-    for (unsigned int ch = cb; ch < ce; ++ch) m = max(m, chunk_key[ch]);
-    part[t] = m;
-    __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-        const unsigned int v = (t >= off) ? part[t - off] : 0u;
+    const unsigned int n_chunks = (carry + chunk_size - 1) / chunk_size;
+    unsigned int mcarry = 0;
+    for (unsigned int base = 0; base < n_chunks; base += kScanTile) {
+        const unsigned int n = min((unsigned int)kScanTile, n_chunks - base);
+        for (unsigned int i = t; i < (unsigned int)kScanTile; i += 1024) tile[i] = i < n ? chunk_key[base + i] : 0u;
         __syncthreads();
-        part[t] = max(part[t], v);
+        unsigned int v[kScanPer], m = 0;
+#pragma unroll
+        for (int k = 0; k < kScanPer; ++k) {
+            m = max(m, tile[kScanPer * t + k]);
+            v[k] = m;
+        }
+        unsigned int tot = 0;
+        ktile[t] = block_scan<true>(m, tmp, tot);  // inclusive maximum over threads 0..t
         __syncthreads();
-    }
-    m = t ? part[t - 1] : 0u;
-    for (unsigned int ch = cb; ch < ce; ++ch) {
-        m = max(m, chunk_key[ch]);
-        chunk_key[ch] = m;
+        const unsigned int before = max(mcarry, t ? ktile[t - 1] : 0u);
+#pragma unroll
+        for (int k = 0; k < kScanPer; ++k) tile[kScanPer * t + k] = max(before, v[k]);
+        __syncthreads();
+        for (unsigned int i = t; i < n; i += 1024) chunk_key[base + i] = tile[i];
+        mcarry = max(mcarry, tot);
+        __syncthreads();
     }
 }
 

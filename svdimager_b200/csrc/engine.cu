@@ -295,13 +295,15 @@ int choose_slabs(svdi_engine* e, bool archive, double r3min, double r3max, doubl
     if (!archive) {  // SVDIntegratedImager.cu:973-991
         const double r3_range = std::max(r3max - r3min, 2.0e-6);
         if (o.k_rule == SVDI_KRULE_TARGET && o.target_alpha <= 0) {
-            // minimise the number of moment planes nslab * K(alpha_slab) at the error target
+            // minimise the number of moment planes nslab * K(alpha_slab) at the error target; among
+            // equal plane counts take the smallest K (a sample is gridded into K planes of its slab,
+            // so fewer terms and more slabs grid the same planes with less work)
             int best_n = 1, best_p = 1 << 30;
             for (int n = 1; n <= 64; ++n) {
                 const double h = std::max(0.5 * r3_range / n, 1.0e-6);
                 const int K = k_for_target(2.0 * kPi * mt3 * h, o.target_error);
                 if (K < 0) continue;
-                if (n * K < best_p) {
+                if (n * K <= best_p) {
                     best_p = n * K;
                     best_n = n;
                 }
