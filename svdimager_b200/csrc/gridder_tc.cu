@@ -43,19 +43,20 @@
 // Tiles. Binning uses 56-row x 8-column tiles (footprint origins); an accumulator covers the tile's
 // 64 rows (56 + halo) and 16 columns (8 + halo).
 //
-// Roles (two CTAs per SM, 10 warps, 256 TMEM columns each):
-//   warps 0-3   producers: warp w fills sub-stage w of the two pipeline stages in turn with K-blocks
-//               j = w, w + 4, w + 8, ... (one thread per sample); the four warps arrive on
+// Roles (two CTAs per SM, 14 warps, 256 TMEM columns each):
+//   warps 0-7   producers: warps w and w + 4 fill sub-stage w of the two pipeline stages in turn
+//               with K-blocks j = w, w + 4, w + 8, ... (one thread per sample), warp w the A'
+//               column and warp w + 4 the B' column of each sample; the eight warps arrive on
 //               full[stage]; a stage is reused once the MMAs of its previous round commit to
 //               empty[stage].
-//   warp 4      scheduler: walks the CTA's share of the K-blocks (runs of up to 32 records of one
+//   warp 8      scheduler: walks the CTA's share of the K-blocks (runs of up to 32 records of one
 //               key), publishes their descriptors to a ring and stages each K-block's records
 //               (one contiguous run of 16-byte records) into shared memory with a bulk copy
 //               (cp.async.bulk, this GPU's own memory, no multicast) that completes on the record
 //               slot's mbarrier.
-//   warp 5      MMA issuer: issues the MMAs, opens and closes intervals and posts a drain event
+//   warp 9      MMA issuer: issues the MMAs, opens and closes intervals and posts a drain event
 //               per interval.
-//   warps 6-9   epilogue: TMEM lane quarter (warp % 4); drain the intervals in event order.
+//   warps 10-13 epilogue: TMEM lane quarter (warp % 4); drain the intervals in event order.
 // The scheduler warps take chunks of 32 K-blocks from a global counter (a chunk can start and end
 // inside a tile).
 //
@@ -87,12 +88,13 @@ constexpr int kM = 2 * kRows;           // MMA rows: A_hi rows, then A_lo rows
 constexpr int kN = 2 * kCols;           // MMA columns: B_hi columns, then B_lo columns
 constexpr int kSubStages = 4;           // K-blocks per pipeline stage (one per producer warp)
 constexpr int kPipe = 2;                // pipeline stages
-constexpr int kProdWarps = kSubStages;                     // 4: warp w fills sub-stage w of both stages
-constexpr int kSchedWarp = kProdWarps;                     // 4
-constexpr int kMmaWarp = kProdWarps + 1;                   // 5
-constexpr int kEpiWarp0 = kProdWarps + 2;                  // 6..9
+// producers: warp w < kSubStages writes A' of sub-stage w, warp kSubStages + w its B'
+constexpr int kProdWarps = 2 * kSubStages;                 // 8
+constexpr int kSchedWarp = kProdWarps;                     // 8
+constexpr int kMmaWarp = kProdWarps + 1;                   // 9
+constexpr int kEpiWarp0 = kProdWarps + 2;                  // 10..13
 constexpr int kWarps = kProdWarps + 2 + 4;
-constexpr int kThreads = kWarps * 32;                      // 320
+constexpr int kThreads = kWarps * 32;                      // 448
 constexpr int kAccBufs = 4;             // TMEM accumulators of kN columns
 constexpr int kIntervalKB = 16;         // K-blocks (32 MMAs) per accumulator interval at most
 constexpr int kTmemCols = 256;
@@ -373,7 +375,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
     const unsigned int kb_lo = P.kb_offsets[P.key_lo], kb_hi = P.kb_offsets[P.key_hi];
     if (tid == 0) {
         for (int s = 0; s < kPipe; ++s) {
-            mbar_init(smem_u32(&S.full[s]), kSubStages);
+            mbar_init(smem_u32(&S.full[s]), kProdWarps);
             mbar_init(smem_u32(&S.empty[s]), 1);
         }
         for (int s = 0; s < kRecSlots; ++s) mbar_init(smem_u32(&S.rec_full[s]), 1);
@@ -410,16 +412,20 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
 
     if (warp < kProdWarps) {
         // =========================== producers ===========================
-        // warp -> sub-stage; lane -> sample (K-slot) of the K-block; round `it` uses stage it % 2
+        // warp -> sub-stage (warp % 4) and operand (A' for warps 0-3, B' for warps 4-7); lane ->
+        // sample (K-slot) of the K-block; round `it` uses stage it % 2. The A' warp also adds the
+        // rare samples to the plane.
+        const int sw = warp % kSubStages;
+        const bool a_role = warp < kSubStages;
         const int kofs = (lane & 7) * 16 + (lane >> 3) * 128;  // byte offset of this K-slot's 16-byte row
         int oldj0 = -1, oldj1 = -1;  // first A chunk of this lane's previous sample per stage (-1: none)
         int pub_seen = 0;  // lane 0: published count last read (acquire)
         bool failed = false;
         for (int it = 0;; ++it) {
-            const int j = it * kProdWarps + warp;
+            const int j = it * kSubStages + sw;
             const int stg = it & 1;
             const int use = it >> 1;  // earlier rounds of this stage
-            unsigned char* const A = smem + stg * kStageBytes + warp * kSubBytes;  // A_hi and A_lo rows
+            unsigned char* const A = smem + stg * kStageBytes + sw * kSubBytes;  // A_hi and A_lo rows
             unsigned char* const B_hi = A + 2 * kABytes;
             unsigned char* const B_lo = B_hi + kBBytes;
             // wait until K-block j is published or the schedule ends before it (warp-uniform)
@@ -444,7 +450,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
                 // the schedule holds T = sdv - 1 K-blocks: when a stage-mate has one in this round, this
                 // warp still arrives (after the stage is free, so the arrival counts for this use)
                 const unsigned int T = __shfl_sync(0xffffffffu, sdv, 0) - 1;
-                if ((unsigned int)(it * kProdWarps) < T) {
+                if ((unsigned int)(it * kSubStages) < T) {
                     bool ok = true;
                     if (use > 0) ok = mbar_wait(smem_u32(&S.empty[stg]), (uint32_t)((use - 1) & 1), abort_flag);
                     if (__all_sync(0xffffffffu, ok)) {
@@ -477,7 +483,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
             const int r0 = cx - (HW - 1), c0 = cy - (HW - 1);
             const bool rare = valid && (fxq == 0 || fyq == 0 || r0 < 0 || c0 < 0 || r0 >= g.T || c0 >= g.T2);
             const bool fast = valid && !rare;
-            if (rare) {  // exact ES weights straight to the moment plane
+            if (rare && a_role) {  // exact ES weights straight to the moment plane
                 const int slab = m.key / tiles2;
                 const int t1 = (m.key / g.ntile2) % g.ntile, t2 = m.key % g.ntile2;
                 const long long o1 = g.gmin + (long long)t1 * g.T, o2 = g.gmin + (long long)t2 * g.T2;
@@ -497,7 +503,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
                 }
             }
             // ---- A: row taps (256 wx), chunks j0 and j0 + 1 at offset r0 % 8
-            {
+            if (a_role) {
                 const float ux = fmaf(2.0f, (float)fxq * (1.0f / 16777216.0f), -1.0f);
                 float a[8];
 #pragma unroll
@@ -535,7 +541,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
                 else oldj0 = fast ? j0 : -1;
             }
             // ---- B: column taps times the visibility (real: chunks 0-1, imaginary: chunks 2-3)
-            {
+            else {
                 const float uy = fmaf(2.0f, (float)fyq * (1.0f / 16777216.0f), -1.0f);
                 float wy[8];
 #pragma unroll
