@@ -822,7 +822,7 @@ def main():
     ap.add_argument("--no-batching", action="store_true")
     ap.add_argument("--no-widefield", action="store_true")
     ap.add_argument("--batch-snapshots", type=int, default=256)
-    ap.add_argument("--lanes", type=int, default=2,
+    ap.add_argument("--lanes", type=int, default=3,
                     help="engines (each on its own stream) taking the snapshots in turn in the throughput loop")
     ap.add_argument("--no-fipipe", action="store_true", help="skip the archive-entry (FIpipe) timing")
     ap.add_argument("--no-ref-binary", action="store_true",

@@ -22,60 +22,45 @@ struct SplatTarget {
 
 // Per-launch constants of the deprojection, computed once per block from Vin.
 struct ReprojConst {
-    double xi, eta;     // V[6] / V[8], V[7] / V[8]
     double inv_v8;      // 1 / |V[8]|
-    double dc, inv_dc;  // cell in degrees and its reciprocal
+    double dc_r0_sq;    // (cell in degrees / r0)^2, r0 = 180 / pi
+    float xi_f, eta_f;  // V[6] / V[8], V[7] / V[8]
+    float r0_dc;        // r0 / cell in degrees
 };
 
 __device__ inline ReprojConst reproj_const(const double* V, double dc_rad) {
     ReprojConst c;
-    c.xi = V[6] / V[8];
-    c.eta = V[7] / V[8];
+    const double r0 = 180.0 / kPi, dc = dc_rad / kPi * 180.0;
     c.inv_v8 = 1.0 / fabs(V[8]);
-    c.dc = dc_rad / kPi * 180.0;
-    c.inv_dc = 1.0 / c.dc;
+    c.dc_r0_sq = (dc / r0) * (dc / r0);
+    c.xi_f = (float)(V[6] / V[8]);
+    c.eta_f = (float)(V[7] / V[8]);
+    c.r0_dc = (float)(r0 / dc);
     return c;
 }
 
-// SVDIntegratedImager.cu:1325-1379 (simplified SIN deprojection; keeps p1, p2 when h > r0), with
-// the divisions by per-launch constants as products by their reciprocals and one 1 / h.
+// SVDIntegratedImager.cu:1325-1379 (simplified SIN deprojection; keeps p1, p2 when h > r0). With
+// (x, y) the pixel's offset in degrees and h = |(x, y)|, the reference normalises (x, y) by h,
+// scales it back by r = h and adds z r0 (xi, eta), z = 1 - sqrt(1 - (h / r0)^2): the target is
+// (p1, p2) moved by z r0 (-xi, eta) / dc pixels. That is evaluated here directly: (p1, p2) in FP64,
+// the displacement (at most some tens of pixels) in FP32 with z in the cancellation-free form
+// s / (1 + sqrt(1 - s)), s = (h / r0)^2 -- no square root or division in FP64 per pixel.
 __device__ inline SplatTarget reproject_sii(long long idx, long long idy, long long N, const ReprojConst& k,
                                             const double* V) {
-    const double r0 = 180.0 / kPi, inv_r0 = kPi / 180.0;
     const double di2 = (double)N * 0.5;
     const long long half = N / 2;
     const double idxf = (double)idx - di2, idyf = (double)idy - di2;
     const double p1 = (-V[0] * idxf + V[3] * idyf) * k.inv_v8 + di2;
     const double p2 = (-V[1] * idxf + V[4] * idyf) * k.inv_v8 + di2;
-    double x = -k.dc * (p1 - (di2 + 1.0));
-    double y = k.dc * (p2 - (di2 + 1.0));
-    const double h = sqrt(fma(x, x, y * y)), hr0 = h * inv_r0;
-    if (h != 0.0) {
-        const double ih = 1.0 / h;
-        x *= ih;
-        y *= -ih;
-    } else {
-        x = 0.0;
-        y = 1.0;
-    }
-    double oi0, oi1;
-    if (h <= r0) {
-        const double r = h;
-        const double sq = sqrt(1.0 - hr0 * hr0);
-        const double z = (h < r0 * sqrt(0.5)) ? 1.0 - sq : hr0 * hr0 / (1.0 + sq);
-        const double w = k.xi * k.xi + k.eta * k.eta;
-        if (w == 0.0) {
-            x = r * x;
-            y = -r * y;
-        } else {
-            x = r * x + z * r0 * k.xi;
-            y = -r * y + z * r0 * k.eta;
-        }
-        oi0 = -x * k.inv_dc + di2 + 1.0;
-        oi1 = y * k.inv_dc + di2 + 1.0;
-    } else {
-        oi0 = p1;
-        oi1 = p2;
+    const double xo = p1 - (di2 + 1.0), yo = p2 - (di2 + 1.0);  // offset in pixels
+    const double s = fma(xo, xo, yo * yo) * k.dc_r0_sq;          // (h / r0)^2
+    double oi0 = p1, oi1 = p2;
+    if (s <= 1.0) {  // h <= r0
+        const float sf = (float)s;
+        const float z = sf / (1.0f + sqrtf(1.0f - sf));
+        const float m = z * k.r0_dc;
+        oi0 = p1 - (double)(m * k.xi_f);
+        oi1 = p2 + (double)(m * k.eta_f);
     }
     return {oi0 - (double)half, oi1 - (double)half, true};
 }
@@ -153,8 +138,16 @@ __device__ __forceinline__ void recombine_pixel(long long x, long long y, const 
     double sum = 0.0;
     for (int j = 0; j < sp.nslab; ++j) {
         const double centre = sp.r3_min + ((double)j + 0.5) * sp.slab_width;
+        const double ph = 2.0 * t3 * centre;     // e^{i pi ph}
         double sb, cb;
-        sincospi(2.0 * t3 * centre, &sb, &cb);   // e^{i 2 pi t3 centre}
+        if (fabs(ph) < 0x1p-8) {  // small phase: FP32 is exact to ~1e-7 of ph, far below 1e-9 rad
+            float sf, cf;
+            sincospif((float)ph, &sf, &cf);
+            sb = (double)sf;
+            cb = (double)cf;
+        } else {
+            sincospi(ph, &sb, &cb);
+        }
         const float2* mp = moments + (long long)j * K * GG + gidx;
         for (int n = 0; n < K; ++n) {
             const float2 m = mp[(long long)n * GG];
