@@ -163,6 +163,12 @@ def serving_phase(api, big, n_requests, rate, device, seed=5, gridder=0):
             "sustained_snapshots_per_s": round(n_requests / wall, 2)}
 
 
+GRIDDER_DTYPE = {"tc": "f16 hi+lo operands, f32 accumulation", "tc_bf16": "bf16 hi+lo operands, f32 accumulation",
+                 "tc_i8": "u8 x s8 operands (22-bit fixed point as three byte digits), s32 accumulation"}
+GRIDDER_LABEL = {"tc": "tcgen05 split-precision (FP16 hi+lo)", "tc_bf16": "tcgen05 split-precision (BF16 hi+lo)",
+                 "tc_i8": "tcgen05 exact integer (kind::i8, three byte digits)"}
+
+
 def algorithmic_bytes(n_samples, n_rows, n_chan, planes, G, N):
     """Algorithmic bytes of one snapshot: 26 B per sample (two polarisations complex64, two flag
     bytes, two weights), 24 B per row (FP64 uvw), 8 B per channel, 32 B per moment-plane cell (one
@@ -394,7 +400,8 @@ def run_ours(args):
     host_cpus = replicas.bind_host_to_gpu(local)  # pinned buffers on the GPU's NUMA node
     snap = make_workload(args.config, rank)
     N, cell = snap.image_size, snap.cell_size
-    gridder = {"tc": api.GRIDDER_TC, "tc_bf16": api.GRIDDER_TC_BF16}.get(args.gridder, api.GRIDDER_FP32)
+    gridder = {"tc": api.GRIDDER_TC, "tc_bf16": api.GRIDDER_TC_BF16, "tc_i8": api.GRIDDER_TC_I8}.get(
+        args.gridder, api.GRIDDER_FP32)
     opts = dict(device=local, edge_mode=api.EDGE_STRICT, k_rule=api.KRULE_TARGET, target_error=1e-6,
                 gridder=gridder)
     eng = api.Engine(**opts)
@@ -505,7 +512,8 @@ def run_ours(args):
     dom = max(ours, key=ours.get)
     if dom == "ms_grid":
         alg = grid_kernel_bytes(st["num_gridded"], planes, G)
-        name = ("k_grid_tc" if st["used_tc"] else "k_grid_fp32") + " (+ plane zeroing)"
+        name = (("k_grid_i8" if args.gridder == "tc_i8" else "k_grid_tc") if st["used_tc"] else "k_grid_fp32") \
+            + " (+ plane zeroing)"
     elif dom == "ms_bin":
         alg = (26 + 8) * snap.num_samples + 16 * st["num_gridded"]
         name = "k_histogram_sep + k_scan + k_scatter_sep"
@@ -536,14 +544,12 @@ def run_ours(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": ("bf16 hi+lo operands, f32 accumulation" if args.gridder == "tc_bf16" else
-                  "f16 hi+lo operands, f32 accumulation") if st["used_tc"] else "f32",
+        "dtype": GRIDDER_DTYPE[args.gridder] if st["used_tc"] else "f32",
         "data": "synthetic (seeded; 512-station layout, 220-source sky, noise, flags, weights)",
         "config": {
             "workload": f"{args.config}: {snap.num_rows} baselines x {snap.num_channels} channels = "
                         f"{snap.num_samples} vis, one snapshot, {N}^2 image, cell {cell} rad",
-            "gridder": ("tcgen05 split-precision (" + ("BF16" if args.gridder == "tc_bf16" else "FP16") + " hi+lo)")
-                       if st["used_tc"] else "fp32 fixed-point",
+            "gridder": GRIDDER_LABEL[args.gridder] if st["used_tc"] else "fp32 fixed-point",
             "grid": G, "planes": planes, "num_slabs": st["num_slabs"], "chebyshev_terms": st["num_terms"],
             "support": 8, "beta": 15.3704324328, "oversampling": 1.5, "tile": st["tile"],
             "k_rule": "target 1e-6", "edges": "strict (samples whose footprint leaves the grid are dropped)",
@@ -827,8 +833,9 @@ def main():
     ap.add_argument("--no-fipipe", action="store_true", help="skip the archive-entry (FIpipe) timing")
     ap.add_argument("--no-ref-binary", action="store_true",
                     help="reference arm: skip timing the reference's own GPU imager")
-    ap.add_argument("--gridder", default="fp32", choices=["tc", "tc_bf16", "fp32"],
+    ap.add_argument("--gridder", default="fp32", choices=["tc", "tc_bf16", "tc_i8", "fp32"],
                     help="tc: split-precision tcgen05 gridder (FP16 hi+lo); tc_bf16: the same with BF16 hi+lo; "
+                         "tc_i8: exact integer tcgen05 gridder (three byte digits, int32 sums); "
                          "fp32: CUDA-core fixed-point gridder")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -132,6 +132,7 @@ typedef struct svdi_engine svdi_engine;
 #define SVDI_GRIDDER_FP32 0      /* tile-local FP32 gridder (CUDA cores, shared memory)         */
 #define SVDI_GRIDDER_TC 1        /* split-precision tcgen05 tensor-core gridder, FP16 hi + lo   */
 #define SVDI_GRIDDER_TC_BF16 2   /* the same with BF16 hi + lo operands (16-bit significand)    */
+#define SVDI_GRIDDER_TC_I8 3     /* exact integer tcgen05 gridder: 3-byte digits, int32 sums    */
 
 typedef struct svdi_options {
     int device;                  /* CUDA device ordinal                                        */

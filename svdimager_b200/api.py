@@ -26,7 +26,7 @@ KRULE_BUCKET, KRULE_MIN, KRULE_TARGET, KRULE_FIXED = 0, 1, 2, 3
 EDGE_CLIP, EDGE_STRICT = 0, 1
 COORD_FP64, COORD_REF32 = 0, 1
 REPROJ_SII, REPROJ_FIPK = 0, 1
-GRIDDER_FP32, GRIDDER_TC, GRIDDER_TC_BF16 = 0, 1, 2
+GRIDDER_FP32, GRIDDER_TC, GRIDDER_TC_BF16, GRIDDER_TC_I8 = 0, 1, 2, 3
 
 # every function the C header declares (the ABI test checks they are all exported)
 EXPORTED_SYMBOLS = (

@@ -28,7 +28,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
            "--expt-relaxed-constexpr", "-I", INCLUDE] + ARCH
-CU_SOURCES = ["preprocess.cu", "binning.cu", "gridder.cu", "gridder_tc.cu", "image.cu", "engine.cu", "server.cu",
+CU_SOURCES = ["preprocess.cu", "binning.cu", "gridder.cu", "gridder_tc.cu", "gridder_i8.cu", "image.cu", "engine.cu", "server.cu",
               "noalloc.cu", "accuracy.cu", "sii_entry.cpp"]
 CLI_SOURCES = {"sharedlibrary_gpu": ["fits.cpp", "cli_sharedlibrary_gpu.cpp"],
                "svd_integrated_imager_gpu": ["fits.cpp", "bundle.cpp", "cli_svd_integrated_imager_gpu.cpp"]}

@@ -420,6 +420,27 @@ int ensure_corr(svdi_engine* e, long long N, long long G, int W, double beta) {
     return SVDI_OK;
 }
 
+bool is_tc_gridder(int gridder) {
+    return gridder == SVDI_GRIDDER_TC || gridder == SVDI_GRIDDER_TC_BF16 || gridder == SVDI_GRIDDER_TC_I8;
+}
+
+// Tile geometry of the tensor-core gridders (the grid size g.G set): 56 x 8 tiles for the FP16 /
+// BF16 form, 24 x 8 for the integer form.
+void tc_tiles(int gridder, GridGeom& g) {
+    if (gridder == SVDI_GRIDDER_TC_I8) {
+        g.T = kI8TileRows;
+        g.T2 = kI8TileCols;
+        g.ntile = (int)((g.G + g.T - 1) / g.T);
+        g.ntile2 = (int)((g.G + g.T2 - 1) / g.T2);
+    } else {
+        g.T = kTcTileRows;
+        g.T2 = kTcTileCols;
+        g.ntile = (int)((g.G + g.T - 1) / g.T);
+        g.ntile2 = (int)((g.G + g.T2 - 1) / g.T2);
+        g.ntile2 = (g.ntile2 + kTcBlocks - 1) / kTcBlocks * kTcBlocks;
+    }
+}
+
 long long grid_size(long long N, double sigma) {
     if (sigma == 1.5) return (3 * N + 1) / 2;  // ceil(1.5 N), SVDIntegratedImager.cu:1510
     return next_nice_even((long long)std::ceil(sigma * (double)N - 1e-9));
@@ -567,15 +588,14 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     g.gmin = -(g.G / 2);
     g.gmax = (g.G - 1) / 2;
     g.W = o.support;
-    // the tensor-core gridder accumulates one moment plane per CTA in TMEM (K == 1) and bins
-    // into 56 x 8 tiles, four of which share a 64-row accumulator (gridder_tc.cu)
-    const bool use_tc = (o.gridder == SVDI_GRIDDER_TC || o.gridder == SVDI_GRIDDER_TC_BF16) && sp.K == 1 && g.W <= 8;
+    // the tensor-core gridders accumulate one moment plane in TMEM (K == 1): the FP16 / BF16 form
+    // bins into 56 x 8 tiles (64 x 16 accumulator window, gridder_tc.cu), the integer form into
+    // 24 x 8 tiles (32 x 16 window, gridder_i8.cu); the integer form scales each key by its own
+    // max |value| from the scatter
+    const bool use_tc = is_tc_gridder(o.gridder) && sp.K == 1 && g.W <= 8;
+    const bool use_i8 = use_tc && o.gridder == SVDI_GRIDDER_TC_I8;
     if (use_tc) {
-        g.T = kTcTileRows;
-        g.ntile = (int)((g.G + g.T - 1) / g.T);
-        g.T2 = kTcTileCols;
-        g.ntile2 = (int)((g.G + g.T2 - 1) / g.T2);
-        g.ntile2 = (g.ntile2 + kTcBlocks - 1) / kTcBlocks * kTcBlocks;
+        tc_tiles(o.gridder, g);
     } else {
         g.T = o.tile ? o.tile : (sp.K == 1 ? 64 : 32);
         g.ntile = (int)((g.G + g.T - 1) / g.T);
@@ -617,8 +637,11 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
                               e->dropped.as<unsigned long long>(), st, dplan));
     if (use_tc) {
         SVDI_TRY(e->kb_offsets.ensure((size_t)(n_keys + 1) * 4));
-    } else {  // the FP32 gridder's chunk table and per-key maxima
+    } else {  // the FP32 gridder's chunk table
         SVDI_TRY(e->chunk_key.ensure(((size_t)std::max<long long>(n, 1) / kGridChunk + 2) * 4));
+    }
+    const bool need_keymax = !use_tc || use_i8;  // per-key max |value| (FP32 and integer gridders)
+    if (need_keymax) {
         SVDI_TRY(e->keymax.ensure((size_t)n_keys * 4));
         SVDI_CUDA(cudaMemsetAsync(e->keymax.p, 0, (size_t)n_keys * 4, st));
     }
@@ -635,7 +658,7 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     SVDI_TRY(launch_scatter(src, g, sp, e->cursor.as<unsigned int>(), n_keys, e->rec.as<SampleRec>(),
                             need_s ? e->rec_s.as<float>() : nullptr,
                             use_tc ? e->tc_status.as<unsigned int>() + 1 : nullptr, st,
-                            use_tc ? nullptr : e->keymax.as<unsigned int>(), dplan));
+                            need_keymax ? e->keymax.as<unsigned int>() : nullptr, dplan));
     if (timed) SVDI_CUDA(cudaEventRecord(e->ev[2], st));
 
     // slab batches: grid -> FFT -> recombine
@@ -671,7 +694,12 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
         if (timed) SVDI_CUDA(cudaEventRecord(e->ev[3], st));
         SVDI_CUDA(cudaMemsetAsync(e->planes.p, 0, plane_bytes * planes_per_batch, st));
         const int tiles2 = g.ntile * g.ntile2;
-        if (use_tc) {
+        if (use_i8) {
+            SVDI_TRY(launch_grid_i8(e->rec.as<SampleRec>(), e->offsets.as<unsigned int>(),
+                                    e->kb_offsets.as<unsigned int>(), n_keys, s0 * tiles2, s1 * tiles2, s0, g,
+                                    e->poly, e->planes.as<float2>(), e->keymax.as<unsigned int>(),
+                                    e->tc_status.as<unsigned int>(), e->sm_count, st));
+        } else if (use_tc) {
             SVDI_TRY(launch_grid_tc(e->rec.as<SampleRec>(), e->offsets.as<unsigned int>(),
                                     e->kb_offsets.as<unsigned int>(), n_keys, s0 * tiles2,
                                     s1 * tiles2, s0, g, e->poly, e->planes.as<float2>(),
@@ -857,7 +885,7 @@ int check_options(const svdi_options& o) {
         set_error("tile must be 0, 32 or 64");
         return SVDI_ERR_UNSUPPORTED;
     }
-    if (o.gridder != SVDI_GRIDDER_FP32 && o.gridder != SVDI_GRIDDER_TC && o.gridder != SVDI_GRIDDER_TC_BF16) {
+    if (o.gridder != SVDI_GRIDDER_FP32 && !is_tc_gridder(o.gridder)) {
         set_error("unknown gridder");
         return SVDI_ERR_INVALID_ARGUMENT;
     }
@@ -1361,11 +1389,7 @@ GridGeom geom_for(const svdi_options& o, long long N, float cell_f, int K, bool 
     g.gmax = (g.G - 1) / 2;
     g.W = o.support;
     if (use_tc) {
-        g.T = kTcTileRows;
-        g.ntile = (int)((g.G + g.T - 1) / g.T);
-        g.T2 = kTcTileCols;
-        g.ntile2 = (int)((g.G + g.T2 - 1) / g.T2);
-        g.ntile2 = (g.ntile2 + kTcBlocks - 1) / kTcBlocks * kTcBlocks;
+        tc_tiles(o.gridder, g);
     } else {
         g.T = o.tile ? o.tile : (K == 1 ? 64 : 32);
         g.ntile = (int)((g.G + g.T - 1) / g.T);
@@ -1396,7 +1420,7 @@ int wide_capture(svdi_batch* b) {
     const float cell_f = b->cell;
     for (const auto& p : b->plans)
         if ((int)p.bslabs < p.sp.nslab) return SVDI_ERR_UNSUPPORTED;
-    const bool tc_opt = o.gridder == SVDI_GRIDDER_TC || o.gridder == SVDI_GRIDDER_TC_BF16;
+    const bool tc_opt = is_tc_gridder(o.gridder);
     // groups of equal Chebyshev order, in order of first appearance
     std::vector<int> group_k;
     std::vector<int> group_of(B);
@@ -1585,7 +1609,13 @@ int wide_capture(svdi_batch* b) {
             sg.nslab = (int)((G.key_hi - G.key_lo) / ((long long)G.g.ntile * G.g.ntile2));
             float2* pl = b->planes.as<float2>() + G.plane_lo * GG;
             unsigned int* stw = b->status.as<unsigned int>() + 4 * gi;
-            if (G.tc) {
+            if (G.tc && o.gridder == SVDI_GRIDDER_TC_I8) {
+                // status in [0], work counter in [2]; per-key scales from the scatter's maxima
+                SVDI_TRY(launch_grid_i8(b->rec.as<SampleRec>(), b->offsets.as<unsigned int>(),
+                                        b->kb_offsets.as<unsigned int>(), (int)nkeys, (int)G.key_lo, (int)G.key_hi,
+                                        (int)G.slab_lo, G.g, e->poly, pl, b->keymax.as<unsigned int>(), stw,
+                                        e->sm_count, st));
+            } else if (G.tc) {
                 // the TC gridder keeps its status in [0], reads max |v| from the pointer and counts work in [2]
                 SVDI_TRY(launch_grid_tc(b->rec.as<SampleRec>(), b->offsets.as<unsigned int>(),
                                         b->kb_offsets.as<unsigned int>(), (int)nkeys, (int)G.key_lo, (int)G.key_hi,

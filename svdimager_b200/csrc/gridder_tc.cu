@@ -73,6 +73,7 @@
 // MMA warp waits (bounded) for its last commit, the scheduler for its last record copies, the
 // tensor memory is freed and the host reports the grid as incomplete.
 #include "svdi_internal.cuh"
+#include "tc_sync.cuh"
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -133,110 +134,7 @@ constexpr uint32_t kIdesc = (1u << 4) | (1u << 15) | (1u << 16) | ((uint32_t)(kN
 // The same with BF16 A and B (both operands always have the same type).
 constexpr uint32_t kIdescBf16 = kIdesc | (1u << 7) | (1u << 10);
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok)
-        : "r"(addr), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(addr), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint32_t addr) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(addr) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t addr, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(addr), "r"(bytes) : "memory");
-}
-// Bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from this GPU's global
-// memory into this CTA's shared memory, completing on the mbarrier at `mbar` (no multicast).
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                 "l"(src), "r"(bytes), "r"(mbar)
-                 : "memory");
-}
-
-__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
-    unsigned int v;
-    asm volatile("ld.acquire.cta.shared::cta.u32 %0, [%1];" : "=r"(v) : "r"(smem_u32(p)) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release(unsigned int* p, unsigned int v) {
-    asm volatile("st.release.cta.shared::cta.u32 [%0], %1;" ::"r"(smem_u32(p)), "r"(v) : "memory");
-}
-
-// Bounded waits (about one second of global time) that also give up when another thread of the
-// CTA has given up (*abort != 0). They return false on either.
-__device__ bool mbar_wait(uint32_t addr, uint32_t parity, const volatile int* abort) {
-    if (mbar_try(addr, parity)) return true;
-    const unsigned long long t0 = global_ns();
-    for (unsigned int it = 1; it < (1u << 28); ++it) {
-        if (mbar_try(addr, parity)) return true;
-        if ((it & 63u) == 0 && (*abort || global_ns() - t0 > 1000000000ull)) return false;
-    }
-    return false;
-}
-__device__ bool wait_at_least(const unsigned int* p, unsigned int target, const volatile int* abort) {
-    if (ld_acquire(p) >= target) return true;
-    const unsigned long long t0 = global_ns();
-    for (unsigned int it = 1; it < (1u << 28); ++it) {
-        __nanosleep(64);
-        if (ld_acquire(p) >= target) return true;
-        if ((it & 15u) == 0 && (*abort || global_ns() - t0 > 1000000000ull)) return false;
-    }
-    return false;
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-__device__ __forceinline__ void mma_f16(uint32_t d_tmem, unsigned long long a, unsigned long long b, uint32_t accum,
-                                        uint32_t idesc) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
-        :
-        : "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accum)
-        : "memory");
-}
-__device__ __forceinline__ void mma_commit(uint32_t mbar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
-                 : "memory");
-}
-
-// 32 consecutive TMEM columns of this thread's lane.
-// 8 consecutive TMEM columns of this thread's lane (the wait is separate: issue several, then wait).
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-                 : "r"(taddr));
-}
-__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-
-__device__ __forceinline__ void red_add_v2(float2* addr, float a, float b) {
-    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(addr), "f"(a), "f"(b) : "memory");
-}
-
-// Exact ES kernel psi(x) = exp(beta (sqrt(1 - x^2) - 1)) written without cancellation.
-__device__ __forceinline__ float es_exact(float beta, float x) {
-    if (fabsf(x) > 1.0f) return 0.0f;
-    return expf(-beta * x * x / (1.0f + sqrtf((1.0f - x) * (1.0f + x))));
-}
+using namespace tc;
 
 
 // Eight values (taps 0..7) as FP16 (or BF16) hi or lo pairs (x = hi + lo + O(2^-22 x) in FP16,
@@ -308,11 +206,6 @@ __device__ __forceinline__ void st_chunk(unsigned char* p, uint32_t a, uint32_t 
     *reinterpret_cast<uint4*>(p) = make_uint4(a, b, c, d);
 }
 
-struct KBMeta {
-    int key;            // tile key of the K-block
-    unsigned int pos;   // first record
-    int cnt;            // records (1..32)
-};
 
 enum EventType : int { kEvDrain = 0, kEvExit = 1 };
 struct Event {
@@ -432,13 +325,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
             int state = 0;  // 1: produce, 0: done, -1: give up
             unsigned int sdv = 0;
             if (lane == 0) {
-                const unsigned long long t0 = global_ns();
+                PollClock pc;
                 for (unsigned int n = 0;; ++n) {
                     if (pub_seen <= j) pub_seen = (int)ld_acquire(&S.published);
                     if (pub_seen > j) { state = 1; break; }
                     sdv = ld_acquire(&S.sched_done);
                     if (sdv && (unsigned int)j >= sdv - 1) { state = 0; break; }
-                    if ((n & 63u) == 0 && (*abort_flag || global_ns() - t0 > 1000000000ull)) {
+                    if ((n & 63u) == 63u && (*abort_flag || pc.expired())) {
                         state = -1;
                         break;
                     }
@@ -581,133 +474,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
         }
     } else if (warp == kSchedWarp) {
         // ============================ scheduler ============================
-        // The K-blocks of keys [key_lo, key_hi) are handed out in chunks of kChunkKB from a global
-        // counter (dynamic balance: CTAs whose tiles cost more take fewer chunks). K-block m of key k
-        // covers records [offsets[k] + 32 m, min(offsets[k + 1], offsets[k] + 32 (m + 1))). Lanes hold
-        // offsets and kb_offsets of the current 32-key window (x = 32 from the *_e registers); the
-        // next window is loaded one window ahead.
-        int kc = 0, ci = 0;
-        unsigned int m_in_key = 0, remaining = 0;
-        unsigned int off_l = 0, kbo_l = 0, off_e = 0, kbo_e = 0;
-        unsigned int noff_l = 0, nkbo_l = 0, noff_e = 0, nkbo_e = 0;
-        auto fetch = [&](int base, unsigned int& o, unsigned int& kb, unsigned int& oe, unsigned int& kbe_) {
-            const int k = min(base + lane, P.key_hi);
-            o = P.offsets[k];
-            kb = P.kb_offsets[k];
-            const int ke = min(base + 32, P.key_hi);
-            oe = P.offsets[ke];
-            kbe_ = P.kb_offsets[ke];
-        };
-        auto at = [&](unsigned int vl, unsigned int ve, int x) -> unsigned int {  // warp-uniform x in [0, 32]
-            const unsigned int v = __shfl_sync(0xffffffffu, vl, x & 31);
-            return x == 32 ? ve : v;
-        };
-        unsigned int published = 0;
-        // current key: records [ka, kend), K-blocks m_in_key .. nkb - 1
-        unsigned int ka = 0, kend = 0, nkb = 0;
-        bool have_key = false;
-        auto schedule_to = [&](unsigned int target) {  // publish K-blocks up to index target - 1
-            const unsigned int before = published;
-            while (remaining && published < target) {
-                if (!have_key || m_in_key >= nkb) {  // advance to the next key with K-blocks left
-                    if (have_key) {
-                        ++ci;
-                        m_in_key = 0;
-                    }
-                    for (;;) {
-                        if (kc + ci >= P.key_hi) {  // inconsistent K-block counts: stop scheduling
-                            remaining = 0;
-                            break;
-                        }
-                        if (ci == 32) {
-                            kc += 32;
-                            ci = 0;
-                            off_l = noff_l; kbo_l = nkbo_l; off_e = noff_e; kbo_e = nkbo_e;
-                            fetch(kc + 32, noff_l, nkbo_l, noff_e, nkbo_e);
-                        }
-                        nkb = at(kbo_l, kbo_e, ci + 1) - at(kbo_l, kbo_e, ci);
-                        if (m_in_key < nkb) break;
-                        ++ci;
-                        m_in_key = 0;
-                    }
-                    if (!remaining) break;
-                    ka = at(off_l, off_e, ci);
-                    kend = at(off_l, off_e, ci + 1);
-                    have_key = true;
-                }
-                // the K-blocks of this key, up to the target (no shuffles)
-                const int key = kc + ci;
-                while (remaining && published < target && m_in_key < nkb) {
-                    const unsigned int pos = ka + (unsigned int)kKB * m_in_key;
-                    const unsigned int cnt = min((unsigned int)kKB, kend - pos);
-                    if (lane == 0) {
-                        S.meta[published % kMetaRing] = KBMeta{key, pos, (int)cnt};
-                        // stage the K-block's records: one contiguous run of 16-byte records
-                        const uint32_t bar = smem_u32(&S.rec_full[published % kRecSlots]);
-                        mbar_arrive_expect_tx(bar, cnt * 16u);
-                        bulk_g2s(smem_u32(smem + kRecOff + (published % kRecSlots) * kKB * 16), P.rec + pos,
-                                 cnt * 16u, bar);
-                    }
-                    ++published;
-                    ++m_in_key;
-                    --remaining;
-                }
-            }
-            if (published != before) {
-                __syncwarp();
-                if (lane == 0) st_release(&S.published, published);
-            }
-        };
-        bool ok = true;
-        for (;;) {
-            // next chunk of K-blocks
-            unsigned int c = 0;
-            if (lane == 0) c = atomicAdd(P.work, 1u);
-            c = __shfl_sync(0xffffffffu, c, 0);
-            const unsigned long long kb0l = (unsigned long long)kb_lo + (unsigned long long)c * kChunkKB;
-            if (kb0l >= kb_hi) break;
-            const unsigned int kb0 = (unsigned int)kb0l, kb1 = min(kb_hi, kb0 + (unsigned int)kChunkKB);
-            // its first key: the last key with kb_offsets[key] <= kb0 (32 probes per round)
-            int lo = P.key_lo, hi = P.key_hi;
-            while (hi - lo > 1) {
-                const int step = (hi - lo + 31) / 32;
-                const int probe = lo + lane * step;
-                const bool le = probe < hi && P.kb_offsets[probe] <= kb0;
-                const unsigned int bal = __ballot_sync(0xffffffffu, le);
-                const int lmax = 31 - __clz(bal);  // lane 0 always qualifies (kb_offsets[lo] <= kb0)
-                const int nlo = lo + lmax * step;
-                hi = min(hi, nlo + step);
-                lo = nlo;
-            }
-            kc = lo;
-            ci = 0;
-            m_in_key = kb0 - P.kb_offsets[lo];
-            remaining = kb1 - kb0;
-            have_key = false;
-            fetch(kc, off_l, kbo_l, off_e, kbo_e);
-            fetch(kc + 32, noff_l, nkbo_l, noff_e, nkbo_e);
-            while (remaining) {  // keep the record slots full: up to kRecSlots K-blocks ahead of consumption
-                int cons = 0;
-                if (lane == 0) cons = (int)ld_acquire(&S.consumed);
-                cons = __shfl_sync(0xffffffffu, cons, 0);
-                schedule_to((unsigned int)cons + kRecSlots);
-                if (!remaining) break;
-                if (lane == 0) ok = wait_at_least(&S.consumed, (unsigned int)cons + 1, abort_flag);
-                ok = __shfl_sync(0xffffffffu, (int)ok, 0);
-                if (!ok) break;  // the waiting role reports the failure
-            }
-            if (!ok) break;
-        }
-        if (ok && lane == 0) st_release(&S.sched_done, published + 1);
-        // no record copy of this CTA may still be in flight when it exits: wait for the last copy of
-        // every slot (the producers normally consumed them all already)
-        if (lane == 0) {
-            const volatile int never = 0;
-            for (unsigned int s = 0; s < (unsigned int)kRecSlots && s < published; ++s) {
-                const unsigned int uses = (published - s + kRecSlots - 1) / kRecSlots;
-                if (!mbar_wait(smem_u32(&S.rec_full[s]), (uint32_t)((uses - 1) & 1u), &never)) atomicOr(P.status, 16u);
-            }
-        }
+        schedule_kblocks<kKB, kMetaRing, kRecSlots, kChunkKB>(S, P, smem + kRecOff, kb_lo, kb_hi, nullptr, abort_flag, lane);
     } else if (warp == kMmaWarp) {
         // ============================ MMA issuer ============================
         // Consecutive K-blocks of one key form an interval (at most kIntervalKB K-blocks) that
@@ -727,14 +494,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
         unsigned int ev_free_seen = 0;  // events consumed by every epilogue warp, last read
         auto push_event = [&](Event ev) {  // lane 0
             if (failed) return;
-            const unsigned long long t0 = global_ns();
+            PollClock pc;
             for (unsigned int n = 0;; ++n) {
                 if (ev_n - ev_free_seen < (unsigned int)kEventRing) break;
                 unsigned int mn = 0xFFFFFFFFu;
                 for (int q = 0; q < 4; ++q) mn = min(mn, ld_acquire(&S.ev_consumed[q]));
                 ev_free_seen = mn;
                 if (ev_n - mn < (unsigned int)kEventRing) break;
-                if ((n & 63u) == 0 && (*abort_flag || global_ns() - t0 > 1000000000ull)) {
+                if ((n & 63u) == 63u && (*abort_flag || pc.expired())) {
                     failed = true;
                     return;
                 }
@@ -758,14 +525,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
             // wait until K-block i is published or the schedule ends before it
             int state = 0;
             if (lane == 0) {
-                const unsigned long long t0 = global_ns();
+                PollClock pc;
                 for (unsigned int n = 0;; ++n) {
                     if (pub_seen > i) { state = 1; break; }
                     pub_seen = ld_acquire(&S.published);
                     if (pub_seen > i) { state = 1; break; }
                     const unsigned int sd = ld_acquire(&S.sched_done);
                     if (sd && i >= sd - 1) { state = 0; break; }
-                    if ((n & 63u) == 0 && (*abort_flag || global_ns() - t0 > 1000000000ull)) {
+                    if ((n & 63u) == 63u && (*abort_flag || pc.expired())) {
                         state = -1;
                         break;
                     }
