@@ -122,6 +122,13 @@ long long next_nice_even(long long n) {
     }
 }
 
+// The two cuFFT plans of a pruned inverse 2-D FFT (get_plan).
+struct FftPlan {
+    cufftHandle rows = 0, cols = 0;  // cols == 0: `rows` is one 2-D plan of the whole grid
+    long long G = 0, N = 0;
+    int batch = 0;
+};
+
 }  // namespace
 
 }  // namespace svdi
@@ -170,7 +177,7 @@ struct svdi_engine {
     bool pending_total = false;             // ev[0] -> ev[7] spans the whole call
     bool pending_need_s = false;
     long long pending_n = 0;
-    std::map<std::pair<long long, int>, cufftHandle> plans;
+    std::map<std::tuple<long long, long long, int>, svdi::FftPlan> plans;
     std::map<std::tuple<long long, long long, int, double>, std::vector<float>> corr_cache;
     std::tuple<long long, long long, int, double> corr_key{-1, -1, -1, 0.0};
     std::map<std::tuple<double, int, int>, std::vector<double>> cheb_cache;
@@ -191,7 +198,10 @@ struct svdi_engine {
 
     ~svdi_engine() {
         if (device >= 0) cudaSetDevice(device);
-        for (auto& kv : plans) cufftDestroy(kv.second);
+        for (auto& kv : plans) {
+            cufftDestroy(kv.second.rows);
+            if (kv.second.cols) cufftDestroy(kv.second.cols);
+        }
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         if (h_stats) cudaFreeHost(h_stats);
@@ -362,18 +372,49 @@ int choose_slabs(svdi_engine* e, bool archive, double r3min, double r3max, doubl
     return SVDI_OK;
 }
 
-int get_plan(svdi_engine* e, long long G, int batch, cufftHandle& plan) {
-    auto key = std::make_pair(G, batch);
+// The inverse 2-D FFT of `batch` moment planes of G x G, pruned to what the recombination reads:
+// every row (length G, contiguous) is transformed, then only the N columns it reads (the checkerboard
+// sign centres the transform, so pixel x reads column G / 2 + x - N / 2: one contiguous run) are
+// transformed along the rows' stride. The second pass does N / G of the full 2-D transform's work
+// there; the other columns keep their first-pass values and are never read. Grid sizes with a prime
+// factor above 7 (cuFFT's Bluestein path, which gave wrong in-place results for the interleaved
+// column batches on B200) keep one 2-D plan.
+int get_plan(svdi_engine* e, long long G, long long N, int batch, FftPlan& plan) {
+    auto key = std::make_tuple(G, N, batch);
     auto it = e->plans.find(key);
     if (it != e->plans.end()) {
         plan = it->second;
         return SVDI_OK;
     }
-    int dims[2] = {(int)G, (int)G};
-    SVDI_CUFFT(cufftPlanMany(&plan, 2, dims, nullptr, 1, (int)(G * G), nullptr, 1, (int)(G * G), CUFFT_C2C,
-                             batch));
-    SVDI_CUFFT(cufftSetStream(plan, e->stream));
+    long long r = G;
+    for (long long f : {2, 3, 5, 7})
+        while (r % f == 0) r /= f;
+    int n = (int)G;
+    if (r == 1) {
+        SVDI_CUFFT(cufftPlanMany(&plan.rows, 1, &n, &n, 1, n, &n, 1, n, CUFFT_C2C, (int)(G * batch)));
+        SVDI_CUFFT(cufftPlanMany(&plan.cols, 1, &n, &n, n, 1, &n, n, 1, CUFFT_C2C, (int)N));
+        SVDI_CUFFT(cufftSetStream(plan.cols, e->stream));
+    } else {
+        int dims[2] = {n, n};
+        SVDI_CUFFT(cufftPlanMany(&plan.rows, 2, dims, nullptr, 1, n * n, nullptr, 1, n * n, CUFFT_C2C, batch));
+        plan.cols = 0;
+    }
+    SVDI_CUFFT(cufftSetStream(plan.rows, e->stream));
+    plan.G = G;
+    plan.N = N;
+    plan.batch = batch;
     e->plans[key] = plan;
+    return SVDI_OK;
+}
+
+int exec_fft(const FftPlan& plan, cufftComplex* planes, int nplanes) {
+    SVDI_CUFFT(cufftExecC2C(plan.rows, planes, planes, CUFFT_INVERSE));
+    if (plan.cols == 0) return SVDI_OK;
+    const long long c0 = plan.G / 2 - plan.N / 2;
+    for (int p = 0; p < nplanes; ++p) {
+        cufftComplex* col0 = planes + (long long)p * plan.G * plan.G + c0;
+        SVDI_CUFFT(cufftExecC2C(plan.cols, col0, col0, CUFFT_INVERSE));
+    }
     return SVDI_OK;
 }
 
@@ -676,8 +717,8 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     const int planes_per_batch = (int)bslabs * sp.K;
     const size_t plane_bytes = (size_t)g.G * g.G * sizeof(float2);
     SVDI_TRY(e->planes.ensure(plane_bytes * planes_per_batch));
-    cufftHandle plan;
-    SVDI_TRY(get_plan(e, g.G, planes_per_batch, plan));
+    FftPlan plan;
+    SVDI_TRY(get_plan(e, g.G, N, planes_per_batch, plan));
     SVDI_TRY(ensure_corr(e, N, g.G, g.W, o.beta));
     SVDI_CUDA(cudaMemsetAsync(d_out, 0, (size_t)N * N * sizeof(float), st));
     // slabs split over several batches: the signed sums of all batches before |.| (the reference
@@ -720,7 +761,7 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
             e->sz_grid = plane_bytes * (size_t)(std::min(sp.nslab, (int)bslabs) * sp.K);
         }
         if (timed) SVDI_CUDA(cudaEventRecord(e->ev[4], st));
-        SVDI_CUFFT(cufftExecC2C(plan, e->planes.as<cufftComplex>(), e->planes.as<cufftComplex>(), CUFFT_INVERSE));
+        SVDI_TRY(exec_fft(plan, e->planes.as<cufftComplex>(), planes_per_batch));
         if (timed) SVDI_CUDA(cudaEventRecord(e->ev[5], st));
         // recombine the slabs of this batch (moment plane index relative to the batch)
         bp.nslab = s1 - s0;
