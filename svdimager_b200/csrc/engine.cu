@@ -129,6 +129,12 @@ struct FftPlan {
     int batch = 0;
 };
 
+void destroy_fft_plan(FftPlan& plan) {
+    if (plan.rows) cufftDestroy(plan.rows);
+    if (plan.cols) cufftDestroy(plan.cols);
+    plan.rows = plan.cols = 0;
+}
+
 }  // namespace
 
 }  // namespace svdi
@@ -198,10 +204,7 @@ struct svdi_engine {
 
     ~svdi_engine() {
         if (device >= 0) cudaSetDevice(device);
-        for (auto& kv : plans) {
-            cufftDestroy(kv.second.rows);
-            if (kv.second.cols) cufftDestroy(kv.second.cols);
-        }
+        for (auto& kv : plans) svdi::destroy_fft_plan(kv.second);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         if (h_stats) cudaFreeHost(h_stats);
@@ -379,13 +382,7 @@ int choose_slabs(svdi_engine* e, bool archive, double r3min, double r3max, doubl
 // there; the other columns keep their first-pass values and are never read. Grid sizes with a prime
 // factor above 7 (cuFFT's Bluestein path, which gave wrong in-place results for the interleaved
 // column batches on B200) keep one 2-D plan.
-int get_plan(svdi_engine* e, long long G, long long N, int batch, FftPlan& plan) {
-    auto key = std::make_tuple(G, N, batch);
-    auto it = e->plans.find(key);
-    if (it != e->plans.end()) {
-        plan = it->second;
-        return SVDI_OK;
-    }
+int make_fft_plan(long long G, long long N, int batch, cudaStream_t st, FftPlan& plan) {
     long long r = G;
     for (long long f : {2, 3, 5, 7})
         while (r % f == 0) r /= f;
@@ -393,16 +390,27 @@ int get_plan(svdi_engine* e, long long G, long long N, int batch, FftPlan& plan)
     if (r == 1) {
         SVDI_CUFFT(cufftPlanMany(&plan.rows, 1, &n, &n, 1, n, &n, 1, n, CUFFT_C2C, (int)(G * batch)));
         SVDI_CUFFT(cufftPlanMany(&plan.cols, 1, &n, &n, n, 1, &n, n, 1, CUFFT_C2C, (int)N));
-        SVDI_CUFFT(cufftSetStream(plan.cols, e->stream));
     } else {
         int dims[2] = {n, n};
         SVDI_CUFFT(cufftPlanMany(&plan.rows, 2, dims, nullptr, 1, n * n, nullptr, 1, n * n, CUFFT_C2C, batch));
         plan.cols = 0;
     }
-    SVDI_CUFFT(cufftSetStream(plan.rows, e->stream));
+    SVDI_CUFFT(cufftSetStream(plan.rows, st));
+    if (plan.cols) SVDI_CUFFT(cufftSetStream(plan.cols, st));
     plan.G = G;
     plan.N = N;
     plan.batch = batch;
+    return SVDI_OK;
+}
+
+int get_plan(svdi_engine* e, long long G, long long N, int batch, FftPlan& plan) {
+    auto key = std::make_tuple(G, N, batch);
+    auto it = e->plans.find(key);
+    if (it != e->plans.end()) {
+        plan = it->second;
+        return SVDI_OK;
+    }
+    SVDI_TRY(make_fft_plan(G, N, batch, e->stream, plan));
     e->plans[key] = plan;
     return SVDI_OK;
 }
@@ -1402,8 +1410,7 @@ struct svdi_batch {
     bool wide = false;
     svdi::DevBuf vr, vi, q, s, vin64, vin32, stats, partial, counts, offsets, cursor, keymax, chunk_key,
         kb_offsets, rec, rec_s, planes, dropped, work, corr;
-    cufftHandle fft = 0;
-    bool have_fft = false;
+    svdi::FftPlan fft;
     std::vector<cudaStream_t> lanes;
     std::vector<cudaEvent_t> lane_ev;
     cudaEvent_t ev_fork = nullptr;
@@ -1411,7 +1418,7 @@ struct svdi_batch {
         if (e) cudaSetDevice(e->device);
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
-        if (have_fft) cufftDestroy(fft);
+        svdi::destroy_fft_plan(fft);
         for (auto ev : lane_ev) cudaEventDestroy(ev);
         for (auto st : lanes) cudaStreamDestroy(st);
         if (ev_fork) cudaEventDestroy(ev_fork);
@@ -1553,10 +1560,7 @@ int wide_capture(svdi_batch* b) {
         e->poly_W = o.support;
         e->poly_beta = o.beta;
     }
-    int dims[2] = {(int)Gs, (int)Gs};
-    SVDI_CUFFT(cufftPlanMany(&b->fft, 2, dims, nullptr, 1, (int)GG, nullptr, 1, (int)GG, CUFFT_C2C, (int)nplanes));
-    b->have_fft = true;
-    SVDI_CUFFT(cufftSetStream(b->fft, e->stream));
+    SVDI_TRY(make_fft_plan(Gs, N, (int)nplanes, e->stream, b->fft));
     int prio_low = 0, prio_high = 0;
     SVDI_CUDA(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
     for (int l = 0; l < L; ++l) {
@@ -1670,7 +1674,7 @@ int wide_capture(svdi_batch* b) {
                                           e->sm_count, st));
             }
         }
-        SVDI_CUFFT(cufftExecC2C(b->fft, b->planes.as<cufftComplex>(), b->planes.as<cufftComplex>(), CUFFT_INVERSE));
+        SVDI_TRY(exec_fft(b->fft, b->planes.as<cufftComplex>(), (int)nplanes));
         for (size_t s = 0; s < B; ++s) {
             const Group& G = groups[group_of[s]];
             SVDI_TRY(launch_recombine(b->planes.as<float2>() + plane_base[s] * GG, G.g, N, (double)cell_f,
