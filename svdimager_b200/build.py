@@ -30,6 +30,9 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler"
            "--expt-relaxed-constexpr", "-I", INCLUDE] + ARCH
 CU_SOURCES = ["preprocess.cu", "binning.cu", "gridder.cu", "gridder_tc.cu", "gridder_i8.cu", "image.cu", "engine.cu", "server.cu",
               "noalloc.cu", "accuracy.cu", "sii_entry.cpp"]
+# diagnostics built beside the CLIs: tcgen05 MMA issue rates and operand-layout check, shared-memory
+# reduction rates (the measurements behind the gridders' design)
+PROBE_SOURCES = {"probe_tcgen05_mma": "probe_tcgen05_mma.cu", "probe_shared_red": "probe_shared_red.cu"}
 CLI_SOURCES = {"sharedlibrary_gpu": ["fits.cpp", "cli_sharedlibrary_gpu.cpp"],
                "svd_integrated_imager_gpu": ["fits.cpp", "bundle.cpp", "cli_svd_integrated_imager_gpu.cpp"]}
 
@@ -79,6 +82,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
             _run(["g++", "-O2", "-std=c++17", "-I", INCLUDE, "-o", out] + paths +
                  ["-L", LIB_DIR, "-lsvdimager_b200", "-Wl,-rpath,$ORIGIN/../lib",
                   "-L/usr/local/cuda/lib64", "-lcudart"])
+    for name, src in PROBE_SOURCES.items():
+        path = os.path.join(CSRC, src)
+        out = os.path.join(BIN_DIR, name)
+        if os.path.exists(path) and (force or _stale(out, [path])):
+            _run([NVCC, "-O3", "-std=c++17", "-lineinfo"] + ARCH + ["-o", out, path])
     return LIB
 
 
