@@ -526,11 +526,10 @@ def run_ours(args):
     achieved = alg / (stage_ms[dom] * 1e-3) / 1e9
     # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of each gridder on
     # this workload, from the one-launch --set full captures summarised in
-    # profiles/k_grid_fp32_precision.md and profiles/k_grid_tc_precision.md
+    # profiles/k_grid_{fp32,tc,i8}_precision.md
     traffic = None
     if dom == "ms_grid" and args.config == "precision":
-        traffic = {"k_grid_fp32": 223432960, "k_grid_tc": 224904960}.get(
-            "k_grid_tc" if st["used_tc"] else "k_grid_fp32")
+        traffic = {"k_grid_fp32": 223432960, "k_grid_tc": 225017856, "k_grid_i8": 224765696}.get(name.split()[0])
 
     cpu = cpu_baseline(snap, eng, api, st, args) if not args.no_cpu else None
     line = {
