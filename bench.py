@@ -525,8 +525,8 @@ def run_ours(args):
         name = "k_recombine"
     achieved = alg / (stage_ms[dom] * 1e-3) / 1e9
     # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of each gridder on
-    # this workload, from the one-launch --set full captures summarised in
-    # profiles/k_grid_{fp32,tc,i8}_precision.md
+    # this workload, from one-launch ncu --set full captures (fourth imaging call of this bench with
+    # --lanes 1 --steps 2 --warmup 3)
     traffic = None
     if dom == "ms_grid" and args.config == "precision":
         traffic = {"k_grid_fp32": 223432960, "k_grid_tc": 225017856, "k_grid_i8": 224765696}.get(name.split()[0])
