@@ -113,8 +113,11 @@ def test_wide_batch_with_mixed_chebyshev_orders(cuda_device, stream5):
     e.close()
 
 
-def test_batch_tensor_core_gridder(cuda_device, stream5):
-    keep, descs, imgs, b, e, out1 = _batch_vs_single(stream5, gridder=api.GRIDDER_TC, k_rule=api.KRULE_FIXED,
+@pytest.mark.parametrize("gridder", [api.GRIDDER_TC, api.GRIDDER_TC_I8])
+def test_batch_tensor_core_gridder(cuda_device, stream5, gridder):
+    """Wide batch on a tensor-core gridder (split FP16 and exact integer): one gridder launch over
+    the tile keys of all snapshots; every image equals the engine's."""
+    keep, descs, imgs, b, e, out1 = _batch_vs_single(stream5, gridder=gridder, k_rule=api.KRULE_FIXED,
                                                      fixed_k=1)
     assert b.wide
     b.close()
