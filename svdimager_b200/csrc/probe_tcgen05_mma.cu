@@ -97,10 +97,14 @@ __device__ __forceinline__ void issue_kblock(const Shape& c, uint32_t d, unsigne
 // `issuers` warps (lane 0 each) issue n_kb / issuers K-blocks into their own accumulators (columns
 // w * N). Slots are filled from src (src_bytes, wrapped). Block 0 optionally reads the first
 // accumulator back (M = 128 only).
+// commit_every > 0: the issuer also commits its MMAs to a second mbarrier after every commit_every
+// K-blocks (as a pipeline frees a stage), without waiting on it.
 __global__ void __launch_bounds__(128) k_probe(Shape c, int n_kb, int issuers, const unsigned char* __restrict__ src,
-                                               int src_bytes, unsigned long long* cyc, int* status, int* out) {
+                                               int src_bytes, unsigned long long* cyc, int* status, int* out,
+                                               int commit_every) {
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ __align__(8) unsigned long long bar[4];
+    __shared__ __align__(8) unsigned long long stage_bar[4];
     __shared__ uint32_t tbase;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int slot_bytes = (c.a_bytes + c.b_bytes + 1023) & ~1023;
@@ -111,7 +115,10 @@ __global__ void __launch_bounds__(128) k_probe(Shape c, int n_kb, int issuers, c
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        for (int w = 0; w < 4; ++w) asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar[w])), "r"(1) : "memory");
+        for (int w = 0; w < 4; ++w) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar[w])), "r"(1) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&stage_bar[w])), "r"(1) : "memory");
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -131,10 +138,16 @@ __global__ void __launch_bounds__(128) k_probe(Shape c, int n_kb, int issuers, c
         const uint32_t d = tmem + (uint32_t)(warp * c.N);
         const int mine = n_kb / issuers;
         const unsigned long long t0 = clock64();
+        int until_commit = commit_every;  // K-blocks left before the next commit (a countdown: no division)
         for (int i = 0; i < mine; i += 8) {
 #pragma unroll
-            for (int s = 0; s < 8; ++s)
+            for (int s = 0; s < 8; ++s) {
                 if (i + s < mine) issue_kblock(c, d, ad[s], bd[s], (i + s) > 0 ? 1u : 0u);
+                if (commit_every > 0 && --until_commit == 0) {
+                    commit(smem_u32(&stage_bar[warp]));
+                    until_commit = commit_every;
+                }
+            }
         }
         const unsigned long long t1 = clock64();
         commit(smem_u32(&bar[warp]));
@@ -246,7 +259,7 @@ int main() {
         CK(cudaMemset(d_cyc, 0, 3 * sizeof(unsigned long long)));
         CK(cudaMemset(d_status, 0, sizeof(int)));
         CK(cudaMemset(d_out, 0, 128 * 256 * sizeof(int)));
-        k_probe<<<1, 128, 4 * slot_bytes>>>(c, 4, 1, d_src, src_bytes, d_cyc, d_status, d_out);
+        k_probe<<<1, 128, 4 * slot_bytes>>>(c, 4, 1, d_src, src_bytes, d_cyc, d_status, d_out, 0);
         CK(cudaGetLastError());
         CK(cudaDeviceSynchronize());
         int st;
@@ -291,7 +304,7 @@ int main() {
                 if (per_sm == 2 && 2 * (req + 1024 + 256) > 228 * 1024) continue;
                 CK(cudaMemset(d_cyc, 0, 3 * sizeof(unsigned long long)));
                 CK(cudaMemset(d_status, 0, sizeof(int)));
-                k_probe<<<SM * per_sm, 128, req>>>(c, n_kb, issuers, d_src, src_bytes, d_cyc, d_status, nullptr);
+                k_probe<<<SM * per_sm, 128, req>>>(c, n_kb, issuers, d_src, src_bytes, d_cyc, d_status, nullptr, 0);
                 CK(cudaGetLastError());
                 CK(cudaDeviceSynchronize());
                 unsigned long long cy[3];
@@ -307,6 +320,27 @@ int main() {
                     per_sm_kb, (c.a_bytes + c.b_bytes) / per_sm_kb, st);
                 if (st) ++failures;
             }
+        }
+    }
+    // ---- a commit (tcgen05.commit to an mbarrier, not waited on) after every 1, 4 or 16 K-blocks
+    for (const Shape& c : {shape(1, 128, 96, 8), shape(0, 128, 64, 8)}) {
+        const int slot_bytes = (c.a_bytes + c.b_bytes + 1023) & ~1023;
+        const int req = std::max(c.slots * slot_bytes, 80 * 1024);
+        for (int every : {0, 16, 4, 1}) {
+            const int n_kb = 4096;
+            CK(cudaMemset(d_cyc, 0, 3 * sizeof(unsigned long long)));
+            CK(cudaMemset(d_status, 0, sizeof(int)));
+            k_probe<<<SM * 2, 128, req>>>(c, n_kb, 1, d_src, src_bytes, d_cyc, d_status, nullptr, every);
+            CK(cudaGetLastError());
+            CK(cudaDeviceSynchronize());
+            unsigned long long cy[3];
+            int st;
+            CK(cudaMemcpy(cy, d_cyc, sizeof(cy), cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost));
+            std::printf("commit %s M %d N %3d, commit every %2d K-blocks (0: none), 2 CTAs/SM: issuer %.1f clk per K-block, "
+                        "%.1f clk per K-block per CTA to completion, wait status %d\n",
+                        c.kind == 0 ? "f16 " : "u8s8", c.M, c.N, every, (double)cy[0] / n_kb, (double)cy[2] / n_kb, st);
+            if (st) ++failures;
         }
     }
     std::printf("%s\n", failures ? "FAILED" : "done");
