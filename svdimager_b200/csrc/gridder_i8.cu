@@ -18,9 +18,10 @@
 //                 imaginary (comp 1) part;
 // so ONE tcgen05.mma kind::i8 (M = 128, N = 96, K = 32, A unsigned, B signed) per 32 samples forms
 // all nine digit products D_de in int32, and the epilogue adds sum_de 2^(8 (d + e)) D_de, which is
-// sum_k A_q B_q exactly. Integer accumulation does not round, so all K-blocks of a tile key go into
-// one accumulator (at most kIntervalKB = 2048 of them: |a_d b_e| <= 255 * 128 keeps the int32 sums
-// of 65,536 samples in range), and the result does not depend on the order of the samples.
+// sum_k A_q B_q exactly. Integer accumulation does not round, so consecutive K-blocks of a tile key
+// share one accumulator for as long as they last within a chunk of the schedule (at most
+// kChunkKB = 64 K-blocks; int32 would hold kIntervalKB = 2048 of them: |a_d b_e| <= 255 * 128 for
+// 65,536 samples), and the result does not depend on the order of the samples.
 //
 // Cost model (measured on B200): a tcgen05.mma costs its issuing thread ~140 clk (8-bit) whatever
 // its N, and the tensor core reads shared-memory operands at ~100-117 B/clk per SM. The 8-bit form
@@ -90,6 +91,8 @@ static_assert(kI8TileRows + 8 <= kWinRows && kI8TileCols + 8 <= kWinCols, "tile 
 static_assert(kSubBytes % 1024 == 0, "K-block operands stay 1 KB aligned");
 static_assert(kEpiWarp0 + 4 == kWarps, "four epilogue warps (one per TMEM lane quarter) come last");
 static_assert(kRecSlots <= kMetaRing && kKB == 32, "one record slot per published K-block, one lane per record");
+static_assert(kChunkKB <= kIntervalKB && kMetaRing % kSubStages == 0,
+              "intervals end with their chunk; a stage's interval flags are one aligned word");
 
 // MN-major, no-swizzle 8-bit operand with kKB K-columns: element (mn, k) at byte
 // (mn % 16) + (k % 8) * 16 + (k / 8) * 128 + (mn / 16) * 512.
@@ -159,6 +162,7 @@ struct __align__(8) I8Shared {
     unsigned long long fdone[kAccBufs];   // MMA -> epilogue: the interval's MMAs done (commit)
     unsigned long long ffree[kAccBufs];   // epilogue -> MMA: accumulator read (4 warp arrivals)
     KBMeta meta[kMetaRing];
+    unsigned char open[kMetaRing];        // scheduler -> MMA: 1 where a K-block starts an interval
     Event events[kEventRing];
     unsigned int published;               // K-block descriptors published
     unsigned int consumed;                // K-blocks whose descriptor and records everyone is done with
@@ -399,10 +403,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_i8(I8Params P, GridGeom g,
         }
     } else if (warp == kSchedWarp) {
         // ============================ scheduler ============================
-        schedule_kblocks<kKB, kMetaRing, kRecSlots, kChunkKB>(S, P, smem + kRecOff, kb_lo, kb_hi, P.keymax, abort_flag, lane);
+        schedule_kblocks<kKB, kMetaRing, kRecSlots, kChunkKB>(S, P, smem + kRecOff, kb_lo, kb_hi, P.keymax, S.open,
+                                                              abort_flag, lane);
     } else if (warp == kMmaWarp) {
         // ============================ MMA issuer ============================
-        // The K-blocks of one key (at most kIntervalKB in a row) accumulate in one of the kAccBufs
+        // An interval -- K-blocks of one key, opened where the scheduler flagged a key change or a
+        // chunk start -- accumulates in one of the kAccBufs
         // TMEM accumulators; closing the interval commits its MMAs to fdone[b] and hands the
         // accumulator to the epilogue.
         int cur_key = -1;
@@ -477,21 +483,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_i8(I8Params P, GridGeom g,
             }
             nin = __shfl_sync(0xffffffffu, nin, 0);
             if (nin <= 0) break;
-            int mkey = 0;
-            float mscale = 0.0f;
-            if (lane < nin) {
-                const KBMeta& mt = S.meta[(i0 + lane) % kMetaRing];
-                mkey = mt.key;
-                mscale = mt.scale;
-            }
-            int keys[kSubStages];
-            float scales[kSubStages];
-#pragma unroll
-            for (int k = 0; k < kSubStages; ++k) {
-                keys[k] = __shfl_sync(0xffffffffu, mkey, k);
-                scales[k] = __shfl_sync(0xffffffffu, mscale, k);
-            }
+            // the stage's interval starts, one byte per K-block (the scheduler's; published with the
+            // descriptors); a K-block's key and scale are read only where an interval opens
             if (lane == 0 && !failed) {
+                const uint32_t opens = *reinterpret_cast<const uint32_t*>(&S.open[i0 % kMetaRing]);
                 if (!mbar_wait(smem_u32(&S.full[stg]), u & 1u, abort_flag)) failed = true;
                 tc_fence_after();  // the producers' operand writes are ordered before the MMAs
                 // producers and this warp are done with the descriptors and records of the stage
@@ -500,10 +495,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_i8(I8Params P, GridGeom g,
 #pragma unroll
                 for (int k = 0; k < kSubStages; ++k) {
                     if (k < nin && !failed) {
-                        if (on > 0 && (keys[k] != cur_key || on == kIntervalKB)) close_interval();
-                        cur_key = keys[k];
-                        cur_scale = scales[k];
-                        if (on == 0) {  // open an interval on the next accumulator, once the epilogue has read it
+                        if ((opens >> (8 * k)) & 1u) {  // a new interval on the next accumulator
+                            close_interval();
+                            const KBMeta& mt = S.meta[(i0 + k) % kMetaRing];
+                            cur_key = mt.key;
+                            cur_scale = mt.scale;
                             const int b = next_buf;
                             next_buf = (next_buf + 1) % kAccBufs;
                             if (fuse[b] > 0 && !mbar_wait(smem_u32(&S.ffree[b]), (fuse[b] - 1) & 1u, abort_flag))

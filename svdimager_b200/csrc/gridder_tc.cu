@@ -474,7 +474,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_tc(TcParams P, GridGeom g,
         }
     } else if (warp == kSchedWarp) {
         // ============================ scheduler ============================
-        schedule_kblocks<kKB, kMetaRing, kRecSlots, kChunkKB>(S, P, smem + kRecOff, kb_lo, kb_hi, nullptr, abort_flag, lane);
+        schedule_kblocks<kKB, kMetaRing, kRecSlots, kChunkKB>(S, P, smem + kRecOff, kb_lo, kb_hi, nullptr, nullptr,
+                                                              abort_flag, lane);
     } else if (warp == kMmaWarp) {
         // ============================ MMA issuer ============================
         // Consecutive K-blocks of one key form an interval (at most kIntervalKB K-blocks) that

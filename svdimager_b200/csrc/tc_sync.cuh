@@ -168,11 +168,13 @@ __device__ __forceinline__ float key_fixed_scale(float vmax) {
 // Run by one warp (`lane` its lane); S and P are the kernel's shared state and parameters (members
 // meta, rec_full, published, consumed, sched_done; offsets, kb_offsets, key_lo, key_hi, work, rec,
 // status), rec_smem the record slots, [kb_lo, kb_hi) the K-blocks of the key range; keymax (may be
-// null) the per-key max |value| from which each K-block's scale is set.
+// null) the per-key max |value| from which each K-block's scale is set; open (may be null, kMetaRing
+// bytes) receives per published K-block 1 when it starts an accumulation interval -- its key differs
+// from the previous published K-block's, or it is the first of its chunk -- and 0 otherwise.
 template <int kKB, int kMetaRing, int kRecSlots, int kChunkKB, class Shared, class Params>
 __device__ void schedule_kblocks(Shared& S, const Params& P, unsigned char* rec_smem, unsigned int kb_lo,
-                                 unsigned int kb_hi, const unsigned int* keymax, const volatile int* abort_flag,
-                                 int lane) {
+                                 unsigned int kb_hi, const unsigned int* keymax, unsigned char* open,
+                                 const volatile int* abort_flag, int lane) {
     static_assert(kRecSlots <= 32 && kRecSlots <= kMetaRing, "one lane per K-block published at once");
     struct Window {
         unsigned int off, kbo, km;  // this lane's key
@@ -190,6 +192,7 @@ __device__ void schedule_kblocks(Shared& S, const Params& P, unsigned char* rec_
         return w;
     };
     unsigned int published = 0;
+    int prev_key = -1;  // key of the last K-block published (warp-uniform)
     bool ok = true;
     for (;;) {
         // next chunk of K-blocks
@@ -253,6 +256,14 @@ __device__ void schedule_kblocks(Shared& S, const Params& P, unsigned char* rec_
                 const uint32_t bar = smem_u32(&S.rec_full[idx % kRecSlots]);
                 mbar_arrive_expect_tx(bar, cnt * 16u);
                 bulk_g2s(smem_u32(rec_smem + (idx % kRecSlots) * kKB * 16), P.rec + pos, cnt * 16u, bar);
+            }
+            if (open) {  // interval starts: a key change, or the first K-block of the chunk
+                const int key_i = kc + ci;
+                int key_p = __shfl_up_sync(0xffffffffu, key_i, 1);
+                if (lane == 0) key_p = prev_key;
+                if ((unsigned int)lane < n)
+                    open[(published + (unsigned int)lane) % kMetaRing] = (key_i != key_p || gi == kb0) ? 1 : 0;
+                prev_key = __shfl_sync(0xffffffffu, key_i, (int)n - 1);
             }
             published += n;
             g += n;

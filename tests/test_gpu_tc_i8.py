@@ -113,9 +113,10 @@ def test_i8_edge_clipping_and_integer_positions(cuda_device):
 
 def test_i8_pile_longer_than_one_accumulator_interval(cuda_device):
     """80,000 coincident samples with near-maximal, nearly equal values in one tile key: more than
-    the 2048 K-blocks (65,536 samples) one int32 accumulator interval may hold, so the key's
-    accumulation is split; every digit product of the pile is the same, the case that would
-    overflow int32 first. Grid and image against the oracle."""
+    the 2048 K-blocks (65,536 samples) an int32 accumulator could hold, so the key's accumulation
+    must be split (the gridder ends every interval with its 64-K-block chunk); every digit product of
+    the pile is the same, the case that would overflow int32 first. Grid and image against the
+    oracle."""
     N, cell, G = 64, 2e-3, 96
     scale = float(np.float32(cell)) * G
     rng = np.random.default_rng(13)
