@@ -152,7 +152,7 @@ struct Event {
     int buf;      // accumulator to drain
     int key;      // its tile key
     int parity;   // phase parity of the accumulator's MMAs-done barrier
-    float scale;  // the key's fixed-point scale of B
+    float inv;    // 1 / the key's fixed-point scale of B (0: no finite non-zero value)
 };
 
 struct __align__(8) I8Shared {
@@ -412,7 +412,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_i8(I8Params P, GridGeom g,
         // TMEM accumulators; closing the interval commits its MMAs to fdone[b] and hands the
         // accumulator to the epilogue.
         int cur_key = -1;
-        float cur_scale = 0.0f;
+        float cur_inv = 0.0f;
         int ob = 0, on = 0, next_buf = 0;
         unsigned int fuse[kAccBufs];
 #pragma unroll
@@ -445,7 +445,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_i8(I8Params P, GridGeom g,
         auto close_interval = [&]() {  // lane 0
             if (on > 0) {
                 mma_commit(smem_u32(&S.fdone[ob]));
-                push_event(Event{kEvDrain, ob, cur_key, (int)(fuse[ob] & 1u), cur_scale});
+                push_event(Event{kEvDrain, ob, cur_key, (int)(fuse[ob] & 1u), cur_inv});
                 ++fuse[ob];
                 on = 0;
             }
@@ -499,7 +499,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_i8(I8Params P, GridGeom g,
                             close_interval();
                             const KBMeta& mt = S.meta[(i0 + k) % kMetaRing];
                             cur_key = mt.key;
-                            cur_scale = mt.scale;
+                            cur_inv = mt.inv_scale;
                             const int b = next_buf;
                             next_buf = (next_buf + 1) % kAccBufs;
                             if (fuse[b] > 0 && !mbar_wait(smem_u32(&S.ffree[b]), (fuse[b] - 1) & 1u, abort_flag))
@@ -606,11 +606,16 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_i8(I8Params P, GridGeom g,
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&S.ffree[ev.buf]));  // the accumulator is read
+            // cells in 32-bit plane coordinates (0 .. G - 1; G <= 46340, so r G + c fits)
             const int slab = ev.key / tiles2;
-            const int t1 = (ev.key / g.ntile2) % g.ntile, t2 = ev.key % g.ntile2;
-            const float inv_scale = ev.scale > 0.0f ? 1.0f / (kAScale * ev.scale) : 0.0f;
+            const int rem = ev.key - slab * tiles2;
+            const int t1 = rem / g.ntile2, t2 = rem - t1 * g.ntile2;
+            const float inv_scale = ev.inv * (1.0f / kAScale);
             const int k2 = lane & 7;
-            const long long g2 = g.gmin + (long long)t2 * g.T2 + 2 * k2;
+            const int last = (int)(g.G - 1);
+            const int gi = (int)g.G;
+            const int c = t2 * g.T2 + 2 * k2;        // this lane's first cell column
+            const int r0 = t1 * g.T + 8 * q;         // the warp's first window row
             float2* const plane = P.planes + (long long)(slab - P.slab_lo) * GG;
 #pragma unroll
             for (int it = 0; it < 2; ++it) {
@@ -624,16 +629,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_i8(I8Params P, GridGeom g,
                     v.z += u.z;
                     v.w += u.w;
                 }
-                const long long g1 = g.gmin + (long long)t1 * g.T + 8 * q + jrow;
-                if (g1 <= g.gmax && g2 <= g.gmax && (v.x != 0.0f || v.y != 0.0f || v.z != 0.0f || v.w != 0.0f)) {
-                    const float s0 = ((g1 + g2) & 1) ? -inv_scale : inv_scale;
-                    const long long cell = (g1 - g.gmin) * g.G + (g2 - g.gmin);
+                const int r = r0 + jrow;
+                if (r <= last && c <= last && (v.x != 0.0f || v.y != 0.0f || v.z != 0.0f || v.w != 0.0f)) {
+                    // checkerboard sign of grid cell (gmin + r, gmin + c): 2 gmin is even
+                    const float s0 = ((r + c) & 1) ? -inv_scale : inv_scale;
+                    const int cell = r * gi + c;
                     float2* p = plane + cell;
-                    if (g2 + 1 <= g.gmax && (cell & 1) == 0) {  // two cells, 16-byte aligned
+                    if (c + 1 <= last && (cell & 1) == 0) {  // two cells, 16-byte aligned
                         red_add_v4(p, s0 * v.x, s0 * v.y, -s0 * v.z, -s0 * v.w);
                     } else {
                         red_add_v2(p, s0 * v.x, s0 * v.y);
-                        if (g2 + 1 <= g.gmax) red_add_v2(p + 1, -s0 * v.z, -s0 * v.w);
+                        if (c + 1 <= last) red_add_v2(p + 1, -s0 * v.z, -s0 * v.w);
                     }
                 }
             }
@@ -662,8 +668,8 @@ int launch_grid_i8(const SampleRec* d_rec, const unsigned int* d_offsets, const 
         set_error("integer tensor-core gridder: bad key range");
         return SVDI_ERR_INTERNAL;
     }
-    if (g.W > 8 || (g.W & 1) || g.T != kI8TileRows || g.T2 != kI8TileCols) {
-        set_error("integer tensor-core gridder: needs even support <= 8 and 24 x 8 tiles");
+    if (g.W > 8 || (g.W & 1) || g.T != kI8TileRows || g.T2 != kI8TileCols || g.G > 46340) {
+        set_error("integer tensor-core gridder: needs even support <= 8, 24 x 8 tiles and a grid of at most 46340");
         return SVDI_ERR_UNSUPPORTED;
     }
     if (reinterpret_cast<uintptr_t>(d_rec) % 16 != 0) {

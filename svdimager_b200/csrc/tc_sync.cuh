@@ -145,6 +145,7 @@ struct KBMeta {
     unsigned int pos;   // first record
     int cnt;            // records (1..32)
     float scale;        // per-key fixed-point scale of the integer gridder (0 elsewhere)
+    float inv_scale;    // 1 / scale (0 with it)
 };
 
 // Fixed-point scale of a key whose largest |value| is vmax: 0.999 2^(22 - e) with vmax < 2^e, so
@@ -251,8 +252,8 @@ __device__ void schedule_kblocks(Shared& S, const Params& P, unsigned char* rec_
                 const unsigned int pos = ka + (unsigned int)kKB * (gi - kbo_k);
                 const unsigned int cnt = min((unsigned int)kKB, kend - pos);
                 const unsigned int idx = published + (unsigned int)lane;
-                S.meta[idx % kMetaRing] =
-                    KBMeta{kc + ci, pos, (int)cnt, keymax ? key_fixed_scale(__uint_as_float(km)) : 0.0f};
+                const float sc = keymax ? key_fixed_scale(__uint_as_float(km)) : 0.0f;
+                S.meta[idx % kMetaRing] = KBMeta{kc + ci, pos, (int)cnt, sc, sc > 0.0f ? 1.0f / sc : 0.0f};
                 const uint32_t bar = smem_u32(&S.rec_full[idx % kRecSlots]);
                 mbar_arrive_expect_tx(bar, cnt * 16u);
                 bulk_g2s(smem_u32(rec_smem + (idx % kRecSlots) * kKB * 16), P.rec + pos, cnt * 16u, bar);
