@@ -290,7 +290,7 @@ def widefield_phase(api, local, npix=256):
     px, py = rng.integers(0, N, npix), rng.integers(0, N, npix)
     points = []
     for W in (6, 8, 10, 12):
-        for tgt in (1e-6, 1e-7):
+        for tgt in (1e-5, 1e-6, 1e-7):
             from svdimager_b200 import autotune
             opts = dict(device=local, edge_mode=api.EDGE_STRICT, k_rule=api.KRULE_TARGET, target_error=tgt,
                         support=W, sigma=1.5, beta=autotune.es_beta(W, 1.5))
