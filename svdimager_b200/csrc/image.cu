@@ -132,7 +132,7 @@ __device__ __forceinline__ void recombine_pixel(long long x, long long y, const 
 
     const int K = sp.K;
     double jv[KMAX];
-    bessel_jn(2.0 * kPi * t3 * sp.slab_half, K - 1, jv);
+    bessel_jn_fast(2.0 * kPi * t3 * sp.slab_half, K - 1, jv);
     const long long G = g.G, GG = G * G;
     const long long gidx = GG / 2 + G / 2 + yr * G + xr;  // SVDIntegratedImager.cu:1397
     double sum = 0.0;
