@@ -637,11 +637,11 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
     g.gmin = -(g.G / 2);
     g.gmax = (g.G - 1) / 2;
     g.W = o.support;
-    // the tensor-core gridders accumulate one moment plane in TMEM (K == 1): the FP16 / BF16 form
-    // bins into 56 x 8 tiles (64 x 16 accumulator window, gridder_tc.cu), the integer form into
-    // 24 x 8 tiles (32 x 16 window, gridder_i8.cu); the integer form scales each key by its own
-    // max |value| from the scatter
-    const bool use_tc = is_tc_gridder(o.gridder) && sp.K == 1 && g.W <= 8;
+    // the tensor-core gridders accumulate one moment plane at a time in TMEM: the FP16 / BF16 form
+    // (K == 1) bins into 56 x 8 tiles (64 x 16 accumulator window, gridder_tc.cu), the integer form
+    // (any K, one launch per Chebyshev term) into 24 x 8 tiles (32 x 16 window, gridder_i8.cu);
+    // the integer form scales each key by its own max |value| from the scatter
+    const bool use_tc = is_tc_gridder(o.gridder) && (sp.K == 1 || o.gridder == SVDI_GRIDDER_TC_I8) && g.W <= 8;
     const bool use_i8 = use_tc && o.gridder == SVDI_GRIDDER_TC_I8;
     if (use_tc) {
         tc_tiles(o.gridder, g);
@@ -744,10 +744,11 @@ int image_core(svdi_engine* e, bool archive, SampleSource src, long long N, floa
         SVDI_CUDA(cudaMemsetAsync(e->planes.p, 0, plane_bytes * planes_per_batch, st));
         const int tiles2 = g.ntile * g.ntile2;
         if (use_i8) {
-            SVDI_TRY(launch_grid_i8(e->rec.as<SampleRec>(), e->offsets.as<unsigned int>(),
-                                    e->kb_offsets.as<unsigned int>(), n_keys, s0 * tiles2, s1 * tiles2, s0, g,
-                                    e->poly, e->planes.as<float2>(), e->keymax.as<unsigned int>(),
-                                    e->tc_status.as<unsigned int>(), e->sm_count, st));
+            SVDI_TRY(launch_grid_i8(e->rec.as<SampleRec>(), need_s ? e->rec_s.as<float>() : nullptr,
+                                    e->offsets.as<unsigned int>(), e->kb_offsets.as<unsigned int>(), n_keys,
+                                    s0 * tiles2, s1 * tiles2, s0, sp.K, g, e->poly, e->planes.as<float2>(),
+                                    e->keymax.as<unsigned int>(), e->tc_status.as<unsigned int>(), e->sm_count,
+                                    st));
         } else if (use_tc) {
             SVDI_TRY(launch_grid_tc(e->rec.as<SampleRec>(), e->offsets.as<unsigned int>(),
                                     e->kb_offsets.as<unsigned int>(), n_keys, s0 * tiles2,
@@ -1492,7 +1493,7 @@ int wide_capture(svdi_batch* b) {
     for (int gi = 0; gi < NG; ++gi) {
         Group& G = groups[gi];
         G.K = group_k[gi];
-        G.tc = tc_opt && G.K == 1 && o.support <= 8;
+        G.tc = tc_opt && (G.K == 1 || o.gridder == SVDI_GRIDDER_TC_I8) && o.support <= 8;
         G.g = geom_for(o, N, cell_f, G.K, G.tc);
         // the gridders take a key's slab as key / (tiles per slab): start the group on a multiple of
         // its tiles per slab (the keys skipped stay empty)
@@ -1656,10 +1657,10 @@ int wide_capture(svdi_batch* b) {
             unsigned int* stw = b->status.as<unsigned int>() + 4 * gi;
             if (G.tc && o.gridder == SVDI_GRIDDER_TC_I8) {
                 // status in [0], work counter in [2]; per-key scales from the scatter's maxima
-                SVDI_TRY(launch_grid_i8(b->rec.as<SampleRec>(), b->offsets.as<unsigned int>(),
-                                        b->kb_offsets.as<unsigned int>(), (int)nkeys, (int)G.key_lo, (int)G.key_hi,
-                                        (int)G.slab_lo, G.g, e->poly, pl, b->keymax.as<unsigned int>(), stw,
-                                        e->sm_count, st));
+                SVDI_TRY(launch_grid_i8(b->rec.as<SampleRec>(), need_s ? b->rec_s.as<float>() : nullptr,
+                                        b->offsets.as<unsigned int>(), b->kb_offsets.as<unsigned int>(), (int)nkeys,
+                                        (int)G.key_lo, (int)G.key_hi, (int)G.slab_lo, G.K, G.g, e->poly, pl,
+                                        b->keymax.as<unsigned int>(), stw, e->sm_count, st));
             } else if (G.tc) {
                 // the TC gridder keeps its status in [0], reads max |v| from the pointer and counts work in [2]
                 SVDI_TRY(launch_grid_tc(b->rec.as<SampleRec>(), b->offsets.as<unsigned int>(),

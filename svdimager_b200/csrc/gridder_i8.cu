@@ -1,8 +1,12 @@
 // Exact integer tensor-core ES gridder (tcgen05.mma kind::i8, int32 accumulation in tensor
-// memory), one moment plane, support W <= 8.
+// memory), one Chebyshev term of the w-slabs' moment planes per launch, support W <= 8.
 //
 // Replaces the same reference kernels as the other gridders (fused_gridding,
-// SVDIntegratedImager.cu:1218-1293; gridding, archive/FIPkernels.cu:383-452) for the K = 1 case.
+// SVDIntegratedImager.cu:1218-1293, whose inner loop over the K Chebyshev terms is :1276-1290;
+// gridding, archive/FIPkernels.cu:383-452). A launch grids term n of every slab in its key range:
+// the sample's value is multiplied by T_n(s) (s the record's Chebyshev argument, T_n by the
+// three-term recurrence in FP32) before B is quantised, and |T_n| <= 1 keeps the key's scale bound.
+// K terms take K launches over the same records.
 //
 // Gridding with a separable kernel is a sum of outer products: for the samples k of one tile,
 //   G[r][c] = sum_k  wx_k[r] * (wy_k[c] v_k)   =   (A B^T)[r][c].
@@ -143,8 +147,22 @@ struct I8Params {
     float2* planes;
     unsigned int* status;
     unsigned int* work;              // next chunk of K-blocks to hand out (zeroed by the host)
+    const float* rec_s;              // per record Chebyshev argument (term > 0 only)
     int key_lo, key_hi, slab_lo;
+    int K, term;                     // moment planes per slab; the term this launch grids
 };
+
+// T_n(s) by the three-term recurrence T_{k+1} = 2 s T_k - T_{k-1} (FP32, as the FP32 gridder)
+__device__ __forceinline__ float cheb_term(int n, float s) {
+    if (n == 0) return 1.0f;
+    float tm2 = 1.0f, tm1 = s;
+    for (int t = 2; t <= n; ++t) {
+        const float tt = 2.0f * s * tm1 - tm2;
+        tm2 = tm1;
+        tm1 = tt;
+    }
+    return tm1;
+}
 
 enum EventType : int { kEvDrain = 0, kEvExit = 1 };
 struct Event {
@@ -287,6 +305,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_i8(I8Params P, GridGeom g,
             const bool valid = lane < m.cnt;
             SampleRec r = {0, 0, 0.0f, 0.0f};
             if (valid) r = recs[slot * kKB + lane];
+            // Chebyshev argument of the sample (launches of term n > 0)
+            const float sarg = (P.term > 0 && valid) ? P.rec_s[m.pos + lane] : 0.0f;
             const int cx = r.xq >> 24, cy = r.yq >> 24;
             const int fxq = r.xq & 0xFFFFFF, fyq = r.yq & 0xFFFFFF;
             const int r0 = cx - (HW - 1), c0 = cy - (HW - 1);
@@ -300,7 +320,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_i8(I8Params P, GridGeom g,
                     const int lo_r = fxq ? r0 : cx - HW, nr = fxq ? W : W + 1;
                     const int lo_c = fyq ? c0 : cy - HW, nc = fyq ? W : W + 1;
                     const float px = (float)fxq * (1.0f / 16777216.0f), py = (float)fyq * (1.0f / 16777216.0f);
-                    float2* plane = P.planes + (long long)(slab - P.slab_lo) * GG;
+                    const float tn = cheb_term(P.term, sarg);
+                    const float vre = r.vre * tn, vim = r.vim * tn;
+                    float2* plane = P.planes + ((long long)(slab - P.slab_lo) * P.K + P.term) * GG;
                     for (int cidx = 0; cidx < nr * nc; ++cidx) {
                         const int rr = lo_r + cidx / nc, cc = lo_c + cidx % nc;
                         const long long g1 = o1 + rr, g2 = o2 + cc;
@@ -309,7 +331,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_i8(I8Params P, GridGeom g,
                         const float y = ((float)(cc - cy) - py) / (float)HW;
                         const float kv = es_exact(poly.beta, x) * es_exact(poly.beta, y);
                         const float sg = ((g1 + g2) & 1) ? -kv : kv;
-                        red_add_v2(plane + (g1 - g.gmin) * g.G + (g2 - g.gmin), sg * r.vre, sg * r.vim);
+                        red_add_v2(plane + (g1 - g.gmin) * g.G + (g2 - g.gmin), sg * vre, sg * vim);
                     }
                 }
                 // ---- A': row taps as 22-bit unsigned integers, three byte digits per row
@@ -361,7 +383,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_i8(I8Params P, GridGeom g,
             } else {
                 // ---- B': column taps times the visibility as 22-bit signed integers, three signed
                 // byte digits, shifted up by c0 bytes in each 16-column group
-                const float ks = m.scale;
+                const float ks = m.scale * cheb_term(P.term, sarg);
                 const float uy = fmaf(2.0f, (float)fyq * (1.0f / 16777216.0f), -1.0f);
                 float wy[8];
 #pragma unroll
@@ -616,7 +638,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_i8(I8Params P, GridGeom g,
             const int gi = (int)g.G;
             const int c = t2 * g.T2 + 2 * k2;        // this lane's first cell column
             const int r0 = t1 * g.T + 8 * q;         // the warp's first window row
-            float2* const plane = P.planes + (long long)(slab - P.slab_lo) * GG;
+            float2* const plane = P.planes + ((long long)(slab - P.slab_lo) * P.K + P.term) * GG;
 #pragma unroll
             for (int it = 0; it < 2; ++it) {
                 const int jrow = 4 * it + (lane >> 3);
@@ -660,12 +682,16 @@ __global__ void __launch_bounds__(kThreads, 2) k_grid_i8(I8Params P, GridGeom g,
 
 }  // namespace
 
-int launch_grid_i8(const SampleRec* d_rec, const unsigned int* d_offsets, const unsigned int* d_kb_offsets,
-                   int n_keys, int key_lo, int key_hi, int slab_lo, const GridGeom& g, const EsPoly& poly,
-                   float2* d_planes, const unsigned int* d_keymax, unsigned int* d_status, int sm_count,
-                   cudaStream_t st) {
+int launch_grid_i8(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d_offsets,
+                   const unsigned int* d_kb_offsets, int n_keys, int key_lo, int key_hi, int slab_lo, int K,
+                   const GridGeom& g, const EsPoly& poly, float2* d_planes, const unsigned int* d_keymax,
+                   unsigned int* d_status, int sm_count, cudaStream_t st) {
     if (key_lo < 0 || key_hi > n_keys || key_lo >= key_hi) {
         set_error("integer tensor-core gridder: bad key range");
+        return SVDI_ERR_INTERNAL;
+    }
+    if (K < 1 || (K > 1 && !d_rec_s)) {
+        set_error("integer tensor-core gridder: K > 1 needs the records' Chebyshev arguments");
         return SVDI_ERR_INTERNAL;
     }
     if (g.W > 8 || (g.W & 1) || g.T != kI8TileRows || g.T2 != kI8TileCols || g.G > 46340) {
@@ -683,12 +709,15 @@ int launch_grid_i8(const SampleRec* d_rec, const unsigned int* d_offsets, const 
         set_error("integer tensor-core gridder: kernel does not fit on an SM");
         return SVDI_ERR_UNSUPPORTED;
     }
-    // d_status: [0] give-up flags, [2] the work counter
-    SVDI_CUDA(cudaMemsetAsync(d_status + 2, 0, sizeof(unsigned int), st));
-    I8Params P{d_rec, d_offsets, d_kb_offsets, d_keymax, d_planes, d_status, d_status + 2, key_lo, key_hi, slab_lo};
-    // two CTAs per SM (two MMA-issuing threads), each with 256 of the SM's 512 TMEM columns
-    k_grid_i8<<<2 * sm_count, kThreads, kSmemBytes, st>>>(P, g, poly);
-    SVDI_LAUNCHED();
+    // d_status: [0] give-up flags, [2] the work counter; one launch per Chebyshev term
+    for (int term = 0; term < K; ++term) {
+        SVDI_CUDA(cudaMemsetAsync(d_status + 2, 0, sizeof(unsigned int), st));
+        I8Params P{d_rec,  d_offsets, d_kb_offsets, d_keymax, d_planes, d_status, d_status + 2,
+                   d_rec_s, key_lo,    key_hi,       slab_lo,  K,        term};
+        // two CTAs per SM (two MMA-issuing threads), each with 256 of the SM's 512 TMEM columns
+        k_grid_i8<<<2 * sm_count, kThreads, kSmemBytes, st>>>(P, g, poly);
+        SVDI_LAUNCHED();
+    }
     return SVDI_OK;
 }
 

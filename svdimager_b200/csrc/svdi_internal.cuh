@@ -212,14 +212,15 @@ int launch_dft_probe(const SampleSource& src, const GridGeom& g, const SlabParam
                      double* d_acc, int sm_count, cudaStream_t st);
 
 constexpr int kTcKBlock = 32;      // records per K-block (one MMA pair of K steps)
-// gridder_i8.cu: exact integer tcgen05 gridder (one moment plane, support <= 8)
+// gridder_i8.cu: exact integer tcgen05 gridder (support <= 8; one launch per Chebyshev term)
 constexpr int kI8TileRows = 24;    // tile rows: footprint origins; 32-row accumulator window with halo
 constexpr int kI8TileCols = 8;     // tile columns: footprint origins; 16-column window with halo
-// d_keymax: the scatter's per-key max |value| (float bits)
-int launch_grid_i8(const SampleRec* d_rec, const unsigned int* d_offsets, const unsigned int* d_kb_offsets,
-                   int n_keys, int key_lo, int key_hi, int slab_lo, const GridGeom& g, const EsPoly& poly,
-                   float2* d_planes, const unsigned int* d_keymax, unsigned int* d_status, int sm_count,
-                   cudaStream_t st);
+// d_keymax: the scatter's per-key max |value| (float bits); d_rec_s: the records' Chebyshev
+// arguments (K > 1); moment plane (slab - slab_lo) * K + n receives term n
+int launch_grid_i8(const SampleRec* d_rec, const float* d_rec_s, const unsigned int* d_offsets,
+                   const unsigned int* d_kb_offsets, int n_keys, int key_lo, int key_hi, int slab_lo, int K,
+                   const GridGeom& g, const EsPoly& poly, float2* d_planes, const unsigned int* d_keymax,
+                   unsigned int* d_status, int sm_count, cudaStream_t st);
 int launch_grid_tc(const SampleRec* d_rec, const unsigned int* d_offsets, const unsigned int* d_kb_offsets,
                    int n_keys, int key_lo, int key_hi, int slab_lo, const GridGeom& g, const EsPoly& poly,
                    float2* d_planes, const unsigned int* d_vmax, unsigned int* d_status, int sm_count,

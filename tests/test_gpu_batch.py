@@ -113,6 +113,21 @@ def test_wide_batch_with_mixed_chebyshev_orders(cuda_device, stream5):
     e.close()
 
 
+def test_wide_batch_integer_gridder_mixed_chebyshev_orders(cuda_device, stream5):
+    """The mixed-order batch on the integer tensor-core gridder: each group of tile keys is gridded
+    by one launch per Chebyshev term (the multi-term group reads the records' Chebyshev arguments);
+    every image equals the engine's."""
+    wf = synth.make_snapshot("widefield", n_rows_limit=3000, nchan=8)
+    snaps = [stream5[0], wf, stream5[1]]
+    keep, descs, imgs, b, e, out1 = _batch_vs_single(snaps, gridder=api.GRIDDER_TC_I8,
+                                                     k_rule=api.KRULE_TARGET, target_error=1e-6)
+    assert b.wide
+    plans = [b.plan(i) for i in range(len(descs))]
+    assert max(p["num_terms"] for p in plans) > 1, plans
+    b.close()
+    e.close()
+
+
 @pytest.mark.parametrize("gridder", [api.GRIDDER_TC, api.GRIDDER_TC_I8])
 def test_batch_tensor_core_gridder(cuda_device, stream5, gridder):
     """Wide batch on a tensor-core gridder (split FP16 and exact integer): one gridder launch over

@@ -2,8 +2,9 @@
 weights and column weights x visibility as three byte digits, int32 accumulation in tensor memory)
 with the oracle, with the FP32 gridder and with the FP64 direct DFT.
 
-The integer path grids one moment plane per w-slab (K = 1), so these tests fix K = 1 on both sides.
-Tile binning (24 x 8 tiles) stays bit-exact. Grid planes: each contribution is quantised to 2^-22
+The integer path grids one Chebyshev term per launch (T_n(s) folded into the sample's value), so
+most tests fix K = 1 on both sides and the multi-term tests compare every moment plane of K = 8 and
+of a multi-slab w-term case. Tile binning (24 x 8 tiles) stays bit-exact. Grid planes: each contribution is quantised to 2^-22
 of the row weight's range and of the key's largest |value| (the sums themselves are exact), plus
 the ES polynomial (<= 1.2e-7); planes are compared at I8_GRID_TOL relative L2. Images: 1e-5
 relative RMS, as for the FP32 path."""
@@ -192,3 +193,68 @@ def test_i8_precision_config_accuracy(cuda_device):
     print("precision (integer tensor core): rel RMS vs FP64 DFT", err, "peak", peak, "vs FP32 path",
           O.rel_rms(R, R32))
     assert err < IMG_TOL
+
+
+@pytest.fixture(scope="module")
+def i8_multi_run(cuda_device, small_snapshot):
+    """The main path's default Chebyshev rule (K = 8 on this snapshot) on the integer gridder."""
+    s = small_snapshot
+    e = api.Engine(gridder=api.GRIDDER_TC_I8, keep_grid=1)
+    img = e.image(s)
+    return dict(engine=e, image=img, stats=e.stats(), snap=s)
+
+
+def test_i8_multi_term_planes_match_oracle(i8_multi_run):
+    """Every one of the K = 8 moment planes (one launch per term, T_n(s) folded into B) against the
+    oracle grid, each relative to its own norm."""
+    s, e, st = i8_multi_run["snap"], i8_multi_run["engine"], i8_multi_run["stats"]
+    assert st["used_tc"] == 1 and st["num_terms"] == 8
+    assert st["tile"] == 24 and st["tile_cols"] == 8
+    G = st["grid_size"]
+    r = O.expand_coords(e.buffer(api.BUF_Q).reshape(-1, 3), e.buffer(api.BUF_S))
+    vin = np.array(st["vin"]).reshape(3, 3)
+    inv_det = 1.0 / abs(vin[0, 0] * vin[1, 1] - vin[0, 1] * vin[1, 0])
+    og = O.grid(r, e.buffer(api.BUF_VIS_REAL), e.buffer(api.BUF_VIS_IMAG), _scale(s.cell_size, G), G,
+                _slab_config_from_stats(st), inv_det)
+    grid = e.buffer(api.BUF_GRID).reshape(-1, G, G)
+    assert grid.shape == og.shape and og.shape[0] == 8
+    for p in range(og.shape[0]):
+        den = np.linalg.norm(og[p])
+        assert den > 0
+        err = np.linalg.norm(grid[p] - og[p]) / den
+        print("term", p, "rel L2 vs oracle", err)
+        assert err < I8_GRID_TOL, (p, err)
+
+
+def test_i8_multi_term_image_matches_oracle_and_fp32_path(i8_multi_run):
+    s = i8_multi_run["snap"]
+    o = O.image_sii(s)
+    assert o.sc.K == 8
+    assert O.rel_rms(i8_multi_run["image"], o.image) < IMG_TOL
+    with api.Engine() as e:
+        img32 = e.image(s)
+        assert e.stats()["used_tc"] == 0 and e.stats()["num_terms"] == 8
+    assert O.rel_rms(i8_multi_run["image"], img32) < IMG_TOL
+
+
+def test_i8_wterm_multi_slab_matches_oracle_and_dft(cuda_device):
+    """Non-coplanar snapshot on the integer gridder: several w-slabs x 12 Chebyshev terms (twelve
+    launches over the slabs' keys), against the oracle and the FP64 DFT."""
+    s = snapshot("widefield", nchan=4, n_rows_limit=6000, image_size=128, cell_size=6e-4)
+    with api.Engine(gridder=api.GRIDDER_TC_I8, k_rule=api.KRULE_FIXED, fixed_k=12, target_alpha=2.0,
+                    edge_mode=api.EDGE_STRICT, presplat=1) as e:
+        R = e.image(s)
+        st = e.stats()
+    o = O.image_sii(s, edge_mode=1, k_rule=12, target_alpha=2.0)
+    assert st["used_tc"] == 1
+    assert st["num_slabs"] == o.sc.num_slabs > 1 and st["num_terms"] == 12
+    assert O.rel_rms(R, o.pre) < IMG_TOL
+    rng = np.random.default_rng(2)
+    N = s.image_size
+    px, py = rng.integers(0, N, 300), rng.integers(0, N, 300)
+    inc = O.inclusion_mask(o.r, _scale(s.cell_size, o.G), o.G, edge_mode=1)
+    inv_det = 1 / abs(o.vin[0, 0] * o.vin[1, 1] - o.vin[0, 1] * o.vin[1, 0])
+    d = O.dft_pixels(o.r, o.vr, o.vi, inv_det, s.num_samples, o.vin, N, float(np.float32(s.cell_size)), px, py,
+                     inc)
+    m = np.isfinite(d)
+    assert O.rel_rms(R[py, px][m], d[m]) < IMG_TOL
