@@ -22,6 +22,16 @@
 // grid position, FP32 Horner), two samples per polynomial pass when 2W <= 16; lane (a, b) then
 // owns footprint cells (a + p * 32/W, b), whose shared-memory addresses are bank-conflict free
 // because the row stride is == W (mod 32).
+//
+// W = 8, one term (the main form): the loop is bound by the MIO pipe (shared-memory reductions,
+// loads and shuffles, about one warp instruction per SM clock), so each warp instruction serves
+// the two samples of a polynomial pass: lanes 16h .. 16h + 15 grid sample j + h, lane (a, rho)
+// the four cells (a, c0), (a, c1), (a + 4, c0), (a + 4, c1) with c1 = c0 ^ 4 and c0 the footprint
+// column whose bank residue (mod 8) is rho for the first half-warp and rho + 4 for the second
+// (the row stride is == 8 mod 32, so a row's eight cells cover the eight residues once). Every
+// reduction instruction then puts one half-warp on residues 0-3 and the other on 4-7 of distinct
+// rows: conflict-free whatever the two footprints' positions. Per sample: four reductions, two
+// shuffles and one load (the one-sample form: four, three and one and a half).
 #include "svdi_internal.cuh"
 
 #include <cmath>
@@ -200,6 +210,8 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
     constexpr int kThreads = C::NT, kWarps = C::NW;
     // per-warp staging of the decoded batch (32 samples + the zero pad): the polynomial arguments
     // {u_x, u_y}, and {v_re, v_im, shared address of the footprint origin, Chebyshev argument}
+    // W = 8, one term: two samples per warp instruction (header comment)
+    constexpr bool kSplit = (W == 8) && (KC == 1) && (C::RS % 32 == 8);
     __shared__ float2 st_u[kWarps][33];
     __shared__ float4 st_v[kWarps][33];
     __shared__ float2 st_t[kWarps][33];  // KC > 1: T_term0(s), T_term0+1(s) of the staged sample
@@ -232,6 +244,9 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
     const unsigned int lane_off_bytes = 4u * (unsigned int)lane_off;
     // this lane's polynomial argument in the staged pair {u_x, u_y} of sample j: u_arg[2 j]
     const float* u_arg = reinterpret_cast<const float*>(&st_u[warp][0]) + (PAIR ? 2 * (lane >> 4) : 0) + (is_x ? 0 : 1);
+    // kSplit: this lane's sample in the pass (h), its rows (ra, ra + 4) and its first column's
+    // bank residue
+    const int sp_h = lane >> 4, sp_ra = (lane >> 2) & 3, sp_rho = (lane & 3) + 4 * sp_h;
 
     for (int i = threadIdx.x; i < KC * 2 * C::PLANE; i += kThreads) tile[i] = 0;
     if (threadIdx.x == 0) {
@@ -379,7 +394,40 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
                     __syncwarp();
                     // ---- fast path: W x W footprint, polynomial weights, no bounds checks
                     constexpr int STEP = PAIR ? 2 : 1;
-                    if (KC == 1) {
+                    if constexpr (kSplit) {
+                        // two samples per warp instruction (header comment); slot nfast is the
+                        // zero pad when nfast is odd
+                        const int sh = 16 * sp_h;
+#pragma unroll 2
+                        for (int j = 0; j < nfast; j += 2) {
+                            const float u = u_arg[2 * j];
+                            float w = coef[kPolyDeg];
+#pragma unroll
+                            for (int d = kPolyDeg - 1; d >= 0; --d) w = fmaf(w, u, coef[d]);
+                            const float4 sf = st_v[warp][j + sp_h];
+                            const unsigned int org = __float_as_uint(sf.z);
+                            const int c0 = (sp_rho - (int)(org >> 2)) & 7;
+                            const int c1 = c0 ^ 4;
+                            const float wx0 = __shfl_sync(0xffffffffu, w, sh + sp_ra);
+                            const float wx1 = __shfl_sync(0xffffffffu, w, sh + sp_ra + 4);
+                            const float wy0 = __shfl_sync(0xffffffffu, w, sh + 8 + c0);
+                            const float wy1 = __shfl_sync(0xffffffffu, w, sh + 8 + c1);
+                            const unsigned int a0 = org + 4u * (unsigned int)(sp_ra * C::RS + c0);
+                            const unsigned int a1 = org + 4u * (unsigned int)(sp_ra * C::RS + c1);
+                            float kv = wx0 * wy0;
+                            red_shared<0>(a0, fx_round(fmaf(kv, sf.x, kMagic)));
+                            red_shared<4 * C::PLANE>(a0, fx_round(fmaf(kv, sf.y, kMagic)));
+                            kv = wx0 * wy1;
+                            red_shared<0>(a1, fx_round(fmaf(kv, sf.x, kMagic)));
+                            red_shared<4 * C::PLANE>(a1, fx_round(fmaf(kv, sf.y, kMagic)));
+                            kv = wx1 * wy0;
+                            red_shared<16 * C::RS>(a0, fx_round(fmaf(kv, sf.x, kMagic)));
+                            red_shared<16 * C::RS + 4 * C::PLANE>(a0, fx_round(fmaf(kv, sf.y, kMagic)));
+                            kv = wx1 * wy1;
+                            red_shared<16 * C::RS>(a1, fx_round(fmaf(kv, sf.x, kMagic)));
+                            red_shared<16 * C::RS + 4 * C::PLANE>(a1, fx_round(fmaf(kv, sf.y, kMagic)));
+                        }
+                    } else if (KC == 1) {
 #pragma unroll 2
                         for (int j = 0; j < nfast; j += STEP) {
                             const float u = u_arg[2 * j];
