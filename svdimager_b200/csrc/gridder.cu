@@ -23,15 +23,15 @@
 // owns footprint cells (a + p * 32/W, b), whose shared-memory addresses are bank-conflict free
 // because the row stride is == W (mod 32).
 //
-// W = 8, one term (the main form): the loop is bound by the MIO pipe (shared-memory reductions,
+// W = 8 (the main form, any number of terms): the loop is bound by the MIO pipe (shared-memory reductions,
 // loads and shuffles, about one warp instruction per SM clock), so each warp instruction serves
 // the two samples of a polynomial pass: lanes 16h .. 16h + 15 grid sample j + h, lane (a, rho)
 // the four cells (a, c0), (a, c1), (a + 4, c0), (a + 4, c1) with c1 = c0 ^ 4 and c0 the footprint
 // column whose bank residue (mod 8) is rho for the first half-warp and rho + 4 for the second
 // (the row stride is == 8 mod 32, so a row's eight cells cover the eight residues once). Every
 // reduction instruction then puts one half-warp on residues 0-3 and the other on 4-7 of distinct
-// rows: conflict-free whatever the two footprints' positions. Per sample: four reductions, two
-// shuffles and one load (the one-sample form: four, three and one and a half).
+// rows: conflict-free whatever the two footprints' positions. Per sample: four reductions per
+// term, two shuffles and one load (the one-sample form: three shuffles and one and a half loads).
 #include "svdi_internal.cuh"
 
 #include <cmath>
@@ -84,6 +84,17 @@ __device__ __forceinline__ void grid_passes(unsigned int a, float w, float wy, f
             red_shared<4 * (P * RPP * RS + PLANE)>(a, fx_round(fmaf(kv, vi, kMagic)));
         }
         grid_passes<P + 1, PASSES, RPP, RS, PLANE, ALL>(a, w, wy, vr, vi, src0, wx_src, pass_on);
+    }
+}
+
+// The KC terms of one cell at shared-window address addr + OFF: term t's real and imaginary planes
+// lie 2 t PLANE and (2 t + 1) PLANE words further (t = T0 .. KC - 1).
+template <int T0, int KC, int OFF, int PLANE>
+__device__ __forceinline__ void red_terms(unsigned int addr, float ar, float ai, const float (&tv)[KC]) {
+    if constexpr (T0 < KC) {
+        red_shared<OFF + 8 * T0 * PLANE>(addr, fx_round(fmaf(ar, tv[T0], kMagic)));
+        red_shared<OFF + 8 * T0 * PLANE + 4 * PLANE>(addr, fx_round(fmaf(ai, tv[T0], kMagic)));
+        red_terms<T0 + 1, KC, OFF, PLANE>(addr, ar, ai, tv);
     }
 }
 
@@ -196,8 +207,9 @@ __device__ __forceinline__ void flush_region(int* __restrict__ tile, const int* 
     }
 }
 
+// KC <= 2: four CTAs per SM (at most 64 registers; the two-term form otherwise takes 80 and three)
 template <int W, int T, int KC>
-__global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
+__global__ void __launch_bounds__(TileCfg<W, T, KC>::NT, (KC <= 2 ? 4 : 1)) k_grid_fp32(
     const SampleRec* __restrict__ rec, const float* __restrict__ rec_s,
     const unsigned int* __restrict__ offsets, const unsigned int* __restrict__ chunk_key,
     const unsigned int* __restrict__ keymax, unsigned int* __restrict__ work, int key_lo, int key_hi,
@@ -210,8 +222,8 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
     constexpr int kThreads = C::NT, kWarps = C::NW;
     // per-warp staging of the decoded batch (32 samples + the zero pad): the polynomial arguments
     // {u_x, u_y}, and {v_re, v_im, shared address of the footprint origin, Chebyshev argument}
-    // W = 8, one term: two samples per warp instruction (header comment)
-    constexpr bool kSplit = (W == 8) && (KC == 1) && (C::RS % 32 == 8);
+    // W = 8: two samples per warp instruction (header comment)
+    constexpr bool kSplit = (W == 8) && (C::RS % 32 == 8);
     __shared__ float2 st_u[kWarps][33];
     __shared__ float4 st_v[kWarps][33];
     __shared__ float2 st_t[kWarps][33];  // KC > 1: T_term0(s), T_term0+1(s) of the staged sample
@@ -414,6 +426,24 @@ __global__ void __launch_bounds__(TileCfg<W, T, KC>::NT) k_grid_fp32(
                             const float wy1 = __shfl_sync(0xffffffffu, w, sh + 8 + c1);
                             const unsigned int a0 = org + 4u * (unsigned int)(sp_ra * C::RS + c0);
                             const unsigned int a1 = org + 4u * (unsigned int)(sp_ra * C::RS + c1);
+                            if constexpr (KC > 1) {
+                                // the lane's sample's terms T_term0 .. T_term0+KC-1 (staged pair, recurrence)
+                                float tv[KC];
+                                const float2 t01 = st_t[warp][j + sp_h];
+                                tv[0] = t01.x;
+                                tv[1] = t01.y;
+#pragma unroll
+                                for (int t = 2; t < KC; ++t) tv[t] = 2.0f * sf.w * tv[t - 1] - tv[t - 2];
+                                float kv = wx0 * wy0;
+                                red_terms<0, KC, 0, C::PLANE>(a0, kv * sf.x, kv * sf.y, tv);
+                                kv = wx0 * wy1;
+                                red_terms<0, KC, 0, C::PLANE>(a1, kv * sf.x, kv * sf.y, tv);
+                                kv = wx1 * wy0;
+                                red_terms<0, KC, 16 * C::RS, C::PLANE>(a0, kv * sf.x, kv * sf.y, tv);
+                                kv = wx1 * wy1;
+                                red_terms<0, KC, 16 * C::RS, C::PLANE>(a1, kv * sf.x, kv * sf.y, tv);
+                                continue;
+                            }
                             float kv = wx0 * wy0;
                             red_shared<0>(a0, fx_round(fmaf(kv, sf.x, kMagic)));
                             red_shared<4 * C::PLANE>(a0, fx_round(fmaf(kv, sf.y, kMagic)));
