@@ -122,9 +122,15 @@ long long next_nice_even(long long n) {
     }
 }
 
-// The two cuFFT plans of a pruned inverse 2-D FFT (get_plan).
+// The plans of a pruned inverse 2-D FFT (make_fft_plan).
 struct FftPlan {
-    cufftHandle rows = 0, cols = 0;  // cols == 0: `rows` is one 2-D plan of the whole grid
+    enum Mode { kFull2D = 0, kRowsCufftCols = 1, kRowsSharedCols = 2 };
+    Mode mode = kFull2D;
+    cufftHandle rows = 0, cols = 0;  // kFull2D: `rows` is one 2-D plan of the whole grid
+    ColFftPlan cp{};                 // kRowsSharedCols: the shared-memory column transforms
+    float2* d_tw = nullptr;
+    int* d_perm = nullptr;
+    cudaStream_t stream = nullptr;
     long long G = 0, N = 0;
     int batch = 0;
 };
@@ -132,7 +138,11 @@ struct FftPlan {
 void destroy_fft_plan(FftPlan& plan) {
     if (plan.rows) cufftDestroy(plan.rows);
     if (plan.cols) cufftDestroy(plan.cols);
+    if (plan.d_tw) cudaFree(plan.d_tw);
+    if (plan.d_perm) cudaFree(plan.d_perm);
     plan.rows = plan.cols = 0;
+    plan.d_tw = nullptr;
+    plan.d_perm = nullptr;
 }
 
 }  // namespace
@@ -379,9 +389,12 @@ int choose_slabs(svdi_engine* e, bool archive, double r3min, double r3max, doubl
 // every row (length G, contiguous) is transformed, then only the N columns it reads (the checkerboard
 // sign centres the transform, so pixel x reads column G / 2 + x - N / 2: one contiguous run) are
 // transformed along the rows' stride. The second pass does N / G of the full 2-D transform's work
-// there; the other columns keep their first-pass values and are never read. Grid sizes with a prime
-// factor above 7 (cuFFT's Bluestein path, which gave wrong in-place results for the interleaved
-// column batches on B200) keep one 2-D plan.
+// there; the other columns keep their first-pass values and are never read. For G = 2^a 3^b
+// (b <= 1, up to 12288) the column pass is this library's shared-memory transform (fft_cols.cu: a
+// CTA per block of adjacent columns, one launch over all planes); other 2,3,5,7-smooth sizes use a
+// strided cuFFT column plan per plane. Grid sizes with a prime factor above 7 (cuFFT's Bluestein
+// path, which gave wrong in-place results for the interleaved column batches on B200) keep one 2-D
+// plan.
 int make_fft_plan(long long G, long long N, int batch, cudaStream_t st, FftPlan& plan) {
     long long r = G;
     for (long long f : {2, 3, 5, 7})
@@ -389,14 +402,22 @@ int make_fft_plan(long long G, long long N, int batch, cudaStream_t st, FftPlan&
     int n = (int)G;
     if (r == 1) {
         SVDI_CUFFT(cufftPlanMany(&plan.rows, 1, &n, &n, 1, n, &n, 1, n, CUFFT_C2C, (int)(G * batch)));
-        SVDI_CUFFT(cufftPlanMany(&plan.cols, 1, &n, &n, n, 1, &n, n, 1, CUFFT_C2C, (int)N));
+        if (col_fft_supported(G)) {
+            SVDI_TRY(make_col_fft(G, plan.cp, &plan.d_tw, &plan.d_perm));
+            plan.mode = FftPlan::kRowsSharedCols;
+        } else {
+            SVDI_CUFFT(cufftPlanMany(&plan.cols, 1, &n, &n, n, 1, &n, n, 1, CUFFT_C2C, (int)N));
+            plan.mode = FftPlan::kRowsCufftCols;
+        }
     } else {
         int dims[2] = {n, n};
         SVDI_CUFFT(cufftPlanMany(&plan.rows, 2, dims, nullptr, 1, n * n, nullptr, 1, n * n, CUFFT_C2C, batch));
         plan.cols = 0;
+        plan.mode = FftPlan::kFull2D;
     }
     SVDI_CUFFT(cufftSetStream(plan.rows, st));
     if (plan.cols) SVDI_CUFFT(cufftSetStream(plan.cols, st));
+    plan.stream = st;
     plan.G = G;
     plan.N = N;
     plan.batch = batch;
@@ -417,8 +438,11 @@ int get_plan(svdi_engine* e, long long G, long long N, int batch, FftPlan& plan)
 
 int exec_fft(const FftPlan& plan, cufftComplex* planes, int nplanes) {
     SVDI_CUFFT(cufftExecC2C(plan.rows, planes, planes, CUFFT_INVERSE));
-    if (plan.cols == 0) return SVDI_OK;
+    if (plan.mode == FftPlan::kFull2D) return SVDI_OK;
     const long long c0 = plan.G / 2 - plan.N / 2;
+    if (plan.mode == FftPlan::kRowsSharedCols)
+        return launch_col_fft(reinterpret_cast<float2*>(planes), nplanes, plan.G, c0, plan.N, plan.cp, plan.d_tw,
+                              plan.d_perm, plan.stream);
     for (int p = 0; p < nplanes; ++p) {
         cufftComplex* col0 = planes + (long long)p * plan.G * plan.G + c0;
         SVDI_CUFFT(cufftExecC2C(plan.cols, col0, col0, CUFFT_INVERSE));

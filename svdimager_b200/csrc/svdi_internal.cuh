@@ -211,6 +211,23 @@ int launch_dft_probe(const SampleSource& src, const GridGeom& g, const SlabParam
                      long long N, double cell, const long long* d_px, const long long* d_py, int npix,
                      double* d_acc, int sm_count, cudaStream_t st);
 
+// fft_cols.cu: the pruned inverse FFT's column transforms in shared memory (G = 2^a 3^b, b <= 1,
+// 16 <= G <= 12288): pass radices, log2 of each pass's stride, twiddle-table steps, log2 of the
+// columns per CTA
+struct ColFftPlan {
+    int npass = 0;
+    int lcb = 0;
+    int rad[6] = {};
+    int s_log[6] = {};
+    int tw_step[6] = {};
+};
+bool col_fft_supported(long long G);
+// allocates the twiddle and output-permutation tables (cudaFree both)
+int make_col_fft(long long G, ColFftPlan& P, float2** d_tw, int** d_perm);
+// columns [c0, c0 + ncols) of each of nplanes G x G planes, in place
+int launch_col_fft(float2* d_planes, int nplanes, long long G, long long c0, long long ncols, const ColFftPlan& P,
+                   const float2* d_tw, const int* d_perm, cudaStream_t st);
+
 constexpr int kTcKBlock = 32;      // records per K-block (one MMA pair of K steps)
 // gridder_i8.cu: exact integer tcgen05 gridder (support <= 8; one launch per Chebyshev term)
 constexpr int kI8TileRows = 24;    // tile rows: footprint origins; 32-row accumulator window with halo
