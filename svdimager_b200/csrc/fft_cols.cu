@@ -124,24 +124,36 @@ __device__ __forceinline__ void cp_async16(float2* dst, const float2* src) {
 template <int R, int NT>
 __device__ __forceinline__ void col_pass(float2* __restrict__ sh, int G, int lcb, int s_log, int tw_step,
                                          const float2* __restrict__ tw) {
-    const int S = 1 << s_log, CB = 1 << lcb;
-    const int nbf = (G / R) << lcb;
+    // a thread takes one butterfly of two adjacent columns: 16-byte shared-memory accesses and
+    // the twiddles loaded once for both
+    const int S = 1 << s_log, CP = 1 << (lcb - 1);
+    const int nbf = (G / R) << (lcb - 1);
     for (int t = threadIdx.x; t < nbf; t += NT) {
-        const int c = t & (CB - 1), q = t >> lcb;
+        const int c = (t & (CP - 1)) * 2, q = t >> (lcb - 1);
         const int b = q >> s_log, j = q & (S - 1);
         const int base = b * R * S + j;
-        float2 v[16];
+        float2 v[16], u[16];
 #pragma unroll
-        for (int m = 0; m < R; ++m) v[m] = sh[((base + S * m) << lcb) + c];
+        for (int m = 0; m < R; ++m) {
+            const float4 w = *reinterpret_cast<const float4*>(sh + ((base + S * m) << lcb) + c);
+            v[m] = make_float2(w.x, w.y);
+            u[m] = make_float2(w.z, w.w);
+        }
         dft_r<R>(v);
+        dft_r<R>(u);
         if (j) {
             const int st = j * tw_step;
             int ix = st;
 #pragma unroll
-            for (int k = 1; k < R; ++k, ix += st) v[k] = c_mul(v[k], __ldg(&tw[ix]));
+            for (int k = 1; k < R; ++k, ix += st) {
+                const float2 w = __ldg(&tw[ix]);
+                v[k] = c_mul(v[k], w);
+                u[k] = c_mul(u[k], w);
+            }
         }
 #pragma unroll
-        for (int m = 0; m < R; ++m) sh[((base + S * m) << lcb) + c] = v[m];
+        for (int m = 0; m < R; ++m)
+            *reinterpret_cast<float4*>(sh + ((base + S * m) << lcb) + c) = make_float4(v[m].x, v[m].y, u[m].x, u[m].y);
     }
 }
 
