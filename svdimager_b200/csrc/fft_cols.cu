@@ -10,8 +10,14 @@
 // a power of two) takes the R elements b R S + j + S m (m < R) of a column, forms their inverse DFT
 // (e^{+2 pi i m k / R}), multiplies element k by e^{+2 pi i j k / (R S)} and writes it back to
 // b R S + j + S k. The twiddles come from a table of e^{+2 pi i t / G} (FP64-rounded), element k of
-// pass p reading entry j k G / (R S) (< G); the output permutation is a table too. The transform is
-// the inverse, unnormalised one, as cuFFT's CUFFT_INVERSE.
+// pass p reading entry j k G / (R S) (< G); the output permutation is a table too (the output row
+// of each block row, so the block is read back in order). The transform is the inverse,
+// unnormalised one, as cuFFT's CUFFT_INVERSE.
+//
+// Shared-memory rows are swizzled: block row r sits at row r ^ (f(r >> 3) & mask), f(x) = x ^
+// (x >> 2) ^ (x >> 4), mask = 16 / CB - 1 (the rows that share a 128-byte bank line). The last
+// passes take rows R or 2 R apart in a warp, which without it fall on the same banks (a 6144-row
+// block lost half its shared-memory wavefronts to conflicts).
 #include "svdi_internal.cuh"
 
 #include <cmath>
@@ -120,6 +126,12 @@ __device__ __forceinline__ void cp_async16(float2* dst, const float2* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
 }
 
+// the shared-memory row of block row r (file comment)
+__device__ __forceinline__ int srow(int r, int mask) {
+    const int x = r >> 3;
+    return r ^ ((x ^ (x >> 2) ^ (x >> 4)) & mask);
+}
+
 // one pass of radix R over the CTA's G x CB block (see the file comment)
 template <int R, int NT>
 __device__ __forceinline__ void col_pass(float2* __restrict__ sh, int G, int lcb, int s_log, int tw_step,
@@ -128,6 +140,7 @@ __device__ __forceinline__ void col_pass(float2* __restrict__ sh, int G, int lcb
     // the twiddles loaded once for both
     const int S = 1 << s_log, CP = 1 << (lcb - 1);
     const int nbf = (G / R) << (lcb - 1);
+    const int mask = (16 >> lcb) - 1;
     for (int t = threadIdx.x; t < nbf; t += NT) {
         const int c = (t & (CP - 1)) * 2, q = t >> (lcb - 1);
         const int b = q >> s_log, j = q & (S - 1);
@@ -135,7 +148,7 @@ __device__ __forceinline__ void col_pass(float2* __restrict__ sh, int G, int lcb
         float2 v[16], u[16];
 #pragma unroll
         for (int m = 0; m < R; ++m) {
-            const float4 w = *reinterpret_cast<const float4*>(sh + ((base + S * m) << lcb) + c);
+            const float4 w = *reinterpret_cast<const float4*>(sh + (srow(base + S * m, mask) << lcb) + c);
             v[m] = make_float2(w.x, w.y);
             u[m] = make_float2(w.z, w.w);
         }
@@ -153,7 +166,8 @@ __device__ __forceinline__ void col_pass(float2* __restrict__ sh, int G, int lcb
         }
 #pragma unroll
         for (int m = 0; m < R; ++m)
-            *reinterpret_cast<float4*>(sh + ((base + S * m) << lcb) + c) = make_float4(v[m].x, v[m].y, u[m].x, u[m].y);
+            *reinterpret_cast<float4*>(sh + (srow(base + S * m, mask) << lcb) + c) =
+                make_float4(v[m].x, v[m].y, u[m].x, u[m].y);
     }
 }
 
@@ -162,9 +176,10 @@ template <int NT>
 __global__ void __launch_bounds__(NT, 512 / NT) k_fft_cols(float2* __restrict__ planes, int G, long long c0,
                                                              int ncols, ColFftPlan P,
                                                              const float2* __restrict__ tw,
-                                                             const int* __restrict__ perm) {
+                                                             const int* __restrict__ out_row) {
     extern __shared__ __align__(16) float2 sh[];
     const int lcb = P.lcb, CB = 1 << lcb;
+    const int mask = (16 >> lcb) - 1;
     const int cb0 = blockIdx.x * CB;
     const int ncb = min(CB, ncols - cb0);
     float2* const pl = planes + (long long)blockIdx.y * G * G + c0 + cb0;
@@ -175,7 +190,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_fft_cols(float2* __restrict__ 
     for (int i = threadIdx.x; i < (n >> 1); i += NT) {
         const int r = i >> (lcb - 1), c = (i & ((CB >> 1) - 1)) * 2;
         const float2* src = pl + (long long)r * G + c;
-        float2* dst = sh + (r << lcb) + c;
+        float2* dst = sh + (srow(r, mask) << lcb) + c;
         if (al16 && c + 1 < ncb) {
             cp_async16(dst, src);
         } else {
@@ -197,11 +212,11 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_fft_cols(float2* __restrict__ 
         }
         __syncthreads();
     }
-    // output row r from its digit-reversed position, pairs of columns as on the way in
+    // block row r to its output row (digit reversal), pairs of columns as on the way in
     for (int i = threadIdx.x; i < (n >> 1); i += NT) {
         const int r = i >> (lcb - 1), c = (i & ((CB >> 1) - 1)) * 2;
-        const float2* src = sh + (__ldg(&perm[r]) << lcb) + c;
-        float2* dst = pl + (long long)r * G + c;
+        const float2* src = sh + (srow(r, mask) << lcb) + c;
+        float2* dst = pl + (long long)__ldg(&out_row[r]) * G + c;
         if (al16 && c + 1 < ncb) {
             *reinterpret_cast<float4*>(dst) = *reinterpret_cast<const float4*>(src);
         } else {
@@ -277,7 +292,7 @@ int make_col_fft(long long G, ColFftPlan& P, float2** d_tw, int** d_perm) {
             t /= rad[p];
             pos += k << P.s_log[p];
         }
-        perm[(size_t)nrow] = (int)pos;
+        perm[(size_t)pos] = (int)nrow;  // block row pos holds output row nrow
     }
     SVDI_CUDA(cudaMalloc(d_tw, (size_t)G * sizeof(float2)));
     SVDI_CUDA(cudaMalloc(d_perm, (size_t)G * sizeof(int)));
