@@ -230,8 +230,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_fft_cols(float2* __restrict__ 
 
 // Where it is used: grid sizes at which it measured faster than cuFFT's strided column plan on
 // B200 -- up to 1536 rows (two CTAs per SM; 1536: configuration B 49.5 -> 46.6 ms per 256
-// snapshots) and from 4096 (6144: 0.38 -> 0.24 ms per plane). At 3072 rows cuFFT's column kernel
-// stays ahead (0.091 against 0.095 ms for the 2048 columns of the precision snapshot's FFT).
+// snapshots) and from 4096 (6144: 0.38 -> 0.17 ms per plane). At 3072 rows cuFFT's column kernel
+// stays ahead (0.091 against 0.093 ms for the precision snapshot's whole FFT).
 bool col_fft_supported(long long G) {
     if (G < 16 || G > 12288 || (G > 1536 && G < 4096)) return false;
     long long r = G;
