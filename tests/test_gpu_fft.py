@@ -2,7 +2,8 @@
 unnormalised inverse 2-D DFT of the gridded planes (BUF_GRID) on the N columns the recombination
 reads, for the grid sizes of the shared-memory column transform (G = 2^a and 3 * 2^a up to 1536
 and from 4096: radix-3, -16 and -2/4/8 passes), of the strided cuFFT column plan (G = 150, 2048,
-3072) and of the full 2-D plan (G = 383, prime). FP32 transforms: 2e-6 relative L2."""
+3072) and of the full 2-D plan (G = 383, prime); odd N puts the read columns at an odd start and leaves the
+last column block short. FP32 transforms: 2e-6 relative L2."""
 import numpy as np
 import pytest
 
@@ -27,7 +28,9 @@ def _planes(N, cell, sigma=1.5, nchan=8, rows=3000, **kw):
 @pytest.mark.parametrize("N,sigma,G_expect", [
     (64, 1.5, 96), (128, 1.5, 192), (256, 1.5, 384), (512, 1.5, 768), (1024, 1.5, 1536),
     (2048, 1.5, 3072), (64, 2.0, 128), (256, 2.0, 512), (1024, 2.0, 2048), (2048, 2.0, 4096),
-    (100, 1.5, 150), (255, 1.5, 383)])
+    (100, 1.5, 150), (255, 1.5, 383),
+    # odd N: the read columns start at an odd column (8-byte copies) and the last block is ragged
+    (47, 2.0, 96), (95, 2.0, 192)])
 def test_moments_are_the_inverse_dft_of_the_grid(cuda_device, N, sigma, G_expect):
     G, grid, mom = _planes(N, 4e-4 * 256 / N, sigma=sigma)
     assert G == G_expect
