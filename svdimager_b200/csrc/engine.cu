@@ -181,10 +181,9 @@ struct svdi_engine {
     float spec_cell = 0.0f;
     svdi::SlabParams spec_sp{};
     cudaEvent_t ev_stats = nullptr;
-    // slabs per batch of the last (slab count, terms, grid size) asked for
-    bool bslab_cache_valid = false;
-    std::tuple<int, int, long long> bslab_key{0, 0, 0};
-    size_t bslab_cached = 1;
+    // slabs per batch of every (slab count, terms, grid size) asked for (a server slot alternates
+    // between request shapes)
+    std::map<std::tuple<int, int, long long>, size_t> bslab_cache;
     // Completion of the last call, read lazily (finish_pending): the device-API call returns once
     // its work is enqueued, so that the host can enqueue the next snapshot meanwhile.
     unsigned long long* h_ndrop = nullptr;  // pinned: dropped-sample count of the last call
@@ -529,7 +528,8 @@ size_t batch_slabs_for(svdi_engine* e, int nslab, int K, long long G) {
     // The free-memory query takes a driver lock that other processes on the GPU contend for (it
     // stalled calls by up to tens of milliseconds), so it is asked once per configuration.
     const auto key = std::make_tuple(nslab, K, G);
-    if (e->bslab_cache_valid && e->bslab_key == key) return e->bslab_cached;
+    const auto hit = e->bslab_cache.find(key);
+    if (hit != e->bslab_cache.end()) return hit->second;
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
         cudaGetLastError();
@@ -538,9 +538,8 @@ size_t batch_slabs_for(svdi_engine* e, int nslab, int K, long long G) {
     const size_t per_slab = (size_t)K * (size_t)G * (size_t)G * sizeof(float2);
     const size_t budget = (free_b + e->planes.cap) / 4;
     const size_t b = std::min<size_t>(nslab, std::max<size_t>(1, budget / per_slab));
-    e->bslab_cache_valid = true;
-    e->bslab_key = key;
-    e->bslab_cached = b;
+    if (e->bslab_cache.size() > 64) e->bslab_cache.clear();
+    e->bslab_cache.emplace(key, b);
     return b;
 }
 
