@@ -1,7 +1,7 @@
 // svd_integrated_imager_gpu Snapshots Image_Size Cell_Size Snapshot_Index Output_Name.fits
 // Argument order and exit codes of SVDIntegratedImager.cu:1763-1854 (argc != 6: usage, exit 2;
 // errors: message, exit 1). The first argument is a snapshot bundle (svdimager_b200/bundle.py),
-// the stand-in for a Measurement Set in this build.
+// which stands in for a Measurement Set: this library reads no casacore tables.
 #include <chrono>
 #include <exception>
 #include <iostream>
