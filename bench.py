@@ -533,7 +533,7 @@ def run_ours(args):
     # --lanes 1 --steps 2 --warmup 3)
     traffic = None
     if dom == "ms_grid" and args.config == "precision":
-        traffic = {"k_grid_fp32": 223104512, "k_grid_tc": 225017856, "k_grid_i8": 226813184}.get(name.split()[0])
+        traffic = {"k_grid_fp32": 223104512, "k_grid_tc": 225017856, "k_grid_i8": 224812288}.get(name.split()[0])
 
     cpu = cpu_baseline(snap, eng, api, st, args) if not args.no_cpu else None
     line = {
