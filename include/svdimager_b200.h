@@ -228,7 +228,10 @@ int svdi_engine_dft_pixels(svdi_engine* e, const int64_t* px, const int64_t* py,
  *              the same layout, sizes and w range: the recorded plans are reused as they are);
  *   d_images:  num_snapshots x N x N floats on the device, image s at d_images + s N^2.
  * The engine holds one batch at a time and must not image anything else while a launch is in
- * flight (the graph uses its buffers). */
+ * flight (the graph uses its buffers). With 16 or more snapshots the batch runs as two halves: the
+ * second half on an engine the batch creates with the same options and owns until
+ * svdi_batch_destroy, launched on a stream of its own beside the first half (svdi_batch_launch
+ * orders both after the caller's stream and the caller's stream after both). */
 typedef struct svdi_batch svdi_batch;
 int svdi_batch_create(svdi_engine* e, const svdi_host_ms* snapshots, size_t num_snapshots, size_t image_size,
                       float cell_size, float* d_images, svdi_batch** out);

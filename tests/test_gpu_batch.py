@@ -91,6 +91,25 @@ def test_batch_matches_single_images(cuda_device, stream5):
     e.close()
 
 
+def test_large_batch_splits_in_two_halves(cuda_device):
+    """A batch of 17 snapshots runs as two halves (8 and 9 snapshots) on two engines whose graphs
+    launch side by side: every image equals the engine's, a second launch repeats them, the plan of
+    a snapshot in either half is the engine's and the batch is wide."""
+    snaps = synth.batching_stream(17, n_rows_limit=2000)
+    keep, descs, imgs, b, e, out1 = _batch_vs_single(snaps)
+    assert b.wide
+    with api.Engine(edge_mode=api.EDGE_STRICT) as ref:
+        import torch
+        single = torch.zeros((N, N), dtype=torch.float32, device="cuda")
+        for i in (0, 8, 16):
+            ref.image_device(descs[i], N, CELL, single.data_ptr())
+            torch.cuda.synchronize()
+            st = ref.stats()
+            assert b.plan(i) == {"num_slabs": st["num_slabs"], "num_terms": st["num_terms"]}
+    b.close()
+    e.close()
+
+
 def test_batch_is_wide(cuda_device, stream5):
     keep, descs, imgs, b, e, out1 = _batch_vs_single(stream5)
     assert b.wide
