@@ -241,8 +241,8 @@ def batching_phase(api, local, n_snapshots=256, launches=3, seed_offset=0):
                      "plan_and_capture_s": round(t_cap, 2)}
         b.close()
         e.close()
-    # the same 256 snapshots as two half batches (alternate snapshots) on two engines whose graphs
-    # run on their own streams at the same time
+    # the same 256 snapshots as two batches (alternate snapshots) on two engines whose launches run
+    # on their own streams at the same time (each batch of 128 is itself two halves)
     halves = [descs[0::2], descs[1::2]]
     engines = [api.Engine(**best) for _ in halves]
     himgs = [torch.zeros((len(h), N, N), dtype=torch.float32, device=dev) for h in halves]
