@@ -278,12 +278,19 @@ class Engine:
                                               float(cell_size), ctypes.c_void_p(out_ptr),
                                               ctypes.c_void_p(stream_ptr)))
 
-    def fipipe(self, visreal, visimag, bin_, vin, image_size: int, cell_size: float) -> np.ndarray:
+    def fipipe(self, visreal, visimag, bin_, vin, image_size: int, cell_size: float,
+               out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Archive-semantics imaging of one quartet on this engine; `out`, when given, is a
+        C-contiguous float32 [image_size][image_size] array that receives the image."""
         vr = np.ascontiguousarray(visreal, np.float32)
         vi = np.ascontiguousarray(visimag, np.float32)
         b = np.ascontiguousarray(bin_, np.float32).reshape(-1)
         v = np.ascontiguousarray(vin, np.float32).reshape(-1)
-        out = np.zeros((image_size, image_size), np.float32)
+        if out is None:
+            out = np.zeros((image_size, image_size), np.float32)
+        elif (out.dtype != np.float32 or out.shape != (image_size, image_size)
+              or not out.flags["C_CONTIGUOUS"]):
+            raise SvdiError(1, "out must be a C-contiguous float32 [image_size][image_size] array")
         _check(lib().svdi_engine_fipipe_host(self._h, _ptr(vr), _ptr(vi), _ptr(b), _ptr(v), _ptr(out),
                                              vr.shape[0], int(image_size), float(cell_size)))
         return out

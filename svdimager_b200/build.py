@@ -29,7 +29,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
            "--expt-relaxed-constexpr", "-I", INCLUDE] + ARCH
 CU_SOURCES = ["preprocess.cu", "binning.cu", "gridder.cu", "gridder_tc.cu", "gridder_i8.cu", "fft_cols.cu", "image.cu", "engine.cu", "server.cu",
-              "noalloc.cu", "accuracy.cu", "sii_entry.cpp"]
+              "noalloc.cu", "accuracy.cu", "host_stage.cu", "sii_entry.cpp"]
 # diagnostics built beside the CLIs: tcgen05 MMA issue rates and operand-layout check, shared-memory
 # reduction rates (the measurements behind the gridders' design)
 PROBE_SOURCES = {"probe_tcgen05_mma": "probe_tcgen05_mma.cu", "probe_shared_red": "probe_shared_red.cu"}

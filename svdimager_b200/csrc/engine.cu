@@ -209,6 +209,8 @@ struct svdi_engine {
     double last_cell = 0.0;
     bool have_last = false;
     svdi::DevBuf probe;
+    // pageable host uploads and image downloads of the archive entry and the host-input call
+    svdi::HostStager stager;
     bool batch_bound = false;  // a batch's captured graph refers to this engine's buffers
 
     ~svdi_engine() {
@@ -254,6 +256,13 @@ int upload(DevBuf& b, const T* host, size_t n, cudaStream_t st) {
     SVDI_TRY(b.ensure(n * sizeof(T)));
     if (n) SVDI_CUDA(cudaMemcpyAsync(b.p, host, n * sizeof(T), cudaMemcpyHostToDevice, st));
     return SVDI_OK;
+}
+
+// upload through the engine's staging ring (pageable sources of several MB; others copy directly)
+template <typename T>
+int upload_staged(svdi_engine* e, DevBuf& b, const T* host, size_t n, cudaStream_t st) {
+    SVDI_TRY(b.ensure(n * sizeof(T)));
+    return e->stager.h2d(b.p, host, n * sizeof(T), st);
 }
 
 double read_target_alpha(const svdi_options& o) {
@@ -1030,9 +1039,9 @@ int archive_path(svdi_engine* e, const float* Visreal, const float* Visimag, con
     cudaStream_t st = e->stream;
     SVDI_CUDA(cudaSetDevice(e->device));
     SVDI_CUDA(cudaEventRecord(e->ev[0], st));
-    SVDI_TRY(upload(e->vr, Visreal, n, st));
-    SVDI_TRY(upload(e->vi, Visimag, n, st));
-    SVDI_TRY(upload(e->in_bin, Bin, n * 3, st));
+    SVDI_TRY(upload_staged(e, e->vr, Visreal, n, st));
+    SVDI_TRY(upload_staged(e, e->vi, Visimag, n, st));
+    SVDI_TRY(upload_staged(e, e->in_bin, Bin, n * 3, st));
     SVDI_TRY(upload(e->vin32, Vin, 9, st));
     SVDI_TRY(e->vin64.ensure(9 * 8));
     SVDI_TRY(e->stats.ensure(ST_COUNT * 8));
@@ -1049,7 +1058,7 @@ int archive_path(svdi_engine* e, const float* Visreal, const float* Visimag, con
     e->sz_q = 0;
     e->sz_s = 0;
     SVDI_TRY(image_core(e, true, src, (long long)N, cell, e->image.as<float>()));
-    SVDI_CUDA(cudaMemcpyAsync(dirty_image, e->image.p, N * N * 4, cudaMemcpyDeviceToHost, st));
+    SVDI_TRY(e->stager.d2h(dirty_image, e->image.p, N * N * 4, st));
     SVDI_CUDA(cudaEventRecord(e->ev[7], st));
     SVDI_CUDA(cudaStreamSynchronize(st));
     SVDI_TRY(finish_pending(e));
@@ -1154,14 +1163,14 @@ int svdi_engine_image_host(svdi_engine* e, const svdi_host_ms* h, size_t N, floa
     SVDI_CUDA(cudaEventRecord(e->ev_fork, st));
     SVDI_CUDA(cudaStreamWaitEvent(e->side, e->ev_fork, 0));
     cudaStream_t sd = e->side;
-    SVDI_TRY(upload(e->in_v0r, h->vis0_real, n, sd));
-    SVDI_TRY(upload(e->in_v0i, h->vis0_imag, n, sd));
-    SVDI_TRY(upload(e->in_v3r, h->vis3_real, n, sd));
-    SVDI_TRY(upload(e->in_v3i, h->vis3_imag, n, sd));
-    SVDI_TRY(upload(e->in_f0, h->flag0, n, sd));
-    SVDI_TRY(upload(e->in_f3, h->flag3, n, sd));
-    SVDI_TRY(upload(e->in_w0, h->weight0, n, sd));
-    SVDI_TRY(upload(e->in_w3, h->weight3, n, sd));
+    SVDI_TRY(upload_staged(e, e->in_v0r, h->vis0_real, n, sd));
+    SVDI_TRY(upload_staged(e, e->in_v0i, h->vis0_imag, n, sd));
+    SVDI_TRY(upload_staged(e, e->in_v3r, h->vis3_real, n, sd));
+    SVDI_TRY(upload_staged(e, e->in_v3i, h->vis3_imag, n, sd));
+    SVDI_TRY(upload_staged(e, e->in_f0, h->flag0, n, sd));
+    SVDI_TRY(upload_staged(e, e->in_f3, h->flag3, n, sd));
+    SVDI_TRY(upload_staged(e, e->in_w0, h->weight0, n, sd));
+    SVDI_TRY(upload_staged(e, e->in_w3, h->weight3, n, sd));
     svdi_host_ms d = *h;
     d.uvw = e->in_uvw.as<float>();
     d.frequencies_hz = e->in_freq.as<float>();
@@ -1175,8 +1184,7 @@ int svdi_engine_image_host(svdi_engine* e, const svdi_host_ms* h, size_t N, floa
     d.weight3 = e->in_w3.as<float>();
     SVDI_TRY(e->image.ensure(N * N * 4));
     SVDI_TRY(main_path_device(e, &d, N, cell, e->image.as<float>()));
-    SVDI_CUDA(cudaMemcpyAsync(dirty_image, e->image.p, N * N * 4, cudaMemcpyDeviceToHost, st));
-    SVDI_CUDA(cudaStreamSynchronize(st));
+    SVDI_TRY(e->stager.d2h(dirty_image, e->image.p, N * N * 4, st));
     SVDI_TRY(finish_pending(e));
     return SVDI_OK;
 }

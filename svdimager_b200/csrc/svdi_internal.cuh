@@ -228,6 +228,34 @@ int make_col_fft(long long G, ColFftPlan& P, float2** d_tw, int** d_perm);
 int launch_col_fft(float2* d_planes, int nplanes, long long G, long long c0, long long ncols, const ColFftPlan& P,
                    const float2* d_tw, const int* d_perm, cudaStream_t st);
 
+// host_stage.cu: copies between pageable host memory and the device through a pinned staging
+// ring that a pool of host threads fills and drains. A pageable cudaMemcpyAsync stages through the
+// driver's buffer with one host thread and so runs at about one core's memcpy speed; here several
+// threads copy slices of one slot while the copy engine moves the previous slot, so the host side
+// keeps up with the PCIe link. Pinned, registered or managed memory and copies below a few MB take
+// the plain cudaMemcpyAsync. The ring (three 16 MB slots) and the threads start on the first
+// staged copy. Not thread-safe: one stager serves one engine, whose calls are serialised.
+class HostStager {
+public:
+    HostStager() = default;
+    HostStager(const HostStager&) = delete;
+    HostStager& operator=(const HostStager&) = delete;
+    ~HostStager();
+    // true for host memory that CUDA neither allocated nor registered
+    static bool pageable(const void* host);
+    // Stream-ordered upload. Returns once `host` has been read (the caller may reuse it), like a
+    // pageable cudaMemcpyAsync; the device copy completes in stream order on `st`.
+    int h2d(void* dev, const void* host, size_t bytes, cudaStream_t st);
+    // Download after the work queued on `st`; returns once `host` holds the bytes.
+    int d2h(void* host, const void* dev, size_t bytes, cudaStream_t st);
+    int threads() const;
+
+private:
+    struct Impl;
+    Impl* impl_ = nullptr;
+    int init();
+};
+
 constexpr int kTcKBlock = 32;      // records per K-block (one MMA pair of K steps)
 // gridder_i8.cu: exact integer tcgen05 gridder (support <= 8; one launch per Chebyshev term)
 constexpr int kI8TileRows = 24;    // tile rows: footprint origins; 32-row accumulator window with halo
