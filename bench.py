@@ -231,8 +231,11 @@ def batching_phase(api, local, n_snapshots=256, launches=3, seed_offset=0):
         torch.cuda.synchronize(dev)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
+        # an NVTX range names the timed launches for a kernel-level profile (ncu --nvtx)
+        torch.cuda.nvtx.range_push(f"config_b_{name}")
         for _ in range(launches):
             b.launch(stream.cuda_stream)
+        torch.cuda.nvtx.range_pop()
         e1.record(stream)
         b.check()
         ms = e0.elapsed_time(e1) / launches
