@@ -493,8 +493,11 @@ def run_ours(args):
     e2e_s = replicas.max_over_ranks(time.perf_counter() - t0, dist, dev)
     e2e_sync_value = replicas.aggregate_rate(args.steps, ws, e2e_s)
     # streaming through the server: the next snapshot uploads while the previous one images
-    stream_out = e2e_stream(api, opts, psnap, N, cell, args.steps, args.warmup, dist, dev)
-    e2e_value = replicas.aggregate_rate(args.steps, ws, stream_out["seconds"])
+    # at least 64 requests: with 4 in flight, the window's fill and drain (about two snapshot
+    # latencies) stay under a tenth of the timed region also for short --steps runs
+    e2e_requests = max(args.steps, 64)
+    stream_out = e2e_stream(api, opts, psnap, N, cell, e2e_requests, args.warmup, dist, dev)
+    e2e_value = replicas.aggregate_rate(e2e_requests, ws, stream_out["seconds"])
     serving = None if args.no_serving else serving_phase(api, snap, args.serving_requests, 50.0, local,
                                                          gridder=gridder)
     batching = None if args.no_batching else batching_phase(api, local, args.batch_snapshots,
@@ -572,6 +575,7 @@ def run_ours(args):
                 "host_cpus": f"{len(host_cpus)} CPUs of the GPU's NUMA node" if host_cpus else "unbound",
                 "api": f"svdi_server submit/wait, {stream_out['slots']} slots, {stream_out['window']} requests "
                        "in flight, pinned host inputs and output images",
+                "requests": e2e_requests,
                 "latency_ms": stream_out["latency_ms"],
                 "sync": {"value": round(e2e_sync_value, 3), "api": "svdi_engine_image_host, one blocking call per step",
                          "latency_ms": {"p50": round(float(np.percentile(e2e_lat, 50)), 3),
