@@ -14,6 +14,7 @@
 #include <condition_variable>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -138,6 +139,7 @@ int HostStager::init() {
     cudaError_t e = cudaMallocHost(&p->ring, kSlots * kSlotBytes);
     for (int s = 0; s < kSlots && e == cudaSuccess; ++s) e = cudaEventCreateWithFlags(&p->ev[s], cudaEventDisableTiming);
     if (e != cudaSuccess) {
+        cudaGetLastError();  // not left for the next launch check to find
         for (int s = 0; s < kSlots; ++s)
             if (p->ev[s]) cudaEventDestroy(p->ev[s]);
         if (p->ring) cudaFreeHost(p->ring);
@@ -150,18 +152,31 @@ int HostStager::init() {
         const int want = std::atoi(env);
         if (want > 0) p->nthreads = std::min(want, 64);
     }
-    for (int w = 1; w < p->nthreads; ++w) p->workers.emplace_back(&Impl::worker, p, w);
+    try {
+        for (int w = 1; w < p->nthreads; ++w) p->workers.emplace_back(&Impl::worker, p, w);
+    } catch (const std::exception&) {  // fewer threads than asked for: slices for those that started
+        p->nthreads = (int)p->workers.size() + 1;
+    }
     impl_ = p;
     return SVDI_OK;
 }
 
+bool HostStager::staged(const void* host, size_t bytes) {
+    if (bytes < kMinStaged || unavailable_ || !pageable(host)) return false;
+    if (init() != SVDI_OK) {
+        unavailable_ = true;
+        set_error("");
+        return false;
+    }
+    return true;
+}
+
 int HostStager::h2d(void* dev, const void* host, size_t bytes, cudaStream_t st) {
     if (bytes == 0) return SVDI_OK;
-    if (bytes < kMinStaged || !pageable(host)) {
+    if (!staged(host, bytes)) {
         SVDI_CUDA(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, st));
         return SVDI_OK;
     }
-    SVDI_TRY(init());
     Impl& I = *impl_;
     for (size_t off = 0; off < bytes; off += kSlotBytes) {
         const size_t n = std::min(kSlotBytes, bytes - off);
@@ -177,12 +192,11 @@ int HostStager::h2d(void* dev, const void* host, size_t bytes, cudaStream_t st) 
 
 int HostStager::d2h(void* host, const void* dev, size_t bytes, cudaStream_t st) {
     if (bytes == 0) return SVDI_OK;
-    if (bytes < kMinStaged || !pageable(host)) {
+    if (!staged(host, bytes)) {
         SVDI_CUDA(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, st));
         SVDI_CUDA(cudaStreamSynchronize(st));
         return SVDI_OK;
     }
-    SVDI_TRY(init());
     Impl& I = *impl_;
     const size_t nch = (bytes + kSlotBytes - 1) / kSlotBytes;
     const int base = I.next;

@@ -234,7 +234,8 @@ int launch_col_fft(float2* d_planes, int nplanes, long long G, long long c0, lon
 // threads copy slices of one slot while the copy engine moves the previous slot, so the host side
 // keeps up with the PCIe link. Pinned, registered or managed memory and copies below a few MB take
 // the plain cudaMemcpyAsync. The ring (three 16 MB slots) and the threads start on the first
-// staged copy. Not thread-safe: one stager serves one engine, whose calls are serialised.
+// staged copy; if its pinned memory cannot be had, every copy takes the plain path. Not
+// thread-safe: one stager serves one engine, whose calls are serialised.
 class HostStager {
 public:
     HostStager() = default;
@@ -253,7 +254,9 @@ public:
 private:
     struct Impl;
     Impl* impl_ = nullptr;
+    bool unavailable_ = false;  // the ring could not be set up: plain copies from then on
     int init();
+    bool staged(const void* host, size_t bytes);
 };
 
 constexpr int kTcKBlock = 32;      // records per K-block (one MMA pair of K steps)
